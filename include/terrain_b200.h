@@ -1,0 +1,119 @@
+/* terrain_b200: the overworld TERRAIN step on one B200, behind a C ABI.
+ *
+ * Drop-in for the reference's GPU generator class mcc::cuda::FullTerrainGenerator
+ * (cuda/include/mccuda_cuda/terrain_gpu.h:31-53 of bonquifo/minecraft-terrain-cuda):
+ * the same chunk-list-in, buffers-out pipeline, with plain pointers, status codes
+ * instead of C++ exceptions, and u16 block-state ids instead of the reference's u8.
+ *
+ * Layouts (identical to the reference's CPU port, cpu/include/mccuda/terrain.h:55-60):
+ *   blocks   per chunk 16 * 16 * height u16, index ((y - min_y) * 16 + z) * 16 + x
+ *   biomes   per chunk 16 * height / 4 u8, index (qy * 4 + qz) * 4 + qx
+ *   chunks   back to back in list order
+ *
+ * Threading: one generator per host thread; calls on one generator are serialised by
+ * the caller. Every call is synchronous on return unless its name says otherwise.
+ */
+#ifndef TERRAIN_B200_H
+#define TERRAIN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tg_status {
+    TG_OK = 0,
+    TG_ERR_INVALID_ARGUMENT = 1,  /* null pointer, bad count, bad config */
+    TG_ERR_MODEL_MISMATCH = 2,    /* model files differ from the model compiled in */
+    TG_ERR_CUDA = 3,              /* a CUDA runtime call failed (message in tg_last_error_string) */
+    TG_ERR_OUT_OF_MEMORY = 4,     /* device or pinned allocation failed */
+    TG_ERR_RANGE = 5,             /* chunk coordinate outside |c| < 2^23 */
+    TG_ERR_NO_SEED = 6,           /* tg_generate before tg_set_seed */
+    TG_ERR_DEVICE_TIMEOUT = 7,    /* a bounded device-side wait expired */
+    TG_ERR_INTERNAL = 8
+} tg_status;
+
+/* reference: mcc::cuda::ChunkXZ (cuda/include/mccuda_cuda/generator.h:14-16) */
+typedef struct tg_chunk_xz {
+    int32_t x, z;
+} tg_chunk_xz;
+
+/* reference: FullTerrainGenerator(ir, tm, max_batch_chunks, pipeline_slots)
+ * (cuda/include/mccuda_cuda/terrain_gpu.h:33); device selects the CUDA device. */
+typedef struct tg_config {
+    int32_t max_batch_chunks; /* chunks per device batch; 0 = 2048 */
+    int32_t pipeline_slots;   /* batches in flight (1 or 2); 0 = 2 */
+    int32_t device;           /* CUDA device ordinal */
+} tg_config;
+
+/* reference: TerrainTiming (cuda/include/mccuda_cuda/terrain_gpu.h:15-22); milliseconds
+ * of device time per stage summed over batches, plus host wall time of the call. */
+typedef struct tg_timing {
+    float h2d_ms, biome_ms, noise_ms, aquifer_ms, fill_ms, surface_ms, d2h_ms, kernel_ms, wall_ms;
+    int32_t batches;
+} tg_timing;
+
+/* Creates a generator for the model compiled into the library. ir_json_path and
+ * terrain_json_path, when not NULL, must be the files it was generated from
+ * (checked by SHA-256; TG_ERR_MODEL_MISMATCH otherwise).
+ * reference: FullTerrainGenerator::FullTerrainGenerator (cuda/src/terrain.cu:1375, :1105-1122) */
+tg_status tg_create(const char* ir_json_path, const char* terrain_json_path, const tg_config* config, struct tg_generator** out);
+
+/* reference: ~FullTerrainGenerator */
+tg_status tg_destroy(struct tg_generator* gen);
+
+/* Builds the per-seed noise tables, random factories and zoom seed on the host and
+ * uploads them. reference: FullTerrainGenerator::set_seed (cuda/src/terrain.cu:1387, :1176-1255) */
+tg_status tg_set_seed(struct tg_generator* gen, int64_t seed);
+
+/* The TERRAIN step for count chunks. blocks_out: count * 16 * 16 * height u16 (required);
+ * biomes_out: count * 16 * height / 4 u8 (may be NULL); aquifer_out: the blocks after the
+ * aquifer fill and before the material rules (may be NULL); timing may be NULL.
+ * Host buffers; pinned ones (tg_alloc_pinned) copy fastest.
+ * reference: FullTerrainGenerator::generate (cuda/src/terrain.cu:1392-1417) */
+tg_status tg_generate(struct tg_generator* gen, const tg_chunk_xz* chunks, int32_t count, uint16_t* blocks_out, uint8_t* biomes_out,
+                      uint16_t* aquifer_out, tg_timing* timing);
+
+/* Device-resident form: chunks, blocks_out and biomes_out (may be NULL) are device
+ * pointers; count <= max_batch_chunks; runs on the generator's stream and returns
+ * when the work is done. No counterpart in the reference (its buffers are host-side);
+ * used to measure the kernels with inputs already in HBM. */
+tg_status tg_generate_device(struct tg_generator* gen, const tg_chunk_xz* chunks_dev, int32_t count, uint16_t* blocks_dev, uint8_t* biomes_dev,
+                             tg_timing* timing);
+
+/* Multi-seed batch: each request is its own seed and chunk list; all requests run in
+ * shared device batches with positions deduplicated per seed. Output buffers are host
+ * memory per request. No counterpart in the reference (single seed per generator). */
+typedef struct tg_request {
+    int64_t seed;
+    const tg_chunk_xz* chunks;
+    int32_t count;
+    uint16_t* blocks_out;
+    uint8_t* biomes_out; /* may be NULL */
+} tg_request;
+tg_status tg_generate_batch(struct tg_generator* gen, const tg_request* requests, int32_t n, tg_timing* timing);
+
+/* BiomeManager.getBiome at block positions (xyz triples) for one seed per position,
+ * with the chunk's R-tree chain exactly as the TERRAIN step computes it.
+ * reference semantics: zoomed_biome over cpu_chunk_biomes (cpu/src/biome.cpp:272-289,
+ * cpu/src/terrain.cpp:152-176). */
+tg_status tg_biome_lookup(struct tg_generator* gen, const int64_t* seeds, const int32_t* xyz, int32_t n, uint8_t* out);
+
+/* Pinned host memory for outputs. reference: alloc_pinned / free_pinned
+ * (cuda/include/mccuda_cuda/terrain_gpu.h:62-63) */
+void* tg_alloc_pinned(size_t bytes);
+void tg_free_pinned(void* p);
+
+/* Model constants: min_y, height, sea_level, palette size, biome count. */
+tg_status tg_model_info(int32_t* min_y, int32_t* height, int32_t* sea_level, int32_t* palette_size, int32_t* biome_count);
+
+/* Message of the last failing call on this thread (empty if none). */
+const char* tg_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TERRAIN_B200_H */

@@ -1,0 +1,983 @@
+// Per-element bodies of the TERRAIN-step kernels (host + device).
+//
+// Each body computes one work item of one kernel from the Batch it is given, so the
+// sm_100a kernels in terrain.cu are one-line wrappers, and a test-only host build can
+// run the same bodies to check generated code on the CPU.
+//
+// Stage -> reference (cpu/src/terrain.cpp unless noted):
+//   biome chunks      cpu_chunk_biomes :152-176 (climate, quantize, R-tree chain)
+//   corner channels   VolumeEvaluator::sample_interpolated_block_step, volume_eval.cpp:619-674
+//   surface levels    Aquifer::max_surface_level / surface_level :307-331 (volume vs point)
+//   aquifer cells     Aquifer location / compute_fluid :225-241, :343-408
+//   fill              cpu_terrain_from_biomes :782-805, Aquifer::compute_substance :217-272
+//   surface           Surface::build :477-522 and its extensions :677-725
+#pragma once
+
+#include <climits>
+
+#include "model_gen.cuh"
+#include "tb_host.h"
+
+namespace tb {
+
+constexpr int kQuartsPerChunk = 16 * (tbm::kHeight / 4);
+constexpr int kBlocksPerChunk = 256 * tbm::kHeight;
+constexpr int kRows = tbm::kHeight / 8 + 1;              // 4x8 cell corner rows
+constexpr int kCellsY = tbm::kHeight / 8;
+constexpr int kMaxY = tbm::kMinY + tbm::kHeight - 1;
+constexpr int kGridX = 27, kGridZ = 19, kGrid = kGridX * kGridZ;   // surface-level quarts per chunk
+constexpr int kAqX = 3, kAqY = 35, kAqZ = 3, kAqCells = kAqX * kAqY * kAqZ;
+constexpr int kAqMinGridY = -7;
+constexpr int kWayBelowMinY = -2032 * 16;   // DimensionType.WAY_BELOW_MIN_Y
+constexpr int kMaxGradientRandoms = 8;
+constexpr int kSearchStack = 16;
+static_assert(tbm::kNumGradientRandoms <= kMaxGradientRandoms, "too many vertical-gradient random names");
+static_assert(tbm::kHeight % 16 == 0 && tbm::kMinY % 16 == 0, "world height must be section aligned");
+
+// ---- device-resident model and per-seed tables -------------------------------------------------
+struct DevModel {
+    const RNode* tree;
+    const int32_t* children;
+    const int32_t* leaf_biome;
+    const int32_t* leaf_node;
+    const int32_t* leaf_rank;
+    int32_t root;
+    const uint8_t* block_flags;     // 1 air, 2 water, 4 lava, 8 fluid
+    const float* biome_temp;
+    const uint8_t* biome_frozen;
+    Simplex2 temp, frozen[3], info;
+    float frozen_amp[3];
+    double f2, g2;
+};
+
+struct DevSeed {
+    NoiseTables nt;
+    Positional random, aquifer, ore;
+    Positional gradient[kMaxGradientRandoms];
+    int64_t zoom_seed;
+    uint16_t clay[192];
+};
+
+// Open-addressing table deduplicating 64-bit position keys; unique keys get dense
+// indices in insertion order of the winning thread.
+struct HashTab {
+    unsigned long long* keys;   // kEmpty when free
+    int32_t* vals;
+    unsigned long long* uniq;
+    int32_t* count;
+    uint32_t mask;
+};
+constexpr unsigned long long kEmpty = ~0ull;
+
+struct Batch {
+    DevModel M;
+    const DevSeed* seeds;
+    int32_t n;                        // chunks in the batch
+    const int32_t* cx;                // chunk coordinates, seed slot
+    const int32_t* cz;
+    const int32_t* cseed;
+    // biome chunks: the union of the 3x3 neighbourhoods
+    HashTab hb;
+    int32_t nb_cap;
+    int32_t* nb9;                     // n * 9 biome-chunk indices, (dz + 1) * 3 + dx + 1
+    float* bcol;                      // nb_cap * 16 * kClimateCols
+    long long* tgt;                   // nb_cap * kQuartsPerChunk * 6, chain order
+    int32_t* lstar;                   // first minimal leaf per quart, chain order
+    long long* mdist;                 // its distance
+    uint8_t* qbiome;                  // nb_cap * kQuartsPerChunk, (qy * 4 + qz) * 4 + qx
+    // corner columns of the 4x8 channels
+    HashTab hc;
+    int32_t cc_cap;
+    int32_t* c25;                     // n * 25 corner-column indices, (k) * 5 + i
+    float* ccol;                      // cc_cap * kCornerCols
+    float* corners;                   // cc_cap * kRows * kNumChannels
+    // surface-level quarts (find_top_surface), volume or point semantics
+    HashTab hs;
+    int32_t sg_cap;
+    int32_t* g513;                    // n * kGrid indices
+    float* sfts;                      // sg_cap: find_top_surface value per unique quart
+    // aquifer
+    int32_t* aq_loc;                  // n * kAqCells * 3 (x, y, z)
+    int32_t* aq_status;               // n * kAqCells * 2 (level, fluid state)
+    int32_t* aq_skip;                 // n
+    // outputs and heights
+    uint16_t* blocks;                 // n * kBlocksPerChunk
+    uint16_t* aquifer_copy;           // optional copy after the fill
+    int32_t* h0;                      // n * 256, x * 16 + z: heights after the fill
+    int32_t* h1;                      // after the eroded-badlands extension
+    int32_t* h2;                      // after the frozen-ocean extension (dry run)
+    uint8_t* biomes_out;              // n * kQuartsPerChunk
+};
+
+// ---- atomics (device) / plain operations (host test build) --------------------------------------
+TB_HD TB_FI unsigned long long cas64(unsigned long long* p, unsigned long long cmp, unsigned long long val) {
+#if defined(__CUDA_ARCH__)
+    return atomicCAS(p, cmp, val);
+#else
+    const unsigned long long old = *p;
+    if (old == cmp) *p = val;
+    return old;
+#endif
+}
+TB_HD TB_FI int32_t add32(int32_t* p, int32_t v) {
+#if defined(__CUDA_ARCH__)
+    return atomicAdd(p, v);
+#else
+    const int32_t old = *p;
+    *p += v;
+    return old;
+#endif
+}
+TB_HD TB_FI void max32(int32_t* p, int32_t v) {
+#if defined(__CUDA_ARCH__)
+    atomicMax(p, v);
+#else
+    if (v > *p) *p = v;
+#endif
+}
+
+TB_HD TB_FI uint32_t hash_slot(unsigned long long k, uint32_t mask) {
+    unsigned long long h = k * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 32;
+    return static_cast<uint32_t>(h) & mask;
+}
+
+TB_HD inline void ht_insert(const HashTab& t, unsigned long long key) {
+    uint32_t s = hash_slot(key, t.mask);
+    for (uint32_t probe = 0; probe <= t.mask; ++probe) {
+        const unsigned long long prev = cas64(&t.keys[s], kEmpty, key);
+        if (prev == kEmpty) {
+            const int32_t idx = add32(t.count, 1);
+            t.vals[s] = idx;
+            t.uniq[idx] = key;
+            return;
+        }
+        if (prev == key) return;
+        s = (s + 1) & t.mask;
+    }
+}
+
+TB_HD inline int32_t ht_find(const HashTab& t, unsigned long long key) {
+    uint32_t s = hash_slot(key, t.mask);
+    for (uint32_t probe = 0; probe <= t.mask; ++probe) {
+        const unsigned long long k = t.keys[s];
+        if (k == key) return t.vals[s];
+        if (k == kEmpty) return -1;
+        s = (s + 1) & t.mask;
+    }
+    return -1;
+}
+
+// Keys: 27-bit offset coordinates (|v| < 2^26), a semantics bit and a 9-bit seed slot.
+constexpr int64_t kKeyBias = 1ll << 26;
+TB_HD TB_FI unsigned long long pack_key(int32_t slot, int32_t a, int32_t b, int32_t sem) {
+    return (static_cast<unsigned long long>(slot) << 55) | (static_cast<unsigned long long>(sem & 1) << 54) |
+           (static_cast<unsigned long long>(static_cast<int64_t>(a) + kKeyBias) << 27) | static_cast<unsigned long long>(static_cast<int64_t>(b) + kKeyBias);
+}
+TB_HD TB_FI void unpack_key(unsigned long long k, int32_t& slot, int32_t& a, int32_t& b, int32_t& sem) {
+    slot = static_cast<int32_t>(k >> 55);
+    sem = static_cast<int32_t>((k >> 54) & 1);
+    a = static_cast<int32_t>(static_cast<int64_t>((k >> 27) & ((1ull << 27) - 1)) - kKeyBias);
+    b = static_cast<int32_t>(static_cast<int64_t>(k & ((1ull << 27) - 1)) - kKeyBias);
+}
+
+// ---- dedupe stages ----------------------------------------------------------------------------
+// biome chunks (item = chunk * 9 + neighbour)
+TB_HD inline void body_nb_insert(const Batch& B, int i) {
+    const int c = i / 9, k = i % 9;
+    ht_insert(B.hb, pack_key(B.cseed[c], B.cx[c] + k % 3 - 1, B.cz[c] + k / 3 - 1, 0));
+}
+TB_HD inline void body_nb_resolve(const Batch& B, int i) {
+    const int c = i / 9, k = i % 9;
+    B.nb9[i] = ht_find(B.hb, pack_key(B.cseed[c], B.cx[c] + k % 3 - 1, B.cz[c] + k / 3 - 1, 0));
+}
+// corner columns in quart units (item = chunk * 25 + k * 5 + i)
+TB_HD inline void body_cc_insert(const Batch& B, int it) {
+    const int c = it / 25, k = (it % 25) / 5, i = it % 5;
+    ht_insert(B.hc, pack_key(B.cseed[c], B.cx[c] * 4 + i, B.cz[c] * 4 + k, 0));
+}
+TB_HD inline void body_cc_resolve(const Batch& B, int it) {
+    const int c = it / 25, k = (it % 25) / 5, i = it % 5;
+    B.c25[it] = ht_find(B.hc, pack_key(B.cseed[c], B.cx[c] * 4 + i, B.cz[c] * 4 + k, 0));
+}
+// surface-level quarts: 27 x 19 per chunk; the 11 x 11 window of the aquifer's
+// constructor uses volume semantics (sem 1), the rest the lazy point path (sem 0).
+TB_HD TB_FI unsigned long long sg_key(const Batch& B, int c, int g) {
+    const int gx = g % kGridX, gz = g / kGridX;
+    const int qx = B.cx[c] * 4 - 16 + gx, qz = B.cz[c] * 4 - 8 + gz;
+    const bool win = qx >= B.cx[c] * 4 - 4 && qx <= B.cx[c] * 4 + 6 && qz >= B.cz[c] * 4 - 4 && qz <= B.cz[c] * 4 + 6;
+    return pack_key(B.cseed[c], qx, qz, win ? 1 : 0);
+}
+TB_HD inline void body_sg_insert(const Batch& B, int it) { ht_insert(B.hs, sg_key(B, it / kGrid, it % kGrid)); }
+TB_HD inline void body_sg_resolve(const Batch& B, int it) { B.g513[it] = ht_find(B.hs, sg_key(B, it / kGrid, it % kGrid)); }
+
+// ---- biomes -------------------------------------------------------------------------------------
+// chain position p -> quart (qx, qy, qz): vanilla order sections, x, y, z
+TB_HD TB_FI void chain_quart(int p, int& qx, int& qy, int& qz) {
+    qz = p & 3;
+    const int y = (p >> 2) & 3;
+    qx = (p >> 4) & 3;
+    qy = (p >> 6) * 4 + y;
+}
+TB_HD TB_FI int chain_pos(int qx, int qy, int qz) { return (((qy >> 2) * 4 + qx) * 4 + (qy & 3)) * 4 + qz; }
+
+TB_HD inline void body_climate_col(const Batch& B, int it) {
+    const int b = it / 16, col = it % 16;
+    if (b >= *B.hb.count) return;
+    int32_t slot, bx, bz, sem;
+    unpack_key(B.hb.uniq[b], slot, bx, bz, sem);
+    const DevSeed& S = B.seeds[slot];
+    tbgen::gen_climate_col(S.nt, bx * 16 + 4 * (col & 3), bz * 16 + 4 * (col >> 2), B.bcol + static_cast<size_t>(it) * tbm::kClimateCols);
+}
+
+TB_HD TB_FI long long param_dist(const RNode& n, const long long* t) {
+    long long d = 0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        const long long tv = i < 6 ? t[i] : 0;
+        const long long above = tv - n.mx[i], below = n.mn[i] - tv;
+        const long long p = above > 0 ? above : (below > 0 ? below : 0);
+        d += p * p;
+    }
+    return d;
+}
+
+// First minimal leaf in depth-first order: the minimum of (distance, leaf rank) over
+// all leaves, pruned with a known leaf as the starting best.
+TB_HD inline int tree_first_min(const DevModel& M, const long long* t, int start_leaf, long long& best_d) {
+    int best = start_leaf;
+    int best_rank = M.leaf_rank[start_leaf];
+    best_d = param_dist(M.tree[M.leaf_node[start_leaf]], t);
+    int stack_node[kSearchStack], stack_next[kSearchStack];
+    int sp = 0;
+    stack_node[0] = M.root;
+    stack_next[0] = 0;
+    sp = 1;
+    while (sp > 0) {
+        const RNode& nd = M.tree[stack_node[sp - 1]];
+        const int k = stack_next[sp - 1];
+        if (k >= nd.child_count) {
+            --sp;
+            continue;
+        }
+        stack_next[sp - 1] = k + 1;
+        const int ci = M.children[nd.first_child + k];
+        const RNode& ch = M.tree[ci];
+        const long long d = param_dist(ch, t);
+        if (d < best_d || (d == best_d && ch.rank < best_rank)) {
+            if (ch.leaf >= 0) {
+                best = ch.leaf;
+                best_rank = ch.rank;
+                best_d = d;
+            } else if (sp < kSearchStack) {
+                stack_node[sp] = ci;
+                stack_next[sp] = 0;
+                ++sp;
+            }
+        }
+    }
+    return best;
+}
+
+// One quart column run: climate per quart, quantized targets, first minimal leaf.
+// item = (biome chunk * 16 + column) * kRuns + run; a run is kRun consecutive quarts in y.
+constexpr int kRun = 8;
+constexpr int kRuns = (tbm::kHeight / 4) / kRun;
+static_assert((tbm::kHeight / 4) % kRun == 0, "quart run must divide the quart height");
+TB_HD inline void body_climate_quart(const Batch& B, int it) {
+    const int run = it % kRuns, cidx = it / kRuns, b = cidx / 16, col = cidx % 16;
+    if (b >= *B.hb.count) return;
+    int32_t slot, bx, bz, sem;
+    unpack_key(B.hb.uniq[b], slot, bx, bz, sem);
+    const DevSeed& S = B.seeds[slot];
+    const int qx = col & 3, qz = col >> 2;
+    const int x = bx * 16 + 4 * qx, z = bz * 16 + 4 * qz;
+    const float* colv = B.bcol + static_cast<size_t>(cidx) * tbm::kClimateCols;
+    int prev = 0;
+    for (int r = 0; r < kRun; ++r) {
+        const int qy = run * kRun + r;
+        float cl[6];
+        tbgen::gen_climate(S.nt, x, tbm::kMinY + 4 * qy, z, colv, cl);
+        long long t[6];
+        for (int k = 0; k < 6; ++k) t[k] = f2l(cl[k] * 10000.0f);
+        long long md;
+        const int leaf = tree_first_min(B.M, t, prev, md);
+        prev = leaf;
+        const size_t p = static_cast<size_t>(b) * kQuartsPerChunk + chain_pos(qx, qy, qz);
+        for (int k = 0; k < 6; ++k) B.tgt[p * 6 + k] = t[k];
+        B.lstar[p] = leaf;
+        B.mdist[p] = md;
+    }
+}
+
+// The last-result rule: the previous result is kept while it reaches the minimum.
+TB_HD inline void body_chain(const Batch& B, int b) {
+    if (b >= *B.hb.count) return;
+    const size_t base = static_cast<size_t>(b) * kQuartsPerChunk;
+    int last = -1;
+    for (int p = 0; p < kQuartsPerChunk; ++p) {
+        int r = B.lstar[base + p];
+        if (last >= 0 && last != r) {
+            if (param_dist(B.M.tree[B.M.leaf_node[last]], B.tgt + (base + p) * 6) == B.mdist[base + p]) r = last;
+        }
+        last = r;
+        int qx, qy, qz;
+        chain_quart(p, qx, qy, qz);
+        B.qbiome[base + (qy * 4 + qz) * 4 + qx] = static_cast<uint8_t>(B.M.leaf_biome[r]);
+    }
+}
+
+// ---- corner channels ----------------------------------------------------------------------------
+TB_HD inline void body_corner_col(const Batch& B, int u) {
+    if (u >= *B.hc.count) return;
+    int32_t slot, qx, qz, sem;
+    unpack_key(B.hc.uniq[u], slot, qx, qz, sem);
+    tbgen::gen_corner_col(B.seeds[slot].nt, qx * 4, qz * 4, B.ccol + static_cast<size_t>(u) * tbm::kCornerCols);
+}
+TB_HD inline void body_corner(const Batch& B, int it) {
+    const int u = it / kRows, row = it % kRows;
+    if (u >= *B.hc.count) return;
+    int32_t slot, qx, qz, sem;
+    unpack_key(B.hc.uniq[u], slot, qx, qz, sem);
+    tbgen::gen_corner(B.seeds[slot].nt, qx * 4, tbm::kMinY + 8 * row, qz * 4, B.ccol + static_cast<size_t>(u) * tbm::kCornerCols,
+                      B.corners + static_cast<size_t>(it) * tbm::kNumChannels);
+}
+
+// ---- surface levels and aquifer cells ---------------------------------------------------------------
+TB_HD inline void body_surface_level(const Batch& B, int u) {
+    if (u >= *B.hs.count) return;
+    int32_t slot, qx, qz, sem;
+    unpack_key(B.hs.uniq[u], slot, qx, qz, sem);
+    const NoiseTables& T = B.seeds[slot].nt;
+    B.sfts[u] = sem ? tbgen::gen_fts_vol(T, qx * 4, qz * 4) : tbgen::gen_fts_pt(T, qx * 4, qz * 4);
+}
+
+struct Fluid {
+    int32_t level, type;
+    TB_HD TB_FI int at(int y) const { return y < level ? type : tbm::kAir; }
+};
+TB_HD TB_FI Fluid global_fluid(int y) {
+    constexpr int lava_level = tbm::kTmSeaLevel < -54 ? tbm::kTmSeaLevel : -54;
+    return y < lava_level ? Fluid{-54, tbm::kLava} : Fluid{tbm::kTmSeaLevel, tbm::kDefaultFluid};
+}
+
+// BlockPos packing: 26 bits x, 12 bits y, 26 bits z (two's complement fields)
+TB_HD TB_FI void blockpos_wrap(int32_t& x, int32_t& y, int32_t& z) {
+    const uint64_t v = ((static_cast<uint64_t>(static_cast<int64_t>(x)) & 0x3FFFFFFull) << 38) |
+                       ((static_cast<uint64_t>(static_cast<int64_t>(z)) & 0x3FFFFFFull) << 12) | (static_cast<uint64_t>(static_cast<int64_t>(y)) & 0xFFFull);
+    const int64_t s = static_cast<int64_t>(v);
+    x = static_cast<int32_t>(s >> 38);
+    y = static_cast<int32_t>(static_cast<int64_t>(v << 52) >> 52);
+    z = static_cast<int32_t>(static_cast<int64_t>(v << 26) >> 38);
+}
+
+// surface level at block (sx, sz) as seen by chunk c
+TB_HD TB_FI int surface_at(const Batch& B, int c, int sx, int sz) {
+    const int gx = (sx >> 2) - (B.cx[c] * 4 - 16), gz = (sz >> 2) - (B.cz[c] * 4 - 8);
+    return jfloor(static_cast<double>(B.sfts[B.g513[static_cast<size_t>(c) * kGrid + gz * kGridX + gx]]));
+}
+
+TB_HD inline void body_aquifer_cell(const Batch& B, int it) {
+    const int c = it / kAqCells, cell = it % kAqCells;
+    const int ix = cell % kAqX, iz = (cell / kAqX) % kAqZ, iy = cell / (kAqX * kAqZ);
+    const int gx = B.cx[c] - 1 + ix, gy = kAqMinGridY + iy, gz = B.cz[c] - 1 + iz;
+    const DevSeed& S = B.seeds[B.cseed[c]];
+    Xoro r = S.aquifer.at(gx, gy, gz);
+    int32_t x = gx * 16 + r.next_int(10);
+    int32_t y = gy * 12 + r.next_int(9);
+    int32_t z = gz * 16 + r.next_int(10);
+    blockpos_wrap(x, y, z);
+    int32_t* loc = B.aq_loc + static_cast<size_t>(it) * 3;
+    loc[0] = x;
+    loc[1] = y;
+    loc[2] = z;
+    // NoiseBasedAquifer.computeFluid
+    const Fluid glob = global_fluid(y);
+    Fluid res{0, 0};
+    bool done = false;
+    int lowest = INT_MAX;
+    const int top = y + 12, bottom = y - 12;
+    bool center_under = false;
+    const signed char off[13][2] = {{0, 0}, {-2, -1}, {-1, -1}, {0, -1}, {1, -1}, {-3, 0}, {-2, 0}, {-1, 0}, {1, 0}, {-2, 1}, {-1, 1}, {0, 1}, {1, 1}};
+    for (int k = 0; k < 13 && !done; ++k) {
+        const int sx = x + (off[k][0] << 4), sz = z + (off[k][1] << 4);
+        const int level = surface_at(B, c, sx, sz);
+        const int adjusted = level + 8;
+        const bool start = k == 0;
+        if (start && bottom > adjusted) {
+            res = glob;
+            done = true;
+            break;
+        }
+        const bool pokes = top > adjusted;
+        if (pokes || start) {
+            const Fluid at_s = global_fluid(adjusted);
+            if (at_s.at(adjusted) != tbm::kAir) {
+                if (start) center_under = true;
+                if (pokes) {
+                    res = at_s;
+                    done = true;
+                    break;
+                }
+            }
+        }
+        lowest = lowest < level ? lowest : level;
+    }
+    if (!done) {
+        const NoiseTables& T = S.nt;
+        double partially, fully;
+        if (tbgen::gen_aq_exclusion(T, x, y, z) > 0.0f) {
+            partially = -1.0;
+            fully = -1.0;
+        } else {
+            const int below = lowest + 8 - y;
+            double factor = 0.0;
+            if (center_under) {
+                const double f = (static_cast<double>(below) - 0.0) / (64.0 - 0.0);
+                factor = f < 0.0 ? 1.0 : (f > 1.0 ? 0.0 : 1.0 + f * (0.0 - 1.0));
+            }
+            const double noise = jclampd(static_cast<double>(tbgen::gen_aq_fluid_level_floodedness(T, x, y, z)), -1.0, 1.0);
+            const double fully_t = -0.3 + ((factor - 1.0) / (0.0 - 1.0)) * (0.8 - -0.3);
+            const double partial_t = -0.8 + ((factor - 1.0) / (0.0 - 1.0)) * (0.4 - -0.8);
+            partially = noise - partial_t;
+            fully = noise - fully_t;
+        }
+        int level;
+        if (fully > 0.0) {
+            level = glob.level;
+        } else if (partially > 0.0) {
+            const int scx = fdiv(x, 16), scy = fdiv(y, 40), scz = fdiv(z, 16);
+            const int middle = scy * 40 + 20;
+            const double spread = static_cast<double>(tbgen::gen_aq_fluid_level_spread(T, scx, scy, scz) * 10.0f);
+            const int q = jfloor(spread / 3.0) * 3;
+            level = lowest < middle + q ? lowest : middle + q;
+        } else {
+            level = kWayBelowMinY;
+        }
+        int type = glob.type;
+        if (level <= -10 && level != kWayBelowMinY && glob.type != tbm::kLava) {
+            const double lv = static_cast<double>(tbgen::gen_aq_lava(T, fdiv(x, 64), fdiv(y, 40), fdiv(z, 64)));
+            if (dabs(lv) > 0.3) type = tbm::kLava;
+        }
+        res = Fluid{level, type};
+    }
+    int32_t* st = B.aq_status + static_cast<size_t>(it) * 2;
+    st[0] = res.level;
+    st[1] = res.type;
+}
+
+// per-chunk skip height from the volume-semantics window maximum
+TB_HD inline void body_aquifer_skip(const Batch& B, int c) {
+    int mx = INT_MIN;
+    for (int gz = 4; gz <= 14; ++gz)
+        for (int gx = 12; gx <= 22; ++gx) {
+            const int v = jfloor(static_cast<double>(B.sfts[B.g513[static_cast<size_t>(c) * kGrid + gz * kGridX + gx]]));
+            mx = v > mx ? v : mx;
+        }
+    const int adjusted = mx + 8;
+    const int skip_grid_y = fdiv(adjusted + 12, 12) + 1;
+    B.aq_skip[c] = skip_grid_y * 12 + 11 - 1;
+}
+
+// ---- fill: channels, final density, aquifer substance --------------------------------------------
+TB_HD TB_FI double aq_similarity(int a, int b) { return 1.0 - static_cast<double>(b - a) / 25.0; }
+
+struct AqBlock {
+    const int32_t* loc;
+    const int32_t* st;
+    int cx, cz;
+};
+
+TB_HD inline double aq_pressure(const NoiseTables& T, int x, int y, int z, double& barrier, bool& barrier_set, Fluid a, Fluid b) {
+    const int t1 = a.at(y), t2 = b.at(y);
+    if ((t1 == tbm::kLava && t2 == tbm::kWater) || (t1 == tbm::kWater && t2 == tbm::kLava)) return 2.0;
+    const int diff = a.level - b.level < 0 ? b.level - a.level : a.level - b.level;
+    if (diff == 0) return 0.0;
+    const double average = 0.5 * static_cast<double>(a.level + b.level);
+    const double above = static_cast<double>(y) + 0.5 - average;
+    const double base = static_cast<double>(diff) / 2.0;
+    const double towards = base - dabs(above);
+    double gradient;
+    if (above > 0.0) {
+        const double center = 0.0 + towards;
+        gradient = center > 0.0 ? center / 1.5 : center / 2.5;
+    } else {
+        const double center = 3.0 + towards;
+        gradient = center > 0.0 ? center / 3.0 : center / 10.0;
+    }
+    double noise;
+    if (!(gradient < -2.0) && !(gradient > 2.0)) {
+        if (!barrier_set) {
+            barrier = static_cast<double>(tbgen::gen_aq_barrier(T, x, y, z));
+            barrier_set = true;
+        }
+        noise = barrier;
+    } else {
+        noise = 0.0;
+    }
+    return 2.0 * (noise + gradient);
+}
+
+// NoiseBasedAquifer.computeSubstance; -1 = keep the default block.
+TB_HD inline int aq_substance(const NoiseTables& T, const AqBlock& A, int skip, int x, int y, int z, double density) {
+    if (density > 0.0) return -1;
+    const Fluid glob = global_fluid(y);
+    if (y > skip) return glob.at(y);
+    if (glob.at(y) == tbm::kLava) return tbm::kLava;
+    const int xa = (x - 5) >> 4, ya = fdiv(y + 1, 12), za = (z - 5) >> 4;
+    int d1 = INT_MAX, d2 = INT_MAX, d3 = INT_MAX, d4 = INT_MAX;
+    int i1 = 0, i2 = 0, i3 = 0, i4 = 0;
+    for (int ox = 0; ox <= 1; ++ox)
+        for (int oy = -1; oy <= 1; ++oy)
+            for (int oz = 0; oz <= 1; ++oz) {
+                const int ix = xa + ox - (A.cx - 1), iy = ya + oy - kAqMinGridY, iz = za + oz - (A.cz - 1);
+                const int idx = (iy * kAqZ + iz) * kAqX + ix;
+                const int32_t* l = A.loc + idx * 3;
+                const int dx = l[0] - x, dy = l[1] - y, dz = l[2] - z;
+                const int nd = dx * dx + dy * dy + dz * dz;
+                if (d1 >= nd) {
+                    i4 = i3; i3 = i2; i2 = i1; i1 = idx;
+                    d4 = d3; d3 = d2; d2 = d1; d1 = nd;
+                } else if (d2 >= nd) {
+                    i4 = i3; i3 = i2; i2 = idx;
+                    d4 = d3; d3 = d2; d2 = nd;
+                } else if (d3 >= nd) {
+                    i4 = i3; i3 = idx;
+                    d4 = d3; d3 = nd;
+                } else if (d4 >= nd) {
+                    i4 = idx;
+                    d4 = nd;
+                }
+            }
+    (void)i4;
+    auto status = [&](int idx) { return Fluid{A.st[idx * 2], A.st[idx * 2 + 1]}; };
+    const Fluid s1 = status(i1);
+    const double sim12 = aq_similarity(d1, d2);
+    const int fluid = s1.at(y);
+    if (sim12 <= 0.0) return fluid;
+    if (fluid == tbm::kWater && global_fluid(y - 1).at(y - 1) == tbm::kLava) return fluid;
+    double barrier = 0.0;
+    bool barrier_set = false;
+    const Fluid s2 = status(i2);
+    const double b12 = sim12 * aq_pressure(T, x, y, z, barrier, barrier_set, s1, s2);
+    if (density + b12 > 0.0) return -1;
+    const Fluid s3 = status(i3);
+    const double sim13 = aq_similarity(d1, d3);
+    if (sim13 > 0.0) {
+        const double b13 = sim12 * sim13 * aq_pressure(T, x, y, z, barrier, barrier_set, s1, s3);
+        if (density + b13 > 0.0) return -1;
+    }
+    const double sim23 = aq_similarity(d2, d3);
+    if (sim23 > 0.0) {
+        const double b23 = sim12 * sim23 * aq_pressure(T, x, y, z, barrier, barrier_set, s2, s3);
+        if (density + b23 > 0.0) return -1;
+    }
+    return fluid;
+}
+
+// Channel values for the 8 blocks of one column cell: the block-step interpolation
+// order of InterpolatedFunction (z, then x, then y in increments).
+struct CellInterp {
+    float a0[tbm::kNumChannels], step[tbm::kNumChannels];
+};
+TB_HD inline void cell_interp(const Batch& B, int c, int lx, int lz, int cell_y, CellInterp& out) {
+    const int ci = lx >> 2, xi = lx & 3, ck = lz >> 2, zi = lz & 3;
+    const int32_t* cc = B.c25 + static_cast<size_t>(c) * 25;
+    const size_t u00 = cc[ck * 5 + ci], u10 = cc[ck * 5 + ci + 1], u01 = cc[(ck + 1) * 5 + ci], u11 = cc[(ck + 1) * 5 + ci + 1];
+    const int C = tbm::kNumChannels;
+    const float* p00 = B.corners + (u00 * kRows + cell_y) * C;
+    const float* p10 = B.corners + (u10 * kRows + cell_y) * C;
+    const float* p01 = B.corners + (u01 * kRows + cell_y) * C;
+    const float* p11 = B.corners + (u11 * kRows + cell_y) * C;
+    const float az = static_cast<float>(zi) * 0.25f, ax = static_cast<float>(xi) * 0.25f;
+    for (int k = 0; k < C; ++k) {
+        const float v000 = p00[k], v100 = p10[k], v001 = p01[k], v101 = p11[k];
+        const float v010 = p00[C + k], v110 = p10[C + k], v011 = p01[C + k], v111 = p11[C + k];
+        const float v00 = lerpf(az, v000, v001), v01 = lerpf(az, v010, v011);
+        const float v10 = lerpf(az, v100, v101), v11 = lerpf(az, v110, v111);
+        const float a0 = lerpf(ax, v00, v10), a1 = lerpf(ax, v01, v11);
+        out.step[k] = (a1 - a0) * 0.125f;
+        out.a0[k] = a0 + out.step[k] * 0.0f;
+    }
+}
+
+// item = (chunk * kCellsY + cell_y) * 256 + z * 16 + x: the 8 blocks of one cell column
+TB_HD inline void body_fill(const Batch& B, int it) {
+    const int col = it & 255, cell_y = (it >> 8) % kCellsY, c = (it >> 8) / kCellsY;
+    const int lx = col & 15, lz = col >> 4;
+    const int bx = B.cx[c] * 16 + lx, bz = B.cz[c] * 16 + lz;
+    const DevSeed& S = B.seeds[B.cseed[c]];
+    CellInterp ci;
+    cell_interp(B, c, lx, lz, cell_y, ci);
+    float ch[tbm::kNumChannels];
+    for (int k = 0; k < tbm::kNumChannels; ++k) ch[k] = ci.a0[k];
+    const AqBlock A{B.aq_loc + static_cast<size_t>(c) * kAqCells * 3, B.aq_status + static_cast<size_t>(c) * kAqCells * 2, B.cx[c], B.cz[c]};
+    const int skip = B.aq_skip[c];
+    uint16_t* out = B.blocks + static_cast<size_t>(c) * kBlocksPerChunk;
+    int top = INT_MIN;
+    for (int k = 0; k < 8; ++k) {
+        const int y = tbm::kMinY + cell_y * 8 + k;
+        const float d = tbgen::gen_final_density(S.nt, bx, y, bz, ch);
+        int s = aq_substance(S.nt, A, skip, bx, y, bz, static_cast<double>(d));
+        if (s < 0) s = tbm::kDefaultBlock;
+        out[((y - tbm::kMinY) * 16 + lz) * 16 + lx] = static_cast<uint16_t>(s);
+        if (!(B.M.block_flags[s] & 1)) top = y;
+        for (int q = 0; q < tbm::kNumChannels; ++q) ch[q] += ci.step[q];
+    }
+    if (top != INT_MIN) max32(B.h0 + static_cast<size_t>(c) * 256 + lx * 16 + lz, top + 1);
+}
+
+// ---- BiomeManager zoom -----------------------------------------------------------------------
+TB_HD inline int zoom_biome(const Batch& B, int c, int64_t seed, int x, int y, int z) {
+    const int ax = x - 2, ay = y - 2, az = z - 2;
+    const int px = ax >> 2, py = ay >> 2, pz = az >> 2;
+    const double fx = static_cast<double>(ax & 3) / 4.0, fy = static_cast<double>(ay & 3) / 4.0, fz = static_cast<double>(az & 3) / 4.0;
+    int best = 0;
+    double best_d = 0.0;
+    for (int i = 0; i < 8; ++i) {
+        const bool xe = (i & 4) == 0, ye = (i & 2) == 0, ze = (i & 1) == 0;
+        const int qx = xe ? px : px + 1, qy = ye ? py : py + 1, qz = ze ? pz : pz + 1;
+        const double dx = xe ? fx : fx - 1.0, dy = ye ? fy : fy - 1.0, dz = ze ? fz : fz - 1.0;
+        int64_t r = seed;
+        r = zoom_lcg(r, qx);
+        r = zoom_lcg(r, qy);
+        r = zoom_lcg(r, qz);
+        r = zoom_lcg(r, qx);
+        r = zoom_lcg(r, qy);
+        r = zoom_lcg(r, qz);
+        const double ox = zoom_fiddle(zoom_fiddle_m(r));
+        r = zoom_lcg(r, seed);
+        const double oy = zoom_fiddle(zoom_fiddle_m(r));
+        r = zoom_lcg(r, seed);
+        const double oz = zoom_fiddle(zoom_fiddle_m(r));
+        const double sz = (dz + oz) * (dz + oz), sy = (dy + oy) * (dy + oy), sx = (dx + ox) * (dx + ox);
+        const double d = sz + sy + sx;
+        if (i == 0 || best_d > d) {
+            best = i;
+            best_d = d;
+        }
+    }
+    const int qx = (best & 4) == 0 ? px : px + 1;
+    const int qy = (best & 2) == 0 ? py : py + 1;
+    const int qz = (best & 1) == 0 ? pz : pz + 1;
+    const int dcx = (qx >> 2) - B.cx[c], dcz = (qz >> 2) - B.cz[c];
+    constexpr int qmin = tbm::kMinY >> 2, qh = tbm::kHeight / 4;
+    const int cqy = (qy < qmin ? qmin : (qy > qmin + qh - 1 ? qmin + qh - 1 : qy)) - qmin;
+    const int b = B.nb9[static_cast<size_t>(c) * 9 + (dcz + 1) * 3 + dcx + 1];
+    return B.qbiome[static_cast<size_t>(b) * kQuartsPerChunk + (cqy * 4 + (qz & 3)) * 4 + (qx & 3)];
+}
+
+TB_HD inline float biome_temperature(const DevModel& M, int biome, int x, int y, int z) {
+    float adjusted = M.biome_temp[biome];
+    if (M.biome_frozen[biome]) {
+        float fv = 0.0f;
+        const double freq[3] = {1.0, 0.5, 0.25};
+        for (int i = 0; i < 3; ++i)
+            fv = fv + M.frozen_amp[i] * simplex2(M.frozen[i], static_cast<double>(x) * 0.05 * freq[i], static_cast<double>(z) * 0.05 * freq[i], M.f2, M.g2);
+        const double large = static_cast<double>(fv * 7.0f);
+        const double edge = static_cast<double>(simplex2(M.info, static_cast<double>(x) * 0.2, static_cast<double>(z) * 0.2, M.f2, M.g2));
+        if (large + edge < 0.3) {
+            const double small = static_cast<double>(simplex2(M.info, static_cast<double>(x) * 0.09, static_cast<double>(z) * 0.09, M.f2, M.g2));
+            if (small < 0.8) adjusted = 0.2f;
+        }
+    }
+    constexpr int snow = tbm::kTmSeaLevel + 17;
+    if (y > snow) {
+        const float v = simplex2(M.temp, static_cast<double>(static_cast<float>(x) / 8.0f), static_cast<double>(static_cast<float>(z) / 8.0f), M.f2, M.g2) * 8.0f;
+        float t = v + static_cast<float>(y);
+        t = t - static_cast<float>(snow);
+        t = t * 0.05f;
+        t = t / 40.0f;
+        return adjusted - t;
+    }
+    return adjusted;
+}
+
+// ---- surface: one column ----------------------------------------------------------------------
+struct Column {
+    const Batch* B;
+    const DevSeed* S;
+    uint16_t* blocks;     // chunk blocks
+    int c, lx, lz, bx, bz;
+    int hm;               // live WORLD_SURFACE_WG value of this column (first available y)
+
+    TB_HD TB_FI size_t idx(int y) const { return static_cast<size_t>(((y - tbm::kMinY) * 16 + lz) * 16 + lx); }
+    TB_HD TB_FI int get(int y) const { return (y < tbm::kMinY || y > kMaxY) ? tbm::kAir : blocks[idx(y)]; }
+    TB_HD TB_FI uint8_t flags(int s) const { return B->M.block_flags[s]; }
+    // ProtoChunk.setBlockState plus the heightmap update
+    TB_HD inline void set(int y, int state) {
+        if (y < tbm::kMinY || y > kMaxY) return;
+        blocks[idx(y)] = static_cast<uint16_t>(state);
+        const int first = hm;
+        if (y <= first - 2) return;
+        if (!(flags(state) & 1)) {
+            if (y >= first) hm = y + 1;
+        } else if (first - 1 == y) {
+            for (int yy = y - 1; yy >= tbm::kMinY; --yy)
+                if (!(flags(blocks[idx(yy)]) & 1)) {
+                    hm = yy + 1;
+                    return;
+                }
+            hm = tbm::kMinY;
+        }
+    }
+    template <int K>
+    TB_HD TB_FI double noise(double x, double y, double z) const {
+        constexpr int first = tbm::kNoiseFirst[K], count = tbm::kNoiseCount[K];
+        return static_cast<double>(stack_point<first, count, false>(S->nt, x, y, z));
+    }
+};
+
+TB_HD inline void eroded_badlands(Column& C, int height) {
+    const double a = dabs(C.noise<tbm::kNoise_badlands_surface>(C.bx, 0.0, C.bz) * 8.25);
+    const double b = static_cast<double>(static_cast<float>(C.noise<tbm::kNoise_badlands_pillar>(C.bx * 0.2, 0.0, C.bz * 0.2)) * 15.0f);
+    const double pillar = jmind(a, b);
+    if (pillar <= 0.0) return;
+    const double floor_v = dabs(C.noise<tbm::kNoise_badlands_pillar_roof>(C.bx * 0.75, 0.0, C.bz * 0.75) * 1.5);
+    const double top = 64.0 + jmind(pillar * pillar * 2.5, ::ceil(floor_v * 50.0) + 24.0);
+    const int start = jfloor(top);
+    if (height > start) return;
+    for (int y = start; y >= tbm::kMinY; --y) {
+        const int old = C.get(y);
+        if (old == tbm::kDefaultBlock) break;
+        if (C.flags(old) & 2) return;
+    }
+    for (int y = start; y >= tbm::kMinY && (C.flags(C.get(y)) & 1); --y) C.set(y, tbm::kDefaultBlock);
+}
+
+// Frozen-ocean iceberg extension; with write == false only the heightmap effect is
+// simulated (the rule tree never turns air or fluid into anything else, so the
+// decisions are the same before and after the rules).
+TB_HD inline void frozen_ocean(Column& C, int min_surface, int biome, int height, bool write) {
+    const double a = dabs(C.noise<tbm::kNoise_iceberg_surface>(C.bx, 0.0, C.bz) * 8.25);
+    const double b = static_cast<double>(static_cast<float>(C.noise<tbm::kNoise_iceberg_pillar>(C.bx * 1.28, 0.0, C.bz * 1.28)) * 15.0f);
+    const double berg = jmind(a, b);
+    if (berg <= 1.8) return;
+    const double roof = dabs(C.noise<tbm::kNoise_iceberg_pillar_roof>(C.bx * 1.17, 0.0, C.bz * 1.17) * 1.5);
+    double top = jmind(berg * berg * 1.2, ::ceil(roof * 40.0) + 14.0);
+    constexpr int sea = tbm::kTmSeaLevel;
+    if (biome_temperature(C.B->M, biome, C.bx, sea, C.bz) > 0.1f) top -= 2.0;
+    if (top <= 2.0) return;
+    const double bottom = static_cast<double>(sea) - top - 7.0;
+    top += static_cast<double>(sea);
+    Xoro r = C.S->random.at(C.bx, 0, C.bz);
+    const int max_snow = 2 + r.next_int(4);
+    const int min_snow_height = sea + 18 + r.next_int(10);
+    int snow = 0;
+    const int itop = d2i(top), ibottom = d2i(bottom);
+    const int y0 = height > itop + 1 ? height : itop + 1;
+    for (int y = y0; y >= min_surface; --y) {
+        const int g = C.get(y);
+        bool place = false;
+        if ((C.flags(g) & 1) && y < itop && r.next_double() > 0.01) place = true;
+        else if (g == tbm::kWater && y > ibottom && y < sea && r.next_double() > 0.15) place = true;
+        if (place) {
+            int state;
+            if (snow <= max_snow && y > min_snow_height) {
+                state = tbm::kSnowBlock;
+                ++snow;
+            } else {
+                state = tbm::kPackedIce;
+            }
+            if (write) {
+                C.set(y, state);
+            } else if (y >= tbm::kMinY && y <= kMaxY) {
+                // heightmap effect of set() for a solid state, without writing
+                if (!(y <= C.hm - 2) && y >= C.hm) C.hm = y + 1;
+            }
+        }
+    }
+}
+
+// surface/chunk_surface_level at column (lx, lz): InterpolatedFunction 16x1 over the
+// four chunk-corner find_top_surface values (volume semantics, in the aquifer window).
+TB_HD TB_FI float prelim_surface(const Batch& B, int c, int lx, int lz) {
+    const int32_t* g = B.g513 + static_cast<size_t>(c) * kGrid;
+    const float c00 = B.sfts[g[8 * kGridX + 16]], c10 = B.sfts[g[8 * kGridX + 20]];
+    const float c01 = B.sfts[g[12 * kGridX + 16]], c11 = B.sfts[g[12 * kGridX + 20]];
+    const float az = static_cast<float>(lz) * 0.0625f, ax = static_cast<float>(lx) * 0.0625f;
+    const float v00 = lerpf(az, c00, c01), v01 = lerpf(az, c00, c01);
+    const float v10 = lerpf(az, c10, c11), v11 = lerpf(az, c10, c11);
+    const float a0 = lerpf(ax, v00, v10), a1 = lerpf(ax, v01, v11);
+    const float step = (a1 - a0) * 1.0f;
+    return a0 + step * 0.0f;
+}
+
+// Block context handed to the generated rule tree (MaterialSystem's per-block state).
+struct RuleCtx {
+    Column* col;
+    const Batch* B;
+    int c;
+    // column
+    int surface_depth, grad_x, grad_z;
+    bool sec_set, min_set;
+    double secondary;
+    int min_surf;
+    float prelim;
+    // block
+    int y, stone_above, stone_below, water_height;
+    bool biome_set, ch_set;
+    int biome_v;
+    float ch[tbm::kNumChannels];
+
+    TB_HD TB_FI int biome() {
+        if (!biome_set) {
+            biome_v = zoom_biome(*B, c, col->S->zoom_seed, col->bx, y, col->bz);
+            biome_set = true;
+        }
+        return biome_v;
+    }
+    TB_HD TB_FI double noise2d(int k, int first, int count) const {
+        return static_cast<double>(stack_point_rt(col->S->nt, first, count, col->bx, 0.0, col->bz));
+    }
+    TB_HD TB_FI double noise3d(int k, int first, int count) const {
+        return static_cast<double>(stack_point_rt(col->S->nt, first, count, col->bx, y, col->bz));
+    }
+    TB_HD TB_FI bool vgradient(int k, int true_at, int false_at) const {
+        if (y <= true_at) return true;
+        if (y >= false_at) return false;
+        const double t = (static_cast<double>(y) - true_at) / static_cast<double>(false_at - true_at);
+        const double probability = 1.0 + t * (0.0 - 1.0);
+        Xoro r = col->S->gradient[k].at(col->bx, y, col->bz);
+        return static_cast<double>(r.next_float()) < probability;
+    }
+    TB_HD TB_FI bool cold() { return !(biome_temperature(B->M, biome(), col->bx, y, col->bz) >= 0.15f); }
+    TB_HD TB_FI int min_surface() {
+        if (!min_set) {
+            min_surf = jfloor(static_cast<double>(prelim)) + surface_depth - 8;
+            min_set = true;
+        }
+        return min_surf;
+    }
+    TB_HD TB_FI int secondary_depth(int range) {
+        if (!sec_set) {
+            secondary = col->noise<tbm::kNoise_surface_secondary>(col->bx, 0.0, col->bz);
+            sec_set = true;
+        }
+        const double t = (secondary - -1.0) / (1.0 - -1.0);
+        return d2i(0.0 + t * (static_cast<double>(range) - 0.0));
+    }
+    TB_HD TB_FI int band() const {
+        const int off = jround(static_cast<float>(col->noise<tbm::kNoise_clay_bands_offset>(col->bx, 0.0, col->bz)) * 4.0f);
+        return col->S->clay[(y + off + 192) % 192];
+    }
+    TB_HD inline void channels() {
+        if (ch_set) return;
+        CellInterp ci;
+        const int cell_y = (y - tbm::kMinY) >> 3, yi = (y - tbm::kMinY) & 7;
+        cell_interp(*B, c, col->lx, col->lz, cell_y, ci);
+        for (int k = 0; k < tbm::kNumChannels; ++k) {
+            float v = ci.a0[k];
+            for (int q = 0; q < yi; ++q) v += ci.step[k];
+            ch[k] = v;
+        }
+        ch_set = true;
+    }
+    TB_HD inline int ore_vein(int k, int ore, int raw, int filler, float chance);
+};
+
+// OreVeinRule: density and richness on the volume path, the filler gap on the point path.
+TB_HD inline int RuleCtx::ore_vein(int k, int ore, int raw, int filler, float chance) {
+    channels();
+    const NoiseTables& T = col->S->nt;
+    const float density = tbgen::gen_ore_density(k, T, col->bx, y, col->bz, ch);
+    if (density <= 0.0f) return -1;
+    Xoro r = col->S->ore.at(col->bx, y, col->bz);
+    if (r.next_float() > density) return -1;
+    const float richness = tbgen::gen_ore_richness(k, T, col->bx, y, col->bz, ch);
+    if (r.next_float() < richness && tbgen::gen_ore_gap(k, T, col->bx, y, col->bz) < 0.0f) return r.next_float() < chance ? raw : ore;
+    return filler;
+}
+
+// pass 1 (item = chunk * 256 + x * 16 + z): eroded badlands (writes), heights after it
+// and after a dry run of the frozen-ocean extension
+TB_HD inline void body_surface1(const Batch& B, int it) {
+    const int c = it >> 8, lx = (it >> 4) & 15, lz = it & 15;
+    Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
+             B.h0[it]};
+    const int start_h = C.hm;
+    const int surface_biome = zoom_biome(B, c, C.S->zoom_seed, C.bx, start_h, C.bz);
+    if (surface_biome == tbm::kBiomeErodedBadlands) eroded_badlands(C, start_h);
+    B.h1[it] = C.hm;
+    if (surface_biome == tbm::kBiomeFrozenOcean || surface_biome == tbm::kBiomeDeepFrozenOcean) {
+        const double n = C.noise<tbm::kNoise_surface>(C.bx, 0.0, C.bz);
+        const double rr = C.S->random.at(C.bx, 0, C.bz).next_double();
+        const int sd = d2i(n * 2.75 + 3.0 + rr * 0.25);
+        const int min_surface = jfloor(static_cast<double>(prelim_surface(B, c, lx, lz))) + sd - 8;
+        frozen_ocean(C, min_surface, surface_biome, start_h, false);
+    }
+    B.h2[it] = C.hm;
+}
+
+// pass 2: the rule walk top-down, then the frozen-ocean extension
+TB_HD inline void body_surface2(const Batch& B, int it) {
+    const int c = it >> 8, lx = (it >> 4) & 15, lz = it & 15;
+    const size_t hb = static_cast<size_t>(c) * 256;
+    Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
+             B.h1[it]};
+    const int start_h = B.h0[it];
+    const int surface_biome = zoom_biome(B, c, C.S->zoom_seed, C.bx, start_h, C.bz);
+    // heights of the neighbours as vanilla's x-major, z-minor column order sees them
+    auto H = [&](int x, int z) -> int {
+        if (x == lx && z == lz) return B.h1[hb + x * 16 + z] - 1;
+        const bool done = x < lx || (x == lx && z < lz);
+        return (done ? B.h2[hb + x * 16 + z] : B.h0[hb + x * 16 + z]) - 1;
+    };
+    const int height = C.hm;
+    RuleCtx R{};
+    R.col = &C;
+    R.B = &B;
+    R.c = c;
+    R.grad_x = H(lx + 1 < 15 ? lx + 1 : 15, lz) - H(lx - 1 > 0 ? lx - 1 : 0, lz);
+    R.grad_z = H(lx, lz + 1 < 15 ? lz + 1 : 15) - H(lx, lz - 1 > 0 ? lz - 1 : 0);
+    {
+        const double n = C.noise<tbm::kNoise_surface>(C.bx, 0.0, C.bz);
+        const double rr = C.S->random.at(C.bx, 0, C.bz).next_double();
+        R.surface_depth = d2i(n * 2.75 + 3.0 + rr * 0.25);
+    }
+    R.prelim = prelim_surface(B, c, lx, lz);
+    int stone_above = 0, water_height = INT_MIN, next_ceiling = INT_MAX;
+    for (int y = height; y >= tbm::kMinY; --y) {
+        const int old = C.get(y);
+        const uint8_t f = C.flags(old);
+        if (f & 1) {
+            stone_above = 0;
+            water_height = INT_MIN;
+        } else if (f & 8) {
+            if (water_height == INT_MIN) water_height = y + 1;
+        } else {
+            if (next_ceiling >= y) {
+                next_ceiling = kWayBelowMinY;
+                for (int la = y - 1; la >= tbm::kMinY - 1; --la) {
+                    if (C.flags(C.get(la)) & 9) {
+                        next_ceiling = la + 1;
+                        break;
+                    }
+                }
+            }
+            ++stone_above;
+            R.y = y;
+            R.stone_above = stone_above;
+            R.stone_below = y - next_ceiling + 1;
+            R.water_height = water_height;
+            R.biome_set = false;
+            R.ch_set = false;
+            if (y >= tbm::kMinY && y <= kMaxY) {
+                const int state = tbgen::apply_rules(R);
+                if (state >= 0) C.set(y, state);
+            }
+        }
+    }
+    if (surface_biome == tbm::kBiomeFrozenOcean || surface_biome == tbm::kBiomeDeepFrozenOcean)
+        frozen_ocean(C, R.min_surface(), surface_biome, start_h, true);
+}
+
+// centre chunk's quart biomes to the output (item = chunk * kQuartsPerChunk + q)
+TB_HD inline void body_gather(const Batch& B, int it) {
+    const int c = it / kQuartsPerChunk, q = it % kQuartsPerChunk;
+    B.biomes_out[it] = B.qbiome[static_cast<size_t>(B.nb9[static_cast<size_t>(c) * 9 + 4]) * kQuartsPerChunk + q];
+}
+
+}  // namespace tb

@@ -1,0 +1,240 @@
+// Test-only host build of the TERRAIN-step kernel bodies.
+//
+// Runs the same per-element bodies as the sm_100a kernels (csrc/tb_pipeline.cuh), in
+// the same stage order, sequentially on the CPU, so the CPU test suite can compare the
+// generated evaluators and every pipeline stage with the reference oracle without a
+// GPU. It is a checker of the device code's arithmetic, not a product path: the
+// product library (libterrain_b200.so) has no host fallback and never loads this file.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "tb_pipeline.cuh"
+
+using namespace tb;
+
+namespace {
+
+struct HostRun {
+    ModelHost m;
+    SeedHost s;
+    DevModel M{};
+    DevSeed D{};
+    std::vector<uint8_t> flags;
+    std::vector<float> btemp;
+    std::vector<uint8_t> bfrozen;
+
+    explicit HostRun(int64_t seed) {
+        build_model_host(m);
+        build_seed_host(seed, s);
+        flags.assign(tbm::kBlockFlags, tbm::kBlockFlags + tbm::kPaletteSize);
+        btemp.assign(tbm::kBiomeTemp, tbm::kBiomeTemp + tbm::kNumBiomes);
+        bfrozen.assign(tbm::kBiomeFrozen, tbm::kBiomeFrozen + tbm::kNumBiomes);
+        M.tree = m.nodes.data();
+        M.children = m.children.data();
+        M.leaf_biome = m.leaf_biome.data();
+        M.leaf_node = m.leaf_node.data();
+        M.leaf_rank = m.leaf_rank.data();
+        M.root = m.root;
+        M.block_flags = flags.data();
+        M.biome_temp = btemp.data();
+        M.biome_frozen = bfrozen.data();
+        M.temp = m.temp;
+        for (int i = 0; i < 3; ++i) {
+            M.frozen[i] = m.frozen[i];
+            M.frozen_amp[i] = m.frozen_amp[i];
+        }
+        M.info = m.info;
+        M.f2 = m.f2;
+        M.g2 = m.g2;
+        D.nt = NoiseTables{s.off.data(), s.perm.data(), s.layers.data()};
+        D.random = s.random;
+        D.aquifer = s.aquifer;
+        D.ore = s.ore;
+        for (size_t k = 0; k < s.gradient.size(); ++k) D.gradient[k] = s.gradient[k];
+        D.zoom_seed = s.zoom_seed;
+        std::memcpy(D.clay, s.clay, sizeof D.clay);
+    }
+};
+
+struct Table {
+    std::vector<unsigned long long> keys, uniq;
+    std::vector<int32_t> vals;
+    int32_t count = 0;
+    uint32_t cap = 0;
+    void init(size_t max_keys) {
+        cap = 1024;
+        while (cap < 2 * max_keys) cap <<= 1;
+        keys.assign(cap, kEmpty);
+        vals.assign(cap, -1);
+        uniq.assign(max_keys, 0);
+        count = 0;
+    }
+    HashTab view() { return HashTab{keys.data(), vals.data(), uniq.data(), &count, cap - 1}; }
+};
+
+template <class F>
+void each(int n, F f) {
+    for (int i = 0; i < n; ++i) f(i);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Full pipeline for n chunks of one seed. blocks: n * 16 * 16 * height u16; biomes: n * 1536 u8
+// (may be null); aquifer: blocks after the fill (may be null).
+int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, uint16_t* blocks, uint8_t* biomes, uint16_t* aquifer) {
+    HostRun R(seed);
+    std::vector<int32_t> vcx(cx, cx + n), vcz(cz, cz + n), vcs(n, 0);
+    Table hb, hc, hs;
+    hb.init(9 * static_cast<size_t>(n));
+    hc.init(25 * static_cast<size_t>(n));
+    hs.init(static_cast<size_t>(kGrid) * n);
+    const size_t N = n, nb = 9 * N, cc = 25 * N, sg = kGrid * N;
+    std::vector<int32_t> nb9(9 * N), c25(25 * N), g513(sg), aq_loc(N * kAqCells * 3), aq_status(N * kAqCells * 2), aq_skip(N);
+    std::vector<float> bcol(nb * 16 * tbm::kClimateCols), ccol(cc * tbm::kCornerCols), corners(cc * kRows * tbm::kNumChannels), sfts(sg);
+    std::vector<long long> tgt(nb * kQuartsPerChunk * 6), mdist(nb * kQuartsPerChunk);
+    std::vector<int32_t> lstar(nb * kQuartsPerChunk), h0(256 * N, tbm::kMinY), h1(256 * N), h2(256 * N);
+    std::vector<uint8_t> qbiome(nb * kQuartsPerChunk), bout(N * kQuartsPerChunk);
+    std::vector<uint16_t> bl(N * kBlocksPerChunk);
+    Batch B{};
+    B.M = R.M;
+    B.seeds = &R.D;
+    B.n = n;
+    B.cx = vcx.data();
+    B.cz = vcz.data();
+    B.cseed = vcs.data();
+    B.hb = hb.view();
+    B.nb_cap = static_cast<int32_t>(nb);
+    B.nb9 = nb9.data();
+    B.bcol = bcol.data();
+    B.tgt = tgt.data();
+    B.lstar = lstar.data();
+    B.mdist = mdist.data();
+    B.qbiome = qbiome.data();
+    B.hc = hc.view();
+    B.cc_cap = static_cast<int32_t>(cc);
+    B.c25 = c25.data();
+    B.ccol = ccol.data();
+    B.corners = corners.data();
+    B.hs = hs.view();
+    B.sg_cap = static_cast<int32_t>(sg);
+    B.g513 = g513.data();
+    B.sfts = sfts.data();
+    B.aq_loc = aq_loc.data();
+    B.aq_status = aq_status.data();
+    B.aq_skip = aq_skip.data();
+    B.blocks = bl.data();
+    B.h0 = h0.data();
+    B.h1 = h1.data();
+    B.h2 = h2.data();
+    B.biomes_out = bout.data();
+    each(9 * n, [&](int i) { body_nb_insert(B, i); });
+    each(9 * n, [&](int i) { body_nb_resolve(B, i); });
+    each(hb.count * 16, [&](int i) { body_climate_col(B, i); });
+    each(hb.count * 16 * kRuns, [&](int i) { body_climate_quart(B, i); });
+    each(hb.count, [&](int i) { body_chain(B, i); });
+    each(25 * n, [&](int i) { body_cc_insert(B, i); });
+    each(25 * n, [&](int i) { body_cc_resolve(B, i); });
+    each(hc.count, [&](int i) { body_corner_col(B, i); });
+    each(hc.count * kRows, [&](int i) { body_corner(B, i); });
+    each(kGrid * n, [&](int i) { body_sg_insert(B, i); });
+    each(kGrid * n, [&](int i) { body_sg_resolve(B, i); });
+    each(hs.count, [&](int i) { body_surface_level(B, i); });
+    each(kAqCells * n, [&](int i) { body_aquifer_cell(B, i); });
+    each(n, [&](int i) { body_aquifer_skip(B, i); });
+    each(256 * kCellsY * n, [&](int i) { body_fill(B, i); });
+    if (aquifer) std::memcpy(aquifer, bl.data(), sizeof(uint16_t) * bl.size());
+    each(256 * n, [&](int i) { body_surface1(B, i); });
+    each(256 * n, [&](int i) { body_surface2(B, i); });
+    each(kQuartsPerChunk * n, [&](int i) { body_gather(B, i); });
+    std::memcpy(blocks, bl.data(), sizeof(uint16_t) * bl.size());
+    if (biomes) std::memcpy(biomes, bout.data(), bout.size());
+    return 0;
+}
+
+// Point-path root values at positions (root: 0 barrier, 1 floodedness, 2 spread, 3 lava,
+// 4 exclusion, 5 find_top_surface density, 6 fts volume (x, z), 7 fts point (x, z)).
+int hc_point(int64_t seed, int32_t root, const int32_t* xyz, int32_t n, float* out) {
+    HostRun R(seed);
+    const NoiseTables& T = R.D.nt;
+    for (int i = 0; i < n; ++i) {
+        const int x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+        float v = 0.0f;
+        switch (root) {
+            case 0: v = tbgen::gen_aq_barrier(T, x, y, z); break;
+            case 1: v = tbgen::gen_aq_fluid_level_floodedness(T, x, y, z); break;
+            case 2: v = tbgen::gen_aq_fluid_level_spread(T, x, y, z); break;
+            case 3: v = tbgen::gen_aq_lava(T, x, y, z); break;
+            case 4: v = tbgen::gen_aq_exclusion(T, x, y, z); break;
+            case 5: v = tbgen::gen_fts_density(T, x, y, z); break;
+            case 6: v = tbgen::gen_fts_vol(T, x, z); break;
+            case 7: v = tbgen::gen_fts_pt(T, x, z); break;
+            default: return -1;
+        }
+        out[i] = v;
+    }
+    return 0;
+}
+
+// Climate roots (volume path) at quart positions: out 6 floats per position.
+int hc_climate(int64_t seed, const int32_t* xyz, int32_t n, float* out) {
+    HostRun R(seed);
+    float col[tbm::kClimateCols];
+    for (int i = 0; i < n; ++i) {
+        tbgen::gen_climate_col(R.D.nt, xyz[3 * i], xyz[3 * i + 2], col);
+        tbgen::gen_climate(R.D.nt, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], col, out + 6 * i);
+    }
+    return 0;
+}
+
+// Interpolation-channel inputs (volume path) at cell-corner positions: kNumChannels floats each.
+int hc_corners(int64_t seed, const int32_t* xyz, int32_t n, float* out) {
+    HostRun R(seed);
+    float col[tbm::kCornerCols];
+    for (int i = 0; i < n; ++i) {
+        tbgen::gen_corner_col(R.D.nt, xyz[3 * i], xyz[3 * i + 2], col);
+        tbgen::gen_corner(R.D.nt, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], col, out + tbm::kNumChannels * i);
+    }
+    return 0;
+}
+
+int hc_num_channels() { return tbm::kNumChannels; }
+
+// Per-seed host scalars: zoom seed, positional factories (random, aquifer, ore), clay bands.
+int hc_seed_scalars(int64_t seed, int64_t* out7, int32_t* clay) {
+    SeedHost s;
+    build_seed_host(seed, s);
+    out7[0] = s.zoom_seed;
+    out7[1] = static_cast<int64_t>(s.random.lo);
+    out7[2] = static_cast<int64_t>(s.random.hi);
+    out7[3] = static_cast<int64_t>(s.aquifer.lo);
+    out7[4] = static_cast<int64_t>(s.aquifer.hi);
+    out7[5] = static_cast<int64_t>(s.ore.lo);
+    out7[6] = static_cast<int64_t>(s.ore.hi);
+    for (int i = 0; i < 192; ++i) clay[i] = s.clay[i];
+    return 0;
+}
+
+// Layers of one noise key index: frequency, amplitude, offsets, permutations.
+int hc_noise_layers(int64_t seed, int32_t key, double* freq, float* amp, double* offs, uint8_t* perms) {
+    SeedHost s;
+    build_seed_host(seed, s);
+    const int first = tbm::kNoiseFirst[key], count = tbm::kNoiseCount[key];
+    for (int i = 0; i < count; ++i) {
+        const Layer& L = s.layers[first + i];
+        freq[i] = L.freq;
+        amp[i] = L.amp;
+        offs[3 * i] = s.off[L.oct].ox;
+        offs[3 * i + 1] = s.off[L.oct].oy;
+        offs[3 * i + 2] = s.off[L.oct].oz;
+        std::memcpy(perms + 256 * i, s.perm.data() + 256 * L.oct, 256);
+    }
+    return count;
+}
+
+void hc_md5(const uint8_t* d, int64_t n, uint8_t* out) { md5(d, static_cast<size_t>(n), out); }
+void hc_sha256(const uint8_t* d, int64_t n, uint8_t* out) { sha256(d, static_cast<size_t>(n), out); }
+
+}  // extern "C"
