@@ -1,0 +1,300 @@
+"""Benchmark of the overworld TERRAIN step on B200 (one JSON line on rank 0).
+
+Workload (the reference's ladder size): one seed, three 64x64-chunk regions of 4,096
+chunks each -- at the origin, at block -1,000,000 (chunk -62,500) and touching the
++1,874,999-block border (chunk 117,187 is the region's last chunk). A step is the full
+TERRAIN step over all 12,288 chunks: biomes, density with caves, aquifers, ore veins and
+material rules, u16 block states and u8 quart biomes out.
+
+  value      chunks/s with the chunk lists already in HBM and the outputs left in HBM
+             (tg_generate_device), device time from CUDA events on the launching stream
+  e2e        chunks/s through tg_generate with host buffers: the chunk list is copied
+             in and every block/biome byte copied out to pinned memory inside the step
+  roofline   the dominant stage's output bytes (198,144 B per chunk: u16 blocks + u8
+             biomes) over its device time, against the measured HBM copy peak
+  cpu_baseline  the reference's own C++ port (oracle/_ref) on this host's cores, on a
+             bounded sample of the same regions
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, 'minecraft-terrain-cuda_b200'))
+sys.path.insert(0, os.path.join(REPO, 'oracle'))
+
+SEED = 0x5445525241494E31   # "TERRAIN1"
+REGIONS = [('origin', 0, 0), ('negative', -62500, -62500), ('border', 117124, 117124)]
+SIDE = 64
+BYTES_PER_CHUNK = 98304 * 2 + 1536
+METRIC = 'bit-exact TERRAIN chunks/s on 1 B200 (plain form, ladder size: one seed, three 64x64-chunk regions)'
+
+
+def region_chunks(x0, z0, side=SIDE):
+    return np.array([(x0 + x, z0 + z) for z in range(side) for x in range(side)], np.int32)
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+        return float(p['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        cmd = ['nvidia-smi', '-i', str(self.index), '--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+               'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+               'clocks_event_reasons.sw_power_cap', '--format=csv,noheader,nounits', '-lms', '100']
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for l in self.lines:
+            f = [x.strip() for x in l.split(',')]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == 'active':
+                    reasons.add(n)
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def cpu_baseline(threads=None, sample_side=8):
+    """The reference C++ port on this host: an 8x8-chunk square of each region."""
+    import ref_oracle
+    if not ref_oracle.available():
+        return None
+    m = ref_oracle.RefModel()
+    s = m.seed(SEED)
+    threads = threads or os.cpu_count()
+    chunks = np.concatenate([region_chunks(x0, z0, sample_side) for _, x0, z0 in REGIONS])
+    s.generate(chunks[:threads], threads=threads)   # warm the caches / page in
+    t0 = time.perf_counter()
+    s.generate(chunks, threads=threads)
+    dt = time.perf_counter() - t0
+    return {'value': round(len(chunks) / dt, 2), 'unit': 'chunks/s', 'cores': threads, 'kind': 'reference',
+            'sample': '%d chunks: an %dx%d square at the corner of each of the three regions, region form (biomes of the '
+                      'square plus a 1-chunk border, then fill + surface per chunk), %d threads' % (len(chunks), sample_side, sample_side, threads)}
+
+
+def run_reference(args, rank):
+    """Reference arm: the reference's own C++ port (oracle/_ref) on the host cores."""
+    if rank != 0:
+        return
+    import ref_oracle
+    if not ref_oracle.available():
+        print(json.dumps({'impl': 'reference', 'unavailable': 'oracle/_ref not built (the reference C++ port compiles only where its sources are)'}))
+        return
+    m = ref_oracle.RefModel()
+    s = m.seed(SEED)
+    threads = os.cpu_count()
+    per_step = 96   # bounded sample per step: a 4x8 block of chunks from each region
+    rng_sets = []
+    for k in range(args.warmup + args.steps):
+        sets = []
+        for _, x0, z0 in REGIONS:
+            ox, oz = (k * 8) % SIDE, (k * 4) % SIDE
+            sets.append(np.array([(x0 + ox + x, z0 + oz + z) for z in range(4) for x in range(8)], np.int32))
+        rng_sets.append(np.concatenate(sets))
+    for k in range(args.warmup):
+        s.generate(rng_sets[k], threads=threads)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        s.generate(rng_sets[args.warmup + k], threads=threads)
+    dt = time.perf_counter() - t0
+    v = per_step * args.steps / dt
+    line = {'metric': METRIC, 'value': round(v, 2), 'unit': 'chunks/s', 'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': round(1000 * dt / args.steps, 3), 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32+f64+int',
+            'data': 'synthetic world model (project-authored, reference JSON formats); seeded chunk lists', 'impl': 'reference',
+            'config': {'workload': 'ladder: one seed, three 64x64-chunk regions (origin, -1,000,000 blocks, +1,874,999-block border)',
+                       'per_step_sample': '%d chunks (4x8 per region), the reference C++ port, %d host threads' % (per_step, threads)},
+            'cpu_baseline': {'value': round(v, 2), 'unit': 'chunks/s', 'cores': threads, 'kind': 'reference',
+                             'sample': '%d chunks per step, 4x8 per region' % per_step},
+            'e2e': {'value': round(v, 2), 'unit': 'chunks/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import terrain_b200
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    g = terrain_b200.TerrainGenerator(max_batch_chunks=SIDE * SIDE, device=dev)
+    stream = torch.cuda.current_stream()
+    g.set_stream(stream.cuda_stream)
+    g.set_seed(SEED)
+    nreg = len(REGIONS)
+    host_chunks = [region_chunks(x0, z0) for _, x0, z0 in REGIONS]
+    d_chunks = [torch.from_numpy(c).cuda() for c in host_chunks]
+    n = SIDE * SIDE
+    d_blocks = [torch.empty(n * 98304, dtype=torch.int16, device='cuda') for _ in range(nreg)]
+    d_biomes = [torch.empty(n * 1536, dtype=torch.uint8, device='cuda') for _ in range(nreg)]
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def step_device(stats=None):
+        for r in range(nreg):
+            t = g.generate_device(d_chunks[r].data_ptr(), n, d_blocks[r].data_ptr(), d_biomes[r].data_ptr())
+            if stats is not None:
+                stats.append(t)
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    stats = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step_device(stats)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    barrier()
+    torch.cuda.synchronize()
+    ms_max = ms
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    chunks_total = n * nreg * args.steps * world
+    value = chunks_total / (ms_max / 1000.0)
+
+    # end to end through the host API: pinned host outputs, copies inside the step
+    pin_blocks = [torch.empty(n * 98304, dtype=torch.int16, pin_memory=True) for _ in range(nreg)]
+    pin_biomes = [torch.empty(n * 1536, dtype=torch.uint8, pin_memory=True) for _ in range(nreg)]
+    np_blocks = [b.numpy().view(np.uint16).reshape(n, -1, 16, 16) for b in pin_blocks]
+    np_biomes = [b.numpy().reshape(n, -1) for b in pin_biomes]
+
+    def step_e2e():
+        for r in range(nreg):
+            g.generate(host_chunks[r], blocks_out=np_blocks[r], biomes_out=np_biomes[r])
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        step_e2e()
+    torch.cuda.synchronize()
+    barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        step_e2e()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms_e2e], device='cuda')
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = chunks_total / (ms_e2e / 1000.0)
+
+    if rank != 0:
+        return
+    stage = {k: sum(t[k] for t in stats) for k in ('biome_ms', 'noise_ms', 'aquifer_ms', 'fill_ms', 'surface_ms', 'kernel_ms')}
+    launches = sum(t['launches'] for t in stats)
+    dom = max(('biome_ms', 'noise_ms', 'aquifer_ms', 'fill_ms', 'surface_ms'), key=lambda k: stage[k])
+    calls = len(stats)
+    per_launch_ms = stage[dom] / calls
+    algo_bytes = BYTES_PER_CHUNK * n
+    achieved = algo_bytes / (per_launch_ms / 1000.0) / 1e9
+    peak, peak_kind = peaks()
+    line = {
+        'metric': METRIC, 'value': round(value, 1), 'unit': 'chunks/s', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': round(ms_max / args.steps, 3), 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32+f64+int',
+        'data': 'synthetic world model (project-authored, reference JSON formats); seeded chunk lists',
+        'config': {'workload': 'ladder: one seed, three 64x64-chunk regions (origin, -1,000,000 blocks, +1,874,999-block border), 12,288 chunks per step',
+                   'seed': SEED, 'chunks_per_step': n * nreg, 'batch_chunks': n, 'l2': 'outputs (2.4 GB per step) larger than L2',
+                   'parallelism': 'replicas: each GPU runs the full workload' if world > 1 else 'single GPU'},
+        'stage_ms_per_step': {k: round(v / args.steps, 3) for k, v in stage.items()},
+        'roofline': {'bound': 'hbm', 'kernel': dom.replace('_ms', ''), 'achieved': round(achieved, 2), 'peak': peak, 'unit': 'GB/s',
+                     'frac': round(achieved / peak, 5), 'traffic': None, 'peak_source': peak_kind,
+                     'note': 'algorithmic bytes = 198,144 B per chunk (u16 blocks + u8 biomes) x 4,096 chunks per launch; the stages are '
+                             'FP32/FP64/INT pipe bound, so the HBM fraction is small by design'},
+        'e2e': {'value': round(e2e_value, 1), 'unit': 'chunks/s', 'h2d_bytes_per_step': int(n * nreg * 8),
+                'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK)},
+        'gpu_launches': int(launches),
+        'clocks': clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        line['cpu_baseline'] = cpu_baseline()
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local_rank = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'reference':
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

@@ -53,6 +53,7 @@ typedef struct tg_config {
 typedef struct tg_timing {
     float h2d_ms, biome_ms, noise_ms, aquifer_ms, fill_ms, surface_ms, d2h_ms, kernel_ms, wall_ms;
     int32_t batches;
+    int32_t launches; /* kernels launched by the call */
 } tg_timing;
 
 /* Creates a generator for the model compiled into the library. ir_json_path and
@@ -63,6 +64,11 @@ tg_status tg_create(const char* ir_json_path, const char* terrain_json_path, con
 
 /* reference: ~FullTerrainGenerator */
 tg_status tg_destroy(struct tg_generator* gen);
+
+/* Runs the generator's work on the caller's CUDA stream (a cudaStream_t; NULL restores
+ * the generator's own stream). Calls still return only when their work is done.
+ * No counterpart in the reference (its streams are internal). */
+tg_status tg_set_stream(struct tg_generator* gen, void* cuda_stream);
 
 /* Builds the per-seed noise tables, random factories and zoom seed on the host and
  * uploads them. reference: FullTerrainGenerator::set_seed (cuda/src/terrain.cu:1387, :1176-1255) */

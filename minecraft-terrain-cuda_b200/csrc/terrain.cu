@@ -79,6 +79,7 @@ __global__ void k_biome_lookup(const __grid_constant__ Batch B, const int32_t* x
 }
 
 int g_sm_count = 148;
+thread_local int g_launches = 0;
 
 template <typename K, typename... Args>
 void launch(K kernel, cudaStream_t s, int items_hint, Args... args) {
@@ -87,6 +88,7 @@ void launch(K kernel, cudaStream_t s, int items_hint, Args... args) {
     const long cap = static_cast<long>(g_sm_count) * 8;
     blocks = std::max(1L, std::min(blocks, cap));
     kernel<<<static_cast<unsigned>(blocks), threads, 0, s>>>(args...);
+    ++g_launches;
 }
 
 uint32_t pow2_at_least(uint64_t v) {
@@ -149,7 +151,8 @@ struct SeedSlot {
 struct Generator {
     int device = 0;
     int max_batch = 2048;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // the stream all work runs on
+    cudaStream_t own_stream = nullptr;
     cudaEvent_t ev[8] = {};
     // model
     DevBuf d_tree, d_children, d_leaf_biome, d_leaf_node, d_leaf_rank, d_flags, d_btemp, d_bfrozen;
@@ -173,7 +176,8 @@ struct Generator {
         cudaDeviceProp prop{};
         ck(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
         g_sm_count = prop.multiProcessorCount;
-        ck(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        stream = own_stream;
         for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
         // generated evaluators and the rule tree use deep inlined frames
         ck(cudaDeviceSetLimit(cudaLimitStackSize, 16384), "cudaDeviceSetLimit");
@@ -188,7 +192,7 @@ struct Generator {
         if (h_chunks) cudaFreeHost(h_chunks);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
-        if (stream) cudaStreamDestroy(stream);
+        if (own_stream) cudaStreamDestroy(own_stream);
     }
 
     template <class T>
@@ -397,6 +401,7 @@ struct Generator {
             t->surface_ms += ms[4];
             t->kernel_ms += ms[0] + ms[1] + ms[2] + ms[3] + ms[4];
             t->batches += 1;
+            t->launches = g_launches;
         }
     }
 
@@ -587,6 +592,13 @@ tg_status tg_destroy(tg_generator* gen) {
     return tb::guarded([&] { delete gen; });
 }
 
+tg_status tg_set_stream(tg_generator* gen, void* cuda_stream) {
+    return tb::guarded([&] {
+        if (!gen) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "gen is null");
+        gen->g->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : gen->g->own_stream;
+    });
+}
+
 tg_status tg_set_seed(tg_generator* gen, int64_t seed) {
     return tb::guarded([&] {
         if (!gen) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "gen is null");
@@ -602,7 +614,9 @@ tg_status tg_generate(tg_generator* gen, const tg_chunk_xz* chunks, int32_t coun
         tb::ck(cudaSetDevice(gen->g->device), "cudaSetDevice");
         const auto t0 = std::chrono::steady_clock::now();
         if (timing) std::memset(timing, 0, sizeof *timing);
+        tb::g_launches = 0;
         gen->g->generate(chunks, count, blocks_out, biomes_out, aquifer_out, timing);
+        if (timing) timing->launches = tb::g_launches;
         if (timing) timing->wall_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     });
 }
@@ -612,7 +626,9 @@ tg_status tg_generate_device(tg_generator* gen, const tg_chunk_xz* chunks_dev, i
         if (!gen || count <= 0 || !chunks_dev || !blocks_dev) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
         tb::ck(cudaSetDevice(gen->g->device), "cudaSetDevice");
         if (timing) std::memset(timing, 0, sizeof *timing);
+        tb::g_launches = 0;
         gen->g->generate_device(chunks_dev, count, blocks_dev, biomes_dev, timing);
+        if (timing) timing->launches = tb::g_launches;
     });
 }
 
@@ -622,7 +638,9 @@ tg_status tg_generate_batch(tg_generator* gen, const tg_request* requests, int32
         tb::ck(cudaSetDevice(gen->g->device), "cudaSetDevice");
         const auto t0 = std::chrono::steady_clock::now();
         if (timing) std::memset(timing, 0, sizeof *timing);
+        tb::g_launches = 0;
         gen->g->generate_batch(requests, n, timing);
+        if (timing) timing->launches = tb::g_launches;
         if (timing) timing->wall_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
     });
 }

@@ -1,0 +1,177 @@
+"""Python binding of the C ABI in include/terrain_b200.h (ctypes, no torch types).
+
+    g = TerrainGenerator()                 # loads lib/libterrain_b200.so, device 0
+    g.set_seed(123456789)
+    blocks, biomes = g.generate([(0, 0), (1, 0)])   # numpy u16 (n, height, 16, 16), u8 (n, 1536)
+
+The library must have been built (python build.py); a missing library raises, there is
+no fallback path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'lib', 'libterrain_b200.so')
+
+STATUS = {0: 'TG_OK', 1: 'TG_ERR_INVALID_ARGUMENT', 2: 'TG_ERR_MODEL_MISMATCH', 3: 'TG_ERR_CUDA', 4: 'TG_ERR_OUT_OF_MEMORY', 5: 'TG_ERR_RANGE',
+          6: 'TG_ERR_NO_SEED', 7: 'TG_ERR_DEVICE_TIMEOUT', 8: 'TG_ERR_INTERNAL'}
+
+
+class TgChunk(ctypes.Structure):
+    _fields_ = [('x', ctypes.c_int32), ('z', ctypes.c_int32)]
+
+
+class TgConfig(ctypes.Structure):
+    _fields_ = [('max_batch_chunks', ctypes.c_int32), ('pipeline_slots', ctypes.c_int32), ('device', ctypes.c_int32)]
+
+
+class TgTiming(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_float) for k in ('h2d_ms', 'biome_ms', 'noise_ms', 'aquifer_ms', 'fill_ms', 'surface_ms', 'd2h_ms', 'kernel_ms',
+                                               'wall_ms')] + [('batches', ctypes.c_int32), ('launches', ctypes.c_int32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TgRequest(ctypes.Structure):
+    _fields_ = [('seed', ctypes.c_int64), ('chunks', ctypes.POINTER(TgChunk)), ('count', ctypes.c_int32),
+                ('blocks_out', ctypes.POINTER(ctypes.c_uint16)), ('biomes_out', ctypes.POINTER(ctypes.c_uint8))]
+
+
+EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+           'tg_alloc_pinned', 'tg_free_pinned', 'tg_model_info', 'tg_last_error_string']
+
+
+class TerrainError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__('%s: %s' % (STATUS.get(status, status), msg))
+        self.status = status
+
+
+_lib = None
+
+
+def load(path=LIB_PATH):
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError('terrain_b200 library not built: %s (run python minecraft-terrain-cuda_b200/build.py)' % path)
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    L.tg_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(TgConfig), ctypes.POINTER(vp)]
+    L.tg_destroy.argtypes = [vp]
+    L.tg_set_seed.argtypes = [vp, ctypes.c_int64]
+    L.tg_set_stream.argtypes = [vp, vp]
+    L.tg_generate.argtypes = [vp, ctypes.POINTER(TgChunk), ctypes.c_int32, vp, vp, vp, ctypes.POINTER(TgTiming)]
+    L.tg_generate_device.argtypes = [vp, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(TgTiming)]
+    L.tg_generate_batch.argtypes = [vp, ctypes.POINTER(TgRequest), ctypes.c_int32, ctypes.POINTER(TgTiming)]
+    L.tg_biome_lookup.argtypes = [vp, vp, vp, ctypes.c_int32, vp]
+    L.tg_alloc_pinned.argtypes = [ctypes.c_size_t]
+    L.tg_alloc_pinned.restype = vp
+    L.tg_free_pinned.argtypes = [vp]
+    L.tg_model_info.argtypes = [ctypes.POINTER(ctypes.c_int32)] * 5
+    L.tg_last_error_string.restype = ctypes.c_char_p
+    for f in ('tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+              'tg_model_info'):
+        getattr(L, f).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def model_info():
+    L = load()
+    v = [ctypes.c_int32() for _ in range(5)]
+    L.tg_model_info(*[ctypes.byref(x) for x in v])
+    return dict(zip(('min_y', 'height', 'sea_level', 'palette_size', 'biome_count'), [x.value for x in v]))
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def chunk_array(chunks):
+    a = np.ascontiguousarray(np.asarray(chunks, dtype=np.int32).reshape(-1, 2))
+    return a
+
+
+class TerrainGenerator:
+    def __init__(self, max_batch_chunks=2048, device=0, ir_path=None, terrain_path=None, pipeline_slots=2):
+        self.L = load()
+        self.h = ctypes.c_void_p()
+        cfg = TgConfig(max_batch_chunks, pipeline_slots, device)
+        self._check(self.L.tg_create(ir_path.encode() if ir_path else None, terrain_path.encode() if terrain_path else None, ctypes.byref(cfg),
+                                     ctypes.byref(self.h)))
+        info = model_info()
+        self.height = info['height']
+        self.min_y = info['min_y']
+        self.per = 256 * self.height
+        self.qper = 16 * (self.height // 4)
+
+    def _check(self, st):
+        if st != 0:
+            raise TerrainError(st, self.L.tg_last_error_string().decode())
+
+    def close(self):
+        if self.h:
+            self.L.tg_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_handle):
+        """cudaStream_t as an int (e.g. torch.cuda.current_stream().cuda_stream); 0 = own stream."""
+        self._check(self.L.tg_set_stream(self.h, ctypes.c_void_p(stream_handle) if stream_handle else None))
+
+    def set_seed(self, seed):
+        self._check(self.L.tg_set_seed(self.h, int(seed)))
+
+    def generate(self, chunks, blocks_out=None, biomes_out=None, aquifer=False, timing=False):
+        a = chunk_array(chunks)
+        n = a.shape[0]
+        blocks = blocks_out if blocks_out is not None else np.empty((n, self.height, 16, 16), np.uint16)
+        biomes = biomes_out if biomes_out is not None else np.empty((n, self.qper), np.uint8)
+        aq = np.empty((n, self.height, 16, 16), np.uint16) if aquifer else None
+        t = TgTiming()
+        self._check(self.L.tg_generate(self.h, a.ctypes.data_as(ctypes.POINTER(TgChunk)), n, _ptr(blocks), _ptr(biomes), _ptr(aq), ctypes.byref(t)))
+        out = (blocks, biomes) + ((aq,) if aquifer else ())
+        return out + (t.as_dict(),) if timing else out
+
+    def generate_device(self, chunks_ptr, count, blocks_ptr, biomes_ptr=None):
+        """Device pointers (ints); returns the stage timing dict."""
+        t = TgTiming()
+        self._check(self.L.tg_generate_device(self.h, ctypes.c_void_p(chunks_ptr), count, ctypes.c_void_p(blocks_ptr),
+                                              ctypes.c_void_p(biomes_ptr) if biomes_ptr else None, ctypes.byref(t)))
+        return t.as_dict()
+
+    def generate_batch(self, requests, timing=False):
+        """requests: list of (seed, chunks). Returns list of (blocks, biomes)."""
+        outs, keep, reqs = [], [], (TgRequest * max(1, len(requests)))()
+        for i, (seed, chunks) in enumerate(requests):
+            a = chunk_array(chunks)
+            n = a.shape[0]
+            b = np.empty((n, self.height, 16, 16), np.uint16)
+            bi = np.empty((n, self.qper), np.uint8)
+            keep.append(a)
+            outs.append((b, bi))
+            reqs[i].seed = int(seed)
+            reqs[i].chunks = a.ctypes.data_as(ctypes.POINTER(TgChunk))
+            reqs[i].count = n
+            reqs[i].blocks_out = b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))
+            reqs[i].biomes_out = bi.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        t = TgTiming()
+        self._check(self.L.tg_generate_batch(self.h, reqs, len(requests), ctypes.byref(t)))
+        return (outs, t.as_dict()) if timing else outs
+
+    def biome_lookup(self, seeds, xyz):
+        xyz = np.ascontiguousarray(np.asarray(xyz, np.int32).reshape(-1, 3))
+        seeds = np.ascontiguousarray(np.broadcast_to(np.asarray(seeds, np.int64), (xyz.shape[0],)))
+        out = np.empty(xyz.shape[0], np.uint8)
+        self._check(self.L.tg_biome_lookup(self.h, _ptr(seeds), _ptr(xyz), xyz.shape[0], _ptr(out)))
+        return out
