@@ -275,12 +275,22 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--profile-small', action='store_true',
+                    help='one untimed step over a 16x16-chunk corner of each region (a small case for ncu captures)')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local_rank = int(os.environ.get('LOCAL_RANK', '0'))
     if args.impl == 'reference':
         run_reference(args, rank)
+        return
+    if args.profile_small:
+        import terrain_b200
+        g = terrain_b200.TerrainGenerator(max_batch_chunks=256)
+        g.set_seed(SEED)
+        for _, x0, z0 in REGIONS:
+            g.generate(region_chunks(x0, z0, 16))
+        g.close()
         return
     if world > 1:
         import datetime

@@ -22,6 +22,8 @@ NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 DEVICE_FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-O3', '-std=c++17', '-lineinfo', '-fmad=false', '-prec-div=true',
                 '-prec-sqrt=true', '-ftz=false']
 HOST_FLAGS = ['-Xcompiler', '-fPIC,-ffp-contract=off,-O2,-fno-fast-math']
+if os.environ.get('TB_PTXAS_VERBOSE'):
+    DEVICE_FLAGS.append('-Xptxas=-v')
 
 
 def run(cmd):

@@ -172,44 +172,71 @@ TB_HD TB_FI float octave_point_smeared(const NoiseTables& T, int32_t oct, double
     return cell_point(cell_hash(T.perm + 256 * oct, fx, fy, fz), rx, fudged, rz, static_cast<float>(rel));
 }
 
-// NoiseStack.addToVolume for one sample starting from acc = 0.
-template <int FIRST, int COUNT, bool SMEARED>
-TB_HD TB_FI float stack_volume(const NoiseTables& T, int32_t bx, int32_t by, int32_t bz, double xzs, double yss, float amplitude) {
+// NoiseStack.addToVolume / NoiseStack.get over a run of layers. One out-of-line copy
+// per variant serves every noise of the evaluators, so the octave code stays resident
+// in the instruction cache; the layer loop is not unrolled for the same reason.
+#if defined(__CUDA_ARCH__)
+#define TB_NOINLINE __noinline__
+#else
+#define TB_NOINLINE
+#endif
+
+TB_HD TB_NOINLINE inline float stack_volume_rt(const NoiseTables& T, int first, int count, int32_t bx, int32_t by, int32_t bz, double xzs, double yss,
+                                                float amplitude) {
     float acc = 0.0f;
-#pragma unroll
-    for (int i = 0; i < COUNT; ++i) {
-        const Layer L = T.layer[FIRST + i];
+#pragma unroll 1
+    for (int i = first; i < first + count; ++i) {
+        const Layer L = T.layer[i];
         const double xs = xzs * L.freq, ys = yss * L.freq;
         const float amp = amplitude * L.amp;
-        const float v = SMEARED ? octave_volume_smeared(T, L.oct, bx, by, bz, xs, ys) : octave_volume(T, L.oct, bx, by, bz, xs, ys);
-        acc = acc + amp * v;
+        acc = acc + amp * octave_volume(T, L.oct, bx, by, bz, xs, ys);
     }
     return acc;
 }
 
-// NoiseStack.get (plain or smeared octaves).
-template <int FIRST, int COUNT, bool SMEARED>
-TB_HD TB_FI float stack_point(const NoiseTables& T, double x, double y, double z) {
+TB_HD TB_NOINLINE inline float stack_volume_smeared_rt(const NoiseTables& T, int first, int count, int32_t bx, int32_t by, int32_t bz, double xzs,
+                                                        double yss, float amplitude) {
     float acc = 0.0f;
-#pragma unroll
-    for (int i = 0; i < COUNT; ++i) {
-        const Layer L = T.layer[FIRST + i];
-        const double f = L.freq;
-        const float n = SMEARED ? octave_point_smeared(T, L.oct, x * f, y * f, z * f) : octave_point(T, L.oct, x * f, y * f, z * f);
-        acc = acc + L.amp * n;
+#pragma unroll 1
+    for (int i = first; i < first + count; ++i) {
+        const Layer L = T.layer[i];
+        const double xs = xzs * L.freq, ys = yss * L.freq;
+        const float amp = amplitude * L.amp;
+        acc = acc + amp * octave_volume_smeared(T, L.oct, bx, by, bz, xs, ys);
     }
     return acc;
 }
 
-// Run-time layer range variant (used by the material system's named noises).
-TB_HD inline float stack_point_rt(const NoiseTables& T, int first, int count, double x, double y, double z) {
+TB_HD TB_NOINLINE inline float stack_point_rt(const NoiseTables& T, int first, int count, double x, double y, double z) {
     float acc = 0.0f;
-    for (int i = 0; i < count; ++i) {
-        const Layer L = T.layer[first + i];
+#pragma unroll 1
+    for (int i = first; i < first + count; ++i) {
+        const Layer L = T.layer[i];
         const double f = L.freq;
         acc = acc + L.amp * octave_point(T, L.oct, x * f, y * f, z * f);
     }
     return acc;
+}
+
+TB_HD TB_NOINLINE inline float stack_point_smeared_rt(const NoiseTables& T, int first, int count, double x, double y, double z) {
+    float acc = 0.0f;
+#pragma unroll 1
+    for (int i = first; i < first + count; ++i) {
+        const Layer L = T.layer[i];
+        const double f = L.freq;
+        acc = acc + L.amp * octave_point_smeared(T, L.oct, x * f, y * f, z * f);
+    }
+    return acc;
+}
+
+template <int FIRST, int COUNT, bool SMEARED>
+TB_HD TB_FI float stack_volume(const NoiseTables& T, int32_t bx, int32_t by, int32_t bz, double xzs, double yss, float amplitude) {
+    return SMEARED ? stack_volume_smeared_rt(T, FIRST, COUNT, bx, by, bz, xzs, yss, amplitude) : stack_volume_rt(T, FIRST, COUNT, bx, by, bz, xzs, yss, amplitude);
+}
+
+template <int FIRST, int COUNT, bool SMEARED>
+TB_HD TB_FI float stack_point(const NoiseTables& T, double x, double y, double z) {
+    return SMEARED ? stack_point_smeared_rt(T, FIRST, COUNT, x, y, z) : stack_point_rt(T, FIRST, COUNT, x, y, z);
 }
 
 // ---- legacy 2-D simplex (SimplexNoise with zero offsets) -----------------------------

@@ -31,6 +31,12 @@ constexpr int kAqMinGridY = -7;
 constexpr int kWayBelowMinY = -2032 * 16;   // DimensionType.WAY_BELOW_MIN_Y
 constexpr int kMaxGradientRandoms = 8;
 constexpr int kSearchStack = 16;
+// quart vertices a chunk's BiomeManager lookups can reach: x and z from 4c - 1 to 4c + 4,
+// y from ((min_y - 2) >> 2) to ((max_y + 1 - 2) >> 2) + 1
+constexpr int kZoomQyMin = (tbm::kMinY - 2) >> 2;
+constexpr int kZoomQyMax = ((tbm::kMinY + tbm::kHeight - 2) >> 2) + 1;
+constexpr int kZoomY = kZoomQyMax - kZoomQyMin + 1;
+constexpr int kZoomVerts = 36 * kZoomY;
 static_assert(tbm::kNumGradientRandoms <= kMaxGradientRandoms, "too many vertical-gradient random names");
 static_assert(tbm::kHeight % 16 == 0 && tbm::kMinY % 16 == 0, "world height must be section aligned");
 
@@ -107,6 +113,7 @@ struct Batch {
     int32_t* h1;                      // after the eroded-badlands extension
     int32_t* h2;                      // after the frozen-ocean extension (dry run)
     uint8_t* biomes_out;              // n * kQuartsPerChunk
+    uint32_t* zoom_tab;               // n * kZoomVerts packed fiddle draws per quart vertex
 };
 
 // ---- atomics (device) / plain operations (host test build) --------------------------------------
@@ -336,13 +343,16 @@ TB_HD inline void body_corner_col(const Batch& B, int u) {
     unpack_key(B.hc.uniq[u], slot, qx, qz, sem);
     tbgen::gen_corner_col(B.seeds[slot].nt, qx * 4, qz * 4, B.ccol + static_cast<size_t>(u) * tbm::kCornerCols);
 }
+// item = row * count + column: a warp evaluates one corner row over neighbouring
+// columns, where the lazy branches (surface, caves, blended-noise limits) agree most.
 TB_HD inline void body_corner(const Batch& B, int it) {
-    const int u = it / kRows, row = it % kRows;
-    if (u >= *B.hc.count) return;
+    const int cnt = *B.hc.count;
+    const int u = it % cnt, row = it / cnt;
+    if (row >= kRows) return;
     int32_t slot, qx, qz, sem;
     unpack_key(B.hc.uniq[u], slot, qx, qz, sem);
     tbgen::gen_corner(B.seeds[slot].nt, qx * 4, tbm::kMinY + 8 * row, qz * 4, B.ccol + static_cast<size_t>(u) * tbm::kCornerCols,
-                      B.corners + static_cast<size_t>(it) * tbm::kNumChannels);
+                      B.corners + (static_cast<size_t>(u) * kRows + row) * tbm::kNumChannels);
 }
 
 // ---- surface levels and aquifer cells ---------------------------------------------------------------
@@ -629,8 +639,30 @@ TB_HD inline void body_fill(const Batch& B, int it) {
     if (top != INT_MIN) max32(B.h0 + static_cast<size_t>(c) * 256 + lx * 16 + lz, top + 1);
 }
 
-// ---- BiomeManager zoom -----------------------------------------------------------------------
-TB_HD inline int zoom_biome(const Batch& B, int c, int64_t seed, int x, int y, int z) {
+// ---- BiomeManager zoom ---------------------------------------------------------------------
+// The three fiddle draws of quart vertex (qx, qy, qz): the LCG chain of
+// BiomeManager.getFiddledDistance (cpu/src/biome.cpp:255-268), as floorMod(r >> 24, 1024)
+// each, packed in 10-bit fields.
+TB_HD TB_FI uint32_t zoom_fiddles(int64_t seed, int qx, int qy, int qz) {
+    int64_t r = seed;
+    r = zoom_lcg(r, qx);
+    r = zoom_lcg(r, qy);
+    r = zoom_lcg(r, qz);
+    r = zoom_lcg(r, qx);
+    r = zoom_lcg(r, qy);
+    r = zoom_lcg(r, qz);
+    const uint32_t mx = static_cast<uint32_t>(zoom_fiddle_m(r));
+    r = zoom_lcg(r, seed);
+    const uint32_t my = static_cast<uint32_t>(zoom_fiddle_m(r));
+    r = zoom_lcg(r, seed);
+    const uint32_t mz = static_cast<uint32_t>(zoom_fiddle_m(r));
+    return mx | (my << 10) | (mz << 20);
+}
+
+// BiomeManager.getBiome: the quart whose fiddled corner is nearest (first on ties), then
+// its stored biome from the chunk's 3x3 neighbourhood (qy clamped to the world).
+template <class Fiddles>
+TB_HD TB_FI int zoom_pick(const Batch& B, int c, int x, int y, int z, Fiddles fid) {
     const int ax = x - 2, ay = y - 2, az = z - 2;
     const int px = ax >> 2, py = ay >> 2, pz = az >> 2;
     const double fx = static_cast<double>(ax & 3) / 4.0, fy = static_cast<double>(ay & 3) / 4.0, fz = static_cast<double>(az & 3) / 4.0;
@@ -638,20 +670,11 @@ TB_HD inline int zoom_biome(const Batch& B, int c, int64_t seed, int x, int y, i
     double best_d = 0.0;
     for (int i = 0; i < 8; ++i) {
         const bool xe = (i & 4) == 0, ye = (i & 2) == 0, ze = (i & 1) == 0;
-        const int qx = xe ? px : px + 1, qy = ye ? py : py + 1, qz = ze ? pz : pz + 1;
+        const uint32_t m = fid(xe ? px : px + 1, ye ? py : py + 1, ze ? pz : pz + 1);
+        const double ox = zoom_fiddle(static_cast<int32_t>(m & 1023u));
+        const double oy = zoom_fiddle(static_cast<int32_t>((m >> 10) & 1023u));
+        const double oz = zoom_fiddle(static_cast<int32_t>(m >> 20));
         const double dx = xe ? fx : fx - 1.0, dy = ye ? fy : fy - 1.0, dz = ze ? fz : fz - 1.0;
-        int64_t r = seed;
-        r = zoom_lcg(r, qx);
-        r = zoom_lcg(r, qy);
-        r = zoom_lcg(r, qz);
-        r = zoom_lcg(r, qx);
-        r = zoom_lcg(r, qy);
-        r = zoom_lcg(r, qz);
-        const double ox = zoom_fiddle(zoom_fiddle_m(r));
-        r = zoom_lcg(r, seed);
-        const double oy = zoom_fiddle(zoom_fiddle_m(r));
-        r = zoom_lcg(r, seed);
-        const double oz = zoom_fiddle(zoom_fiddle_m(r));
         const double sz = (dz + oz) * (dz + oz), sy = (dy + oy) * (dy + oy), sx = (dx + ox) * (dx + ox);
         const double d = sz + sy + sx;
         if (i == 0 || best_d > d) {
@@ -667,6 +690,25 @@ TB_HD inline int zoom_biome(const Batch& B, int c, int64_t seed, int x, int y, i
     const int cqy = (qy < qmin ? qmin : (qy > qmin + qh - 1 ? qmin + qh - 1 : qy)) - qmin;
     const int b = B.nb9[static_cast<size_t>(c) * 9 + (dcz + 1) * 3 + dcx + 1];
     return B.qbiome[static_cast<size_t>(b) * kQuartsPerChunk + (cqy * 4 + (qz & 3)) * 4 + (qx & 3)];
+}
+
+// any position (biome lookups): the LCG chains computed in place
+TB_HD inline int zoom_biome(const Batch& B, int c, int64_t seed, int x, int y, int z) {
+    return zoom_pick(B, c, x, y, z, [&](int qx, int qy, int qz) { return zoom_fiddles(seed, qx, qy, qz); });
+}
+
+// blocks of chunk c (and its surface height): the chunk's precomputed vertex table
+TB_HD inline int zoom_biome_tab(const Batch& B, int c, int x, int y, int z) {
+    const uint32_t* tab = B.zoom_tab + static_cast<size_t>(c) * kZoomVerts;
+    const int qx0 = B.cx[c] * 4 - 1, qz0 = B.cz[c] * 4 - 1;
+    return zoom_pick(B, c, x, y, z, [&](int qx, int qy, int qz) { return tab[((qy - kZoomQyMin) * 6 + (qz - qz0)) * 6 + (qx - qx0)]; });
+}
+
+// item = chunk * kZoomVerts + vertex
+TB_HD inline void body_zoom_table(const Batch& B, int it) {
+    const int c = it / kZoomVerts, v = it % kZoomVerts;
+    const int qx = B.cx[c] * 4 - 1 + v % 6, qz = B.cz[c] * 4 - 1 + (v / 6) % 6, qy = kZoomQyMin + v / 36;
+    B.zoom_tab[it] = zoom_fiddles(B.seeds[B.cseed[c]].zoom_seed, qx, qy, qz);
 }
 
 TB_HD inline float biome_temperature(const DevModel& M, int biome, int x, int y, int z) {
@@ -824,7 +866,7 @@ struct RuleCtx {
 
     TB_HD TB_FI int biome() {
         if (!biome_set) {
-            biome_v = zoom_biome(*B, c, col->S->zoom_seed, col->bx, y, col->bz);
+            biome_v = zoom_biome_tab(*B, c, col->bx, y, col->bz);
             biome_set = true;
         }
         return biome_v;
@@ -898,7 +940,7 @@ TB_HD inline void body_surface1(const Batch& B, int it) {
     Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
              B.h0[it]};
     const int start_h = C.hm;
-    const int surface_biome = zoom_biome(B, c, C.S->zoom_seed, C.bx, start_h, C.bz);
+    const int surface_biome = zoom_biome_tab(B, c, C.bx, start_h, C.bz);
     if (surface_biome == tbm::kBiomeErodedBadlands) eroded_badlands(C, start_h);
     B.h1[it] = C.hm;
     if (surface_biome == tbm::kBiomeFrozenOcean || surface_biome == tbm::kBiomeDeepFrozenOcean) {
@@ -918,7 +960,7 @@ TB_HD inline void body_surface2(const Batch& B, int it) {
     Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
              B.h1[it]};
     const int start_h = B.h0[it];
-    const int surface_biome = zoom_biome(B, c, C.S->zoom_seed, C.bx, start_h, C.bz);
+    const int surface_biome = zoom_biome_tab(B, c, C.bx, start_h, C.bz);
     // heights of the neighbours as vanilla's x-major, z-minor column order sees them
     auto H = [&](int x, int z) -> int {
         if (x == lx && z == lz) return B.h1[hb + x * 16 + z] - 1;

@@ -166,7 +166,7 @@ struct Generator {
     int current_slot = -1;
     // batch buffers
     DevBuf d_chunks, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_loc,
-        d_aq_status, d_aq_skip, d_blocks, d_h0, d_h1, d_h2, d_biomes, d_aqcopy;
+        d_aq_status, d_aq_skip, d_blocks, d_h0, d_h1, d_h2, d_biomes, d_aqcopy, d_zoom;
     TableBufs tb_b, tb_c, tb_s;
     // pinned staging
     tg_chunk_xz* h_chunks = nullptr;
@@ -265,6 +265,7 @@ struct Generator {
         d_h1.alloc(4 * 256 * N);
         d_h2.alloc(4 * 256 * N);
         d_biomes.alloc(N * kQuartsPerChunk);
+        d_zoom.alloc(sizeof(uint32_t) * N * kZoomVerts);
     }
 
     // Resident per-seed tables: returns the slot, building and uploading on a miss.
@@ -342,6 +343,7 @@ struct Generator {
         B.h1 = d_h1.as<int32_t>();
         B.h2 = d_h2.as<int32_t>();
         B.biomes_out = d_biomes.as<uint8_t>();
+        B.zoom_tab = d_zoom.as<uint32_t>();
         return B;
     }
 
@@ -371,6 +373,7 @@ struct Generator {
         launch(k_items<body_cc_resolve>, s, 25 * n, B, 25 * n);
         launch(k_dyn<body_corner_col, 1>, s, 16 * n, B, cnt_c);
         launch(k_dyn<body_corner, kRows>, s, 16 * n * kRows, B, cnt_c);
+        launch(k_items<body_zoom_table>, s, kZoomVerts * n, B, kZoomVerts * n);
         ck(cudaEventRecord(ev[2], s), "event");
         // aquifer stage
         tb_s.reset(s);

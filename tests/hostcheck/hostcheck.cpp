@@ -98,6 +98,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     std::vector<int32_t> lstar(nb * kQuartsPerChunk), h0(256 * N, tbm::kMinY), h1(256 * N), h2(256 * N);
     std::vector<uint8_t> qbiome(nb * kQuartsPerChunk), bout(N * kQuartsPerChunk);
     std::vector<uint16_t> bl(N * kBlocksPerChunk);
+    std::vector<uint32_t> ztab(N * kZoomVerts);
     Batch B{};
     B.M = R.M;
     B.seeds = &R.D;
@@ -130,6 +131,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     B.h1 = h1.data();
     B.h2 = h2.data();
     B.biomes_out = bout.data();
+    B.zoom_tab = ztab.data();
     each(9 * n, [&](int i) { body_nb_insert(B, i); });
     each(9 * n, [&](int i) { body_nb_resolve(B, i); });
     each(hb.count * 16, [&](int i) { body_climate_col(B, i); });
@@ -139,6 +141,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     each(25 * n, [&](int i) { body_cc_resolve(B, i); });
     each(hc.count, [&](int i) { body_corner_col(B, i); });
     each(hc.count * kRows, [&](int i) { body_corner(B, i); });
+    each(kZoomVerts * n, [&](int i) { body_zoom_table(B, i); });
     each(kGrid * n, [&](int i) { body_sg_insert(B, i); });
     each(kGrid * n, [&](int i) { body_sg_resolve(B, i); });
     each(hs.count, [&](int i) { body_surface_level(B, i); });
