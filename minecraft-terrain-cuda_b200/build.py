@@ -49,15 +49,16 @@ def sources():
     return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(GEN, 'model_gen.cuh')]
 
 
-def build_device(force=False):
+def build_device(force=False, out=None, defines=()):
     os.makedirs(LIB, exist_ok=True)
-    out = os.path.join(LIB, 'libterrain_b200.so')
+    out = out or os.path.join(LIB, 'libterrain_b200.so')
     if not force and not newer(out, sources()):
         return out
     objs = []
+    tag = os.path.splitext(os.path.basename(out))[0]
     for src in ('terrain.cu', 'tb_host.cpp'):
-        obj = os.path.join(LIB, src + '.o')
-        run([NVCC] + DEVICE_FLAGS + HOST_FLAGS + ['-I', CSRC, '-I', GEN, '-c', os.path.join(CSRC, src), '-o', obj])
+        obj = os.path.join(os.path.dirname(out), '%s.%s.o' % (tag, src))
+        run([NVCC] + DEVICE_FLAGS + HOST_FLAGS + ['-D%s' % d for d in defines] + ['-I', CSRC, '-I', GEN, '-c', os.path.join(CSRC, src), '-o', obj])
         objs.append(obj)
     run([NVCC, '-shared', '-gencode', 'arch=compute_100a,code=sm_100a', '-o', out] + objs + ['-lcudart'])
     return out

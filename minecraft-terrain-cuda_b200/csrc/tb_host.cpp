@@ -91,7 +91,8 @@ void sha256(const uint8_t* data, size_t len, uint8_t out[32]) {
             return static_cast<uint32_t>(static_cast<uint64_t>(std::floor(f * 4294967296.0L)));
         };
         for (int i = 0; i < 64; ++i) {
-            // exact integer cube root correction on top of the long double estimate
+            // long double cube root: 61 fraction bits, far more than the 32 kept; the MD5 /
+            // SHA-256 known-answer tests pin every constant
             long double r = std::cbrt(static_cast<long double>(primes[i]));
             K[i] = frac32(r);
         }
@@ -496,8 +497,10 @@ void build_model_host(ModelHost& m) {
         if (r.leaf >= 0) m.leaf_node[r.leaf] = static_cast<int32_t>(i);
     }
     int rank = 0;
+    std::vector<char> reachable(m.nodes.size(), 0);
     std::function<int(int, int)> dfs = [&](int node, int depth) -> int {
         m.depth = std::max(m.depth, depth);
+        reachable[node] = 1;
         RNode& r = m.nodes[node];
         r.rank = rank;
         if (r.leaf >= 0) {
@@ -509,6 +512,28 @@ void build_model_host(ModelHost& m) {
     };
     dfs(m.root, 1);
     if (rank != tbm::kNumParams) throw std::runtime_error("climate tree does not cover every parameter box");
+    // (nodes the build made only to order its buckets are not part of the tree)
+    bool fits = true;
+    for (size_t i = 0; i < m.nodes.size(); ++i) {
+        if (!reachable[i]) continue;
+        const RNode& r = m.nodes[i];
+        if (r.child_count >= 32) fits = false;
+        for (int d = 0; d < 7; ++d)
+            if (r.mn[d] > r.mx[d] || r.mn[d] < -kBox32Limit || r.mx[d] > kBox32Limit) fits = false;
+    }
+    if (fits) {
+        m.boxes.resize(m.nodes.size());
+        for (size_t i = 0; i < m.nodes.size(); ++i) {
+            const RNode& r = m.nodes[i];
+            RBox& b = m.boxes[i];
+            for (int d = 0; d < 7; ++d) {
+                b.mn[d] = static_cast<int32_t>(r.mn[d]);
+                b.mx[d] = static_cast<int32_t>(r.mx[d]);
+            }
+            b.info = !reachable[i] ? 0 : (r.leaf >= 0 ? ~r.leaf : ((r.first_child << 5) | r.child_count));
+            b.rank = r.rank;
+        }
+    }
     // biome temperature simplex noises
     Lcg r1(1234);
     m.temp = make_simplex(r1);

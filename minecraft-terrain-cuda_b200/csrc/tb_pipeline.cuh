@@ -42,6 +42,7 @@ static_assert(tbm::kHeight % 16 == 0 && tbm::kMinY % 16 == 0, "world height must
 
 // ---- device-resident model and per-seed tables -------------------------------------------------
 struct DevModel {
+    const RBox* boxes;              // null when the 32-bit search does not apply
     const RNode* tree;
     const int32_t* children;
     const int32_t* leaf_biome;
@@ -114,7 +115,17 @@ struct Batch {
     int32_t* h2;                      // after the frozen-ocean extension (dry run)
     uint8_t* biomes_out;              // n * kQuartsPerChunk
     uint32_t* zoom_tab;               // n * kZoomVerts packed fiddle draws per quart vertex
+    uint32_t* walk;                   // n * kBlocksPerChunk packed column-walk state per block
+    struct ColumnRec* colrec;         // n * 256 per-column surface context
 };
+
+// Per-column context of the material rules (MaterialSystem column state).
+struct ColumnRec {
+    double secondary;                 // surface_secondary noise at (x, 0, z)
+    int32_t surface_depth, min_surface, grad_x, grad_z;
+    int32_t surface_biome, start_h;
+};
+constexpr uint32_t kNoWalk = 0xFFFFFFFFu;
 
 // ---- atomics (device) / plain operations (host test build) --------------------------------------
 TB_HD TB_FI unsigned long long cas64(unsigned long long* p, unsigned long long cmp, unsigned long long val) {
@@ -288,14 +299,70 @@ TB_HD inline int tree_first_min(const DevModel& M, const long long* t, int start
     return best;
 }
 
+// 32-bit form of the same search (exact: every bound and target is within +/-2^29, so
+// no difference overflows and each squared term fits 60 bits).
+TB_HD TB_FI long long box_dist32(const RBox& n, const int32_t* t) {
+    long long d = 0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        const int32_t tv = i < 6 ? t[i] : 0;
+        int32_t p = tv - n.mx[i];
+        const int32_t q = n.mn[i] - tv;
+        p = p > q ? p : q;
+        p = p > 0 ? p : 0;
+        d += static_cast<long long>(static_cast<unsigned long long>(static_cast<uint32_t>(p)) * static_cast<uint32_t>(p));
+    }
+    return d;
+}
+
+TB_HD inline int tree_first_min32(const DevModel& M, const int32_t* t, int start_leaf, long long& best_d) {
+    int best = start_leaf;
+    int best_rank = M.leaf_rank[start_leaf];
+    best_d = box_dist32(M.boxes[M.leaf_node[start_leaf]], t);
+    int stack_node[kSearchStack], stack_next[kSearchStack];
+    int sp = 1;
+    stack_node[0] = M.root;
+    stack_next[0] = 0;
+    while (sp > 0) {
+        const int info = M.boxes[stack_node[sp - 1]].info;
+        const int k = stack_next[sp - 1];
+        if (k >= (info & 31)) {
+            --sp;
+            continue;
+        }
+        stack_next[sp - 1] = k + 1;
+        const int ci = M.children[(info >> 5) + k];
+        const RBox ch = M.boxes[ci];
+        const long long d = box_dist32(ch, t);
+        if (d < best_d || (d == best_d && ch.rank < best_rank)) {
+            if (ch.info < 0) {
+                best = ~ch.info;
+                best_rank = ch.rank;
+                best_d = d;
+            } else if (sp < kSearchStack) {
+                stack_node[sp] = ci;
+                stack_next[sp] = 0;
+                ++sp;
+            }
+        }
+    }
+    return best;
+}
+
 // One quart column run: climate per quart, quantized targets, first minimal leaf.
-// item = (biome chunk * 16 + column) * kRuns + run; a run is kRun consecutive quarts in y.
-constexpr int kRun = 8;
+// item = run * (biome chunks * 16) + biome chunk * 16 + column; a run is kRun
+// consecutive quarts in y. A warp holds 32 neighbouring columns at the same heights,
+// whose targets (and so tree paths) are alike.
+#ifndef TB_QUART_RUN
+#define TB_QUART_RUN 16
+#endif
+constexpr int kRun = TB_QUART_RUN;
 constexpr int kRuns = (tbm::kHeight / 4) / kRun;
 static_assert((tbm::kHeight / 4) % kRun == 0, "quart run must divide the quart height");
 TB_HD inline void body_climate_quart(const Batch& B, int it) {
-    const int run = it % kRuns, cidx = it / kRuns, b = cidx / 16, col = cidx % 16;
-    if (b >= *B.hb.count) return;
+    const int ncol = *B.hb.count * 16;
+    const int run = it / ncol, cidx = it % ncol, b = cidx / 16, col = cidx % 16;
+    if (run >= kRuns) return;
     int32_t slot, bx, bz, sem;
     unpack_key(B.hb.uniq[b], slot, bx, bz, sem);
     const DevSeed& S = B.seeds[slot];
@@ -310,7 +377,13 @@ TB_HD inline void body_climate_quart(const Batch& B, int it) {
         long long t[6];
         for (int k = 0; k < 6; ++k) t[k] = f2l(cl[k] * 10000.0f);
         long long md;
-        const int leaf = tree_first_min(B.M, t, prev, md);
+        bool small = B.M.boxes != nullptr;
+        int32_t t32[6];
+        for (int k = 0; k < 6; ++k) {
+            small = small && t[k] >= -kBox32Limit && t[k] <= kBox32Limit;
+            t32[k] = static_cast<int32_t>(t[k]);
+        }
+        const int leaf = small ? tree_first_min32(B.M, t32, prev, md) : tree_first_min(B.M, t, prev, md);
         prev = leaf;
         const size_t p = static_cast<size_t>(b) * kQuartsPerChunk + chain_pos(qx, qy, qz);
         for (int k = 0; k < 6; ++k) B.tgt[p * 6 + k] = t[k];
@@ -698,7 +771,7 @@ TB_HD inline int zoom_biome(const Batch& B, int c, int64_t seed, int x, int y, i
 }
 
 // blocks of chunk c (and its surface height): the chunk's precomputed vertex table
-TB_HD inline int zoom_biome_tab(const Batch& B, int c, int x, int y, int z) {
+TB_HD TB_NOINLINE inline int zoom_biome_tab(const Batch& B, int c, int x, int y, int z) {
     const uint32_t* tab = B.zoom_tab + static_cast<size_t>(c) * kZoomVerts;
     const int qx0 = B.cx[c] * 4 - 1, qz0 = B.cz[c] * 4 - 1;
     return zoom_pick(B, c, x, y, z, [&](int qx, int qy, int qz) { return tab[((qy - kZoomQyMin) * 6 + (qz - qz0)) * 6 + (qx - qx0)]; });
@@ -711,7 +784,7 @@ TB_HD inline void body_zoom_table(const Batch& B, int it) {
     B.zoom_tab[it] = zoom_fiddles(B.seeds[B.cseed[c]].zoom_seed, qx, qy, qz);
 }
 
-TB_HD inline float biome_temperature(const DevModel& M, int biome, int x, int y, int z) {
+TB_HD TB_NOINLINE inline float biome_temperature(const DevModel& M, int biome, int x, int y, int z) {
     float adjusted = M.biome_temp[biome];
     if (M.biome_frozen[biome]) {
         float fv = 0.0f;
@@ -905,7 +978,7 @@ struct RuleCtx {
         const int off = jround(static_cast<float>(col->noise<tbm::kNoise_clay_bands_offset>(col->bx, 0.0, col->bz)) * 4.0f);
         return col->S->clay[(y + off + 192) % 192];
     }
-    TB_HD inline void channels() {
+    TB_HD TB_NOINLINE void channels() {
         if (ch_set) return;
         CellInterp ci;
         const int cell_y = (y - tbm::kMinY) >> 3, yi = (y - tbm::kMinY) & 7;
@@ -917,11 +990,11 @@ struct RuleCtx {
         }
         ch_set = true;
     }
-    TB_HD inline int ore_vein(int k, int ore, int raw, int filler, float chance);
+    TB_HD TB_NOINLINE int ore_vein(int k, int ore, int raw, int filler, float chance);
 };
 
 // OreVeinRule: density and richness on the volume path, the filler gap on the point path.
-TB_HD inline int RuleCtx::ore_vein(int k, int ore, int raw, int filler, float chance) {
+TB_HD TB_NOINLINE int RuleCtx::ore_vein(int k, int ore, int raw, int filler, float chance) {
     channels();
     const NoiseTables& T = col->S->nt;
     const float density = tbgen::gen_ore_density(k, T, col->bx, y, col->bz, ch);
@@ -933,16 +1006,17 @@ TB_HD inline int RuleCtx::ore_vein(int k, int ore, int raw, int filler, float ch
     return filler;
 }
 
-// pass 1 (item = chunk * 256 + x * 16 + z): eroded badlands (writes), heights after it
+// pass 1 (item = chunk * 256 + z * 16 + x): eroded badlands (writes), heights after it
 // and after a dry run of the frozen-ocean extension
 TB_HD inline void body_surface1(const Batch& B, int it) {
-    const int c = it >> 8, lx = (it >> 4) & 15, lz = it & 15;
+    const int c = it >> 8, lz = (it >> 4) & 15, lx = it & 15;
+    const int ci = (c << 8) | (lx << 4) | lz;   // x * 16 + z column index
     Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
-             B.h0[it]};
+             B.h0[ci]};
     const int start_h = C.hm;
     const int surface_biome = zoom_biome_tab(B, c, C.bx, start_h, C.bz);
     if (surface_biome == tbm::kBiomeErodedBadlands) eroded_badlands(C, start_h);
-    B.h1[it] = C.hm;
+    B.h1[ci] = C.hm;
     if (surface_biome == tbm::kBiomeFrozenOcean || surface_biome == tbm::kBiomeDeepFrozenOcean) {
         const double n = C.noise<tbm::kNoise_surface>(C.bx, 0.0, C.bz);
         const double rr = C.S->random.at(C.bx, 0, C.bz).next_double();
@@ -950,40 +1024,43 @@ TB_HD inline void body_surface1(const Batch& B, int it) {
         const int min_surface = jfloor(static_cast<double>(prelim_surface(B, c, lx, lz))) + sd - 8;
         frozen_ocean(C, min_surface, surface_biome, start_h, false);
     }
-    B.h2[it] = C.hm;
+    B.h2[ci] = C.hm;
 }
 
-// pass 2: the rule walk top-down, then the frozen-ocean extension
-TB_HD inline void body_surface2(const Batch& B, int it) {
-    const int c = it >> 8, lx = (it >> 4) & 15, lz = it & 15;
+// pass 2a (item = chunk * 256 + z * 16 + x): the column context and the top-down walk
+// state of every solid block (stone above, stone below, water height), packed per block.
+// The rule tree reads no block other than its own and never turns a block into air or a
+// fluid, so these states are those the sequential walk sees.
+TB_HD inline void body_surface_walk(const Batch& B, int it) {
+    const int c = it >> 8, lz = (it >> 4) & 15, lx = it & 15;
+    const int ci = (c << 8) | (lx << 4) | lz;   // x * 16 + z column index
     const size_t hb = static_cast<size_t>(c) * 256;
     Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
-             B.h1[it]};
-    const int start_h = B.h0[it];
-    const int surface_biome = zoom_biome_tab(B, c, C.bx, start_h, C.bz);
+             B.h1[ci]};
     // heights of the neighbours as vanilla's x-major, z-minor column order sees them
     auto H = [&](int x, int z) -> int {
         if (x == lx && z == lz) return B.h1[hb + x * 16 + z] - 1;
         const bool done = x < lx || (x == lx && z < lz);
         return (done ? B.h2[hb + x * 16 + z] : B.h0[hb + x * 16 + z]) - 1;
     };
+    ColumnRec r;
+    r.start_h = B.h0[ci];
+    r.surface_biome = zoom_biome_tab(B, c, C.bx, r.start_h, C.bz);
+    r.grad_x = H(lx + 1 < 15 ? lx + 1 : 15, lz) - H(lx - 1 > 0 ? lx - 1 : 0, lz);
+    r.grad_z = H(lx, lz + 1 < 15 ? lz + 1 : 15) - H(lx, lz - 1 > 0 ? lz - 1 : 0);
+    const double n = C.noise<tbm::kNoise_surface>(C.bx, 0.0, C.bz);
+    const double rr = C.S->random.at(C.bx, 0, C.bz).next_double();
+    r.surface_depth = d2i(n * 2.75 + 3.0 + rr * 0.25);
+    r.min_surface = jfloor(static_cast<double>(prelim_surface(B, c, lx, lz))) + r.surface_depth - 8;
+    r.secondary = C.noise<tbm::kNoise_surface_secondary>(C.bx, 0.0, C.bz);
+    B.colrec[ci] = r;
+    uint32_t* walk = B.walk + static_cast<size_t>(c) * kBlocksPerChunk;
     const int height = C.hm;
-    RuleCtx R{};
-    R.col = &C;
-    R.B = &B;
-    R.c = c;
-    R.grad_x = H(lx + 1 < 15 ? lx + 1 : 15, lz) - H(lx - 1 > 0 ? lx - 1 : 0, lz);
-    R.grad_z = H(lx, lz + 1 < 15 ? lz + 1 : 15) - H(lx, lz - 1 > 0 ? lz - 1 : 0);
-    {
-        const double n = C.noise<tbm::kNoise_surface>(C.bx, 0.0, C.bz);
-        const double rr = C.S->random.at(C.bx, 0, C.bz).next_double();
-        R.surface_depth = d2i(n * 2.75 + 3.0 + rr * 0.25);
-    }
-    R.prelim = prelim_surface(B, c, lx, lz);
+    for (int y = kMaxY; y > height && y >= tbm::kMinY; --y) walk[C.idx(y)] = kNoWalk;
     int stone_above = 0, water_height = INT_MIN, next_ceiling = INT_MAX;
-    for (int y = height; y >= tbm::kMinY; --y) {
-        const int old = C.get(y);
-        const uint8_t f = C.flags(old);
+    for (int y = height > kMaxY ? kMaxY : height; y >= tbm::kMinY; --y) {
+        const uint8_t f = C.flags(C.get(y));
+        uint32_t w = kNoWalk;
         if (f & 1) {
             stone_above = 0;
             water_height = INT_MIN;
@@ -1000,20 +1077,54 @@ TB_HD inline void body_surface2(const Batch& B, int it) {
                 }
             }
             ++stone_above;
-            R.y = y;
-            R.stone_above = stone_above;
-            R.stone_below = y - next_ceiling + 1;
-            R.water_height = water_height;
-            R.biome_set = false;
-            R.ch_set = false;
-            if (y >= tbm::kMinY && y <= kMaxY) {
-                const int state = tbgen::apply_rules(R);
-                if (state >= 0) C.set(y, state);
-            }
+            const uint32_t below = static_cast<uint32_t>(y - next_ceiling + 1);
+            const uint32_t wh = water_height == INT_MIN ? 1023u : static_cast<uint32_t>(water_height - tbm::kMinY);
+            w = static_cast<uint32_t>(stone_above) | (below << 10) | (wh << 20);
         }
+        walk[C.idx(y)] = w;
     }
-    if (surface_biome == tbm::kBiomeFrozenOcean || surface_biome == tbm::kBiomeDeepFrozenOcean)
-        frozen_ocean(C, R.min_surface(), surface_biome, start_h, true);
+}
+
+// pass 2b (item = chunk * kBlocksPerChunk + block index): the rule tree for one solid block
+TB_HD inline void body_surface_rules(const Batch& B, int it) {
+    const int c = it / kBlocksPerChunk, b = it % kBlocksPerChunk;
+    const uint32_t w = B.walk[it];
+    if (w == kNoWalk) return;
+    const int lx = b & 15, lz = (b >> 4) & 15, y = tbm::kMinY + (b >> 8);
+    const int col = lx * 16 + lz;
+    const ColumnRec& r = B.colrec[static_cast<size_t>(c) * 256 + col];
+    Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz, 0};
+    RuleCtx R{};
+    R.col = &C;
+    R.B = &B;
+    R.c = c;
+    R.surface_depth = r.surface_depth;
+    R.grad_x = r.grad_x;
+    R.grad_z = r.grad_z;
+    R.min_set = true;
+    R.min_surf = r.min_surface;
+    R.sec_set = true;
+    R.secondary = r.secondary;
+    R.y = y;
+    R.stone_above = static_cast<int>(w & 1023u);
+    R.stone_below = static_cast<int>((w >> 10) & 1023u);
+    const uint32_t wh = w >> 20;
+    R.water_height = wh == 1023u ? INT_MIN : static_cast<int>(wh) + tbm::kMinY;
+    R.biome_set = false;
+    R.ch_set = false;
+    const int state = tbgen::apply_rules(R);
+    if (state >= 0) C.blocks[b] = static_cast<uint16_t>(state);
+}
+
+// pass 2c (item = chunk * 256 + z * 16 + x): the frozen-ocean extension after the rules
+TB_HD inline void body_surface_frozen(const Batch& B, int it) {
+    const int c = it >> 8, lz = (it >> 4) & 15, lx = it & 15;
+    const int ci = (c << 8) | (lx << 4) | lz;   // x * 16 + z column index
+    const ColumnRec& r = B.colrec[ci];
+    if (r.surface_biome != tbm::kBiomeFrozenOcean && r.surface_biome != tbm::kBiomeDeepFrozenOcean) return;
+    Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
+             B.h1[ci]};
+    frozen_ocean(C, r.min_surface, r.surface_biome, r.start_h, true);
 }
 
 // centre chunk's quart biomes to the output (item = chunk * kQuartsPerChunk + q)

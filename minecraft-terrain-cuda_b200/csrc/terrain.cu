@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -48,14 +49,28 @@ void ck(cudaError_t e, const char* what) {
 }
 
 // ---- kernels: grid-stride loops over the bodies --------------------------------------------------
-template <void (*F)(const Batch&, int)>
-__global__ void __launch_bounds__(256) k_items(const __grid_constant__ Batch B, int n) {
+// Minimum resident 256-thread blocks per SM for the register-heavy kernels (caps registers).
+#ifndef TB_MINB_SURFACE2
+#define TB_MINB_SURFACE2 3
+#endif
+#ifndef TB_MINB_FILL
+#define TB_MINB_FILL 1
+#endif
+#ifndef TB_MINB_CORNER
+#define TB_MINB_CORNER 1
+#endif
+#ifndef TB_MINB_QUART
+#define TB_MINB_QUART 2
+#endif
+
+template <void (*F)(const Batch&, int), int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_items(const __grid_constant__ Batch B, int n) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) F(B, i);
 }
 
 // item count = *count * MUL (a device-side dedupe count)
-template <void (*F)(const Batch&, int), int MUL>
-__global__ void __launch_bounds__(256) k_dyn(const __grid_constant__ Batch B, const int32_t* count) {
+template <void (*F)(const Batch&, int), int MUL, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_dyn(const __grid_constant__ Batch B, const int32_t* count) {
     const int n = *count * MUL;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) F(B, i);
 }
@@ -155,7 +170,7 @@ struct Generator {
     cudaStream_t own_stream = nullptr;
     cudaEvent_t ev[8] = {};
     // model
-    DevBuf d_tree, d_children, d_leaf_biome, d_leaf_node, d_leaf_rank, d_flags, d_btemp, d_bfrozen;
+    DevBuf d_boxes, d_tree, d_children, d_leaf_biome, d_leaf_node, d_leaf_rank, d_flags, d_btemp, d_bfrozen;
     DevModel model{};
     int tree_depth = 0;
     // seeds
@@ -166,7 +181,7 @@ struct Generator {
     int current_slot = -1;
     // batch buffers
     DevBuf d_chunks, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_loc,
-        d_aq_status, d_aq_skip, d_blocks, d_h0, d_h1, d_h2, d_biomes, d_aqcopy, d_zoom;
+        d_aq_status, d_aq_skip, d_blocks, d_h0, d_h1, d_h2, d_biomes, d_aqcopy, d_zoom, d_walk, d_colrec;
     TableBufs tb_b, tb_c, tb_s;
     // pinned staging
     tg_chunk_xz* h_chunks = nullptr;
@@ -205,6 +220,7 @@ struct Generator {
         ModelHost m;
         build_model_host(m);
         upload(d_tree, m.nodes);
+        if (!m.boxes.empty()) upload(d_boxes, m.boxes);
         upload(d_children, m.children);
         upload(d_leaf_biome, m.leaf_biome);
         upload(d_leaf_node, m.leaf_node);
@@ -217,6 +233,7 @@ struct Generator {
         upload(d_bfrozen, bf);
         if (m.depth >= kSearchStack) throw Error(TG_ERR_INTERNAL, "climate tree deeper than the search stack");
         tree_depth = m.depth;
+        model.boxes = m.boxes.empty() ? nullptr : d_boxes.as<RBox>();
         model.tree = d_tree.as<RNode>();
         model.children = d_children.as<int32_t>();
         model.leaf_biome = d_leaf_biome.as<int32_t>();
@@ -266,6 +283,8 @@ struct Generator {
         d_h2.alloc(4 * 256 * N);
         d_biomes.alloc(N * kQuartsPerChunk);
         d_zoom.alloc(sizeof(uint32_t) * N * kZoomVerts);
+        d_walk.alloc(sizeof(uint32_t) * N * kBlocksPerChunk);
+        d_colrec.alloc(sizeof(ColumnRec) * N * 256);
     }
 
     // Resident per-seed tables: returns the slot, building and uploading on a miss.
@@ -344,6 +363,8 @@ struct Generator {
         B.h2 = d_h2.as<int32_t>();
         B.biomes_out = d_biomes.as<uint8_t>();
         B.zoom_tab = d_zoom.as<uint32_t>();
+        B.walk = d_walk.as<uint32_t>();
+        B.colrec = d_colrec.as<ColumnRec>();
         return B;
     }
 
@@ -354,7 +375,7 @@ struct Generator {
         launch(k_items<body_nb_insert>, s, 9 * n, B, 9 * n);
         launch(k_items<body_nb_resolve>, s, 9 * n, B, 9 * n);
         launch(k_dyn<body_climate_col, 16>, s, n * 16 * 2, B, static_cast<const int32_t*>(tb_b.count.as<int32_t>()));
-        launch(k_dyn<body_climate_quart, 16 * kRuns>, s, n * 16 * kRuns * 2, B, static_cast<const int32_t*>(tb_b.count.as<int32_t>()));
+        launch(k_dyn<body_climate_quart, 16 * kRuns, TB_MINB_QUART>, s, n * 16 * kRuns * 2, B, static_cast<const int32_t*>(tb_b.count.as<int32_t>()));
         launch(k_dyn<body_chain, 1>, s, n * 2, B, static_cast<const int32_t*>(tb_b.count.as<int32_t>()));
     }
 
@@ -372,7 +393,7 @@ struct Generator {
         launch(k_items<body_cc_insert>, s, 25 * n, B, 25 * n);
         launch(k_items<body_cc_resolve>, s, 25 * n, B, 25 * n);
         launch(k_dyn<body_corner_col, 1>, s, 16 * n, B, cnt_c);
-        launch(k_dyn<body_corner, kRows>, s, 16 * n * kRows, B, cnt_c);
+        launch(k_dyn<body_corner, kRows, TB_MINB_CORNER>, s, 16 * n * kRows, B, cnt_c);
         launch(k_items<body_zoom_table>, s, kZoomVerts * n, B, kZoomVerts * n);
         ck(cudaEventRecord(ev[2], s), "event");
         // aquifer stage
@@ -385,11 +406,13 @@ struct Generator {
         ck(cudaEventRecord(ev[3], s), "event");
         // fill
         launch(k_fill_i32, s, 256 * n, B.h0, static_cast<int32_t>(tbm::kMinY), 256 * n);
-        launch(k_items<body_fill>, s, 256 * kCellsY * n, B, 256 * kCellsY * n);
+        launch(k_items<body_fill, TB_MINB_FILL>, s, 256 * kCellsY * n, B, 256 * kCellsY * n);
         ck(cudaEventRecord(ev[4], s), "event");
         // surface
         launch(k_items<body_surface1>, s, 256 * n, B, 256 * n);
-        launch(k_items<body_surface2>, s, 256 * n, B, 256 * n);
+        launch(k_items<body_surface_walk>, s, 256 * n, B, 256 * n);
+        launch(k_items<body_surface_rules, TB_MINB_SURFACE2>, s, kBlocksPerChunk * n, B, kBlocksPerChunk * n);
+        launch(k_items<body_surface_frozen>, s, 256 * n, B, 256 * n);
         launch(k_items<body_gather>, s, kQuartsPerChunk * n, B, kQuartsPerChunk * n);
         ck(cudaEventRecord(ev[5], s), "event");
         ck(cudaGetLastError(), "kernel launch");

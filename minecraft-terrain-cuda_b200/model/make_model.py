@@ -636,12 +636,13 @@ def build_terrain(rng, ir_roots):
         cond(biome(*mesa), cond(sdepth(0, True, 30, False), B('terracotta'))),
         cond(ON_CEIL, cond(biome(*stony, *snowy), B('stone'))),
     )
+    # cave surfaces only: the cheap stone-depth tests gate the 3-D noise tests
     cave_rules = seq(
-        cond(biome(s('drip_caves')), seq(cond(noise('synth:calcite', -0.05, 0.05, True), B('dripstone_block')),
+        cond(biome(s('drip_caves')), seq(cond(ON_FLOOR, cond(noise('synth:calcite', -0.05, 0.05, True), B('dripstone_block'))),
                                          cond(ON_CEIL, B('dripstone_block')))),
         cond(biome(s('lush_caves')), seq(cond(ON_FLOOR, B('moss_block')), cond(ON_CEIL, B('clay')))),
-        cond(biome(s('ashen_flats')), seq(cond(noise('synth:calcite', 0.3, 0.7, True), B('smooth_basalt')),
-                                          cond(sdepth(2, False, 3, False), B('tuff')))),
+        cond(biome(s('ashen_flats')), seq(cond(sdepth(2, False, 3, False), seq(cond(noise('synth:calcite', 0.3, 0.7, True), B('smooth_basalt')),
+                                                                               B('tuff'))))),
     )
     ore = lambda k, o, raw, filler, chance: {'t': 'ore_vein', 'ore': P(o), 'raw_ore': P(raw), 'filler': P(filler),
                                              'raw_ore_chance': fbits(chance), 'density': 'ore_vein/%d/density' % k,

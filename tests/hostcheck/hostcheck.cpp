@@ -30,6 +30,7 @@ struct HostRun {
         flags.assign(tbm::kBlockFlags, tbm::kBlockFlags + tbm::kPaletteSize);
         btemp.assign(tbm::kBiomeTemp, tbm::kBiomeTemp + tbm::kNumBiomes);
         bfrozen.assign(tbm::kBiomeFrozen, tbm::kBiomeFrozen + tbm::kNumBiomes);
+        M.boxes = m.boxes.empty() ? nullptr : m.boxes.data();
         M.tree = m.nodes.data();
         M.children = m.children.data();
         M.leaf_biome = m.leaf_biome.data();
@@ -98,7 +99,8 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     std::vector<int32_t> lstar(nb * kQuartsPerChunk), h0(256 * N, tbm::kMinY), h1(256 * N), h2(256 * N);
     std::vector<uint8_t> qbiome(nb * kQuartsPerChunk), bout(N * kQuartsPerChunk);
     std::vector<uint16_t> bl(N * kBlocksPerChunk);
-    std::vector<uint32_t> ztab(N * kZoomVerts);
+    std::vector<uint32_t> ztab(N * kZoomVerts), walk(N * kBlocksPerChunk);
+    std::vector<ColumnRec> colrec(N * 256);
     Batch B{};
     B.M = R.M;
     B.seeds = &R.D;
@@ -132,6 +134,8 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     B.h2 = h2.data();
     B.biomes_out = bout.data();
     B.zoom_tab = ztab.data();
+    B.walk = walk.data();
+    B.colrec = colrec.data();
     each(9 * n, [&](int i) { body_nb_insert(B, i); });
     each(9 * n, [&](int i) { body_nb_resolve(B, i); });
     each(hb.count * 16, [&](int i) { body_climate_col(B, i); });
@@ -150,7 +154,9 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     each(256 * kCellsY * n, [&](int i) { body_fill(B, i); });
     if (aquifer) std::memcpy(aquifer, bl.data(), sizeof(uint16_t) * bl.size());
     each(256 * n, [&](int i) { body_surface1(B, i); });
-    each(256 * n, [&](int i) { body_surface2(B, i); });
+    each(256 * n, [&](int i) { body_surface_walk(B, i); });
+    each(kBlocksPerChunk * n, [&](int i) { body_surface_rules(B, i); });
+    each(256 * n, [&](int i) { body_surface_frozen(B, i); });
     each(kQuartsPerChunk * n, [&](int i) { body_gather(B, i); });
     std::memcpy(blocks, bl.data(), sizeof(uint16_t) * bl.size());
     if (biomes) std::memcpy(biomes, bout.data(), bout.size());
@@ -241,3 +247,59 @@ void hc_md5(const uint8_t* d, int64_t n, uint8_t* out) { md5(d, static_cast<size
 void hc_sha256(const uint8_t* d, int64_t n, uint8_t* out) { sha256(d, static_cast<size_t>(n), out); }
 
 }  // extern "C"
+
+extern "C" {
+// Distance evaluations of the first-minimal-leaf search for each target (6 int64 each),
+// starting from the previous target's leaf (a column run), for search-cost studies.
+int hc_tree_visits(const long long* t, int32_t n, int32_t* visits, int32_t* leaves) {
+    ModelHost m;
+    build_model_host(m);
+    int prev = 0;
+    for (int i = 0; i < n; ++i) {
+        const long long* q = t + 6 * i;
+        int best = prev, best_rank = m.leaf_rank[prev];
+        auto dist = [&](const RNode& nd) {
+            long long d = 0;
+            for (int k = 0; k < 7; ++k) {
+                const long long tv = k < 6 ? q[k] : 0;
+                const long long a = tv - nd.mx[k], b = nd.mn[k] - tv;
+                const long long p = a > 0 ? a : (b > 0 ? b : 0);
+                d += p * p;
+            }
+            return d;
+        };
+        long long best_d = dist(m.nodes[m.leaf_node[prev]]);
+        int cnt = 0;
+        std::vector<std::pair<int, int>> st{{m.root, 0}};
+        while (!st.empty()) {
+            auto& f = st.back();
+            const RNode& nd = m.nodes[f.first];
+            if (f.second >= nd.child_count) { st.pop_back(); continue; }
+            const int ci = m.children[nd.first_child + f.second++];
+            const RNode& ch = m.nodes[ci];
+            const long long d = dist(ch);
+            ++cnt;
+            if (d < best_d || (d == best_d && ch.rank < best_rank)) {
+                if (ch.leaf >= 0) { best = ch.leaf; best_rank = ch.rank; best_d = d; }
+                else st.push_back({ci, 0});
+            }
+        }
+        visits[i] = cnt;
+        leaves[i] = best;
+        prev = best;
+    }
+    return 0;
+}
+}
+
+extern "C" {
+// Climate tree shape: depth (root = 1), node count, whether the 32-bit search applies.
+int hc_tree_info(int32_t* out3) {
+    ModelHost m;
+    build_model_host(m);
+    out3[0] = m.depth;
+    out3[1] = static_cast<int32_t>(m.nodes.size());
+    out3[2] = m.boxes.empty() ? 0 : 1;
+    return 0;
+}
+}
