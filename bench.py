@@ -35,7 +35,7 @@ SEED = 0x5445525241494E31   # "TERRAIN1"
 REGIONS = [('origin', 0, 0), ('negative', -62500, -62500), ('border', 117124, 117124)]
 SIDE = 64
 BYTES_PER_CHUNK = 98304 * 2 + 1536
-METRIC = 'bit-exact TERRAIN chunks/s on 1 B200 (plain form, ladder size: one seed, three 64x64-chunk regions)'
+METRIC = 'bit-exact TERRAIN chunks/s on 1 B200, served vs plain; p50/p99 request latency'
 
 
 def region_chunks(x0, z0, side=SIDE):
@@ -156,6 +156,101 @@ def run_reference(args, rank):
     print(json.dumps(line))
 
 
+def serving_requests(n, rng):
+    """View-distance requests: a (2r+1)^2 square or the ring of radius r (r in 2..12) around a
+    uniform centre within +/-117,187 chunks; seeds from a pool of 64."""
+    seeds = [int(v) for v in rng.integers(-(1 << 62), 1 << 62, 64)]
+    reqs = []
+    for _ in range(n):
+        r = int(rng.integers(2, 13))
+        cx, cz = (int(v) for v in rng.integers(-117187 + r, 117187 - r, 2))
+        if rng.random() < 0.5:
+            chunks = [(cx + dx, cz + dz) for dz in range(-r, r + 1) for dx in range(-r, r + 1)]
+        else:
+            chunks = [(cx + dx, cz + dz) for dz in range(-r, r + 1) for dx in range(-r, r + 1) if max(abs(dx), abs(dz)) == r]
+        reqs.append((seeds[int(rng.integers(0, 64))], np.array(chunks, np.int32)))
+    return seeds, reqs
+
+
+def served_bench(g, n_requests=96, batch_chunks=1024, load_frac=0.6, seed=2024):
+    """Plain (one synchronous tg_generate per request, in order) against the continuous-batching
+    server on the same request stream: saturated throughput of both, then latency of the server
+    under Poisson arrivals at load_frac of its saturated throughput. Outputs go to pinned host
+    memory in both forms."""
+    import torch
+    import terrain_b200
+    rng = np.random.default_rng(seed)
+    seeds, reqs = serving_requests(n_requests, rng)
+    total = sum(len(c) for _, c in reqs)
+    h = g.height
+    pool = torch.empty(total * (256 * h + 768), dtype=torch.int16, pin_memory=True).numpy().view(np.uint16)
+    offs, at = [], 0
+    for _, c in reqs:
+        offs.append(at)
+        at += len(c) * (256 * h + 768)
+
+    def bufs(i):
+        n = len(reqs[i][1])
+        b = pool[offs[i]:offs[i] + n * 256 * h].reshape(n, h, 16, 16)
+        q = pool[offs[i] + n * 256 * h:offs[i] + n * (256 * h + 768)].view(np.uint8).reshape(n, 1536)
+        return b, q
+
+    for sd in seeds:                      # resident tables for the whole pool
+        g.set_seed(sd)
+    g.generate(reqs[0][1][:1])
+    t0 = time.perf_counter()
+    for i, (sd, c) in enumerate(reqs):
+        b, q = bufs(i)
+        g.set_seed(sd)
+        g.generate(c, blocks_out=b, biomes_out=q)
+    plain_s = time.perf_counter() - t0
+    plain_cps = total / plain_s
+    out = {'requests': n_requests, 'chunks': total, 'seed_pool': 64, 'batch_chunks': batch_chunks,
+           'plain_chunks_per_s': round(plain_cps, 1)}
+    with terrain_b200.TerrainServer(g, batch_chunks=batch_chunks) as srv:
+        warm = [srv.submit(sd, c) for sd, c in reqs[:4]]
+        for t in warm:
+            srv.wait(t)
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        tickets = []
+        for i, (sd, c) in enumerate(reqs):
+            b, q = bufs(i)
+            tickets.append(srv.submit(sd, c, b, q))
+        for t in tickets:
+            srv.wait(t)
+        sat_s = time.perf_counter() - t0
+        st = srv.stats()
+        out['served_saturated_chunks_per_s'] = round(total / sat_s, 1)
+        out['saturated_p50_ms'] = round(st['p50_ms'], 2)
+        out['saturated_p99_ms'] = round(st['p99_ms'], 2)
+        # Poisson arrivals at a fraction of the saturated throughput
+        rate = load_frac * (total / sat_s) / (total / n_requests)      # requests per second
+        gaps = rng.exponential(1.0 / rate, n_requests)
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        tickets = []
+        due = t0
+        for i, (sd, c) in enumerate(reqs):
+            due += gaps[i]
+            wait = due - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            b, q = bufs(i)
+            tickets.append(srv.submit(sd, c, b, q))
+        for t in tickets:
+            srv.wait(t)
+        st = srv.stats()
+        out['offered_requests_per_s'] = round(rate, 1)
+        out['offered_chunks_per_s'] = round(rate * total / n_requests, 1)
+        out['served_chunks_per_s'] = round(st['chunks_per_s'], 1)
+        out['p50_ms'] = round(st['p50_ms'], 2)
+        out['p99_ms'] = round(st['p99_ms'], 2)
+        out['max_ms'] = round(st['max_ms'], 2)
+    out['served_over_plain'] = round(out['served_saturated_chunks_per_s'] / plain_cps, 3)
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import terrain_b200
@@ -209,14 +304,13 @@ def run_ours(args, rank, world, local_rank):
     value = chunks_total / (ms_max / 1000.0)
 
     # end to end through the host API: pinned host outputs, copies inside the step
-    pin_blocks = [torch.empty(n * 98304, dtype=torch.int16, pin_memory=True) for _ in range(nreg)]
-    pin_biomes = [torch.empty(n * 1536, dtype=torch.uint8, pin_memory=True) for _ in range(nreg)]
-    np_blocks = [b.numpy().view(np.uint16).reshape(n, -1, 16, 16) for b in pin_blocks]
-    np_biomes = [b.numpy().reshape(n, -1) for b in pin_biomes]
+    all_chunks = np.concatenate(host_chunks)
+    pin_all_blocks = torch.empty(n * nreg * 98304, dtype=torch.int16, pin_memory=True).numpy().view(np.uint16).reshape(n * nreg, -1, 16, 16)
+    pin_all_biomes = torch.empty(n * nreg * 1536, dtype=torch.uint8, pin_memory=True).numpy().reshape(n * nreg, -1)
 
     def step_e2e():
-        for r in range(nreg):
-            g.generate(host_chunks[r], blocks_out=np_blocks[r], biomes_out=np_biomes[r])
+        # one call per step: the library pipelines its batches (copies of batch k overlap batch k + 1)
+        g.generate(all_chunks, blocks_out=pin_all_blocks, biomes_out=pin_all_biomes)
 
     for _ in range(max(1, min(args.warmup, 2))):
         step_e2e()
@@ -263,6 +357,9 @@ def run_ours(args, rank, world, local_rank):
         'gpu_launches': int(launches),
         'clocks': clk.summary(),
     }
+    if not args.no_serve:
+        g.set_stream(0)
+        line['served'] = served_bench(g)
     if not args.no_cpu_baseline:
         line['cpu_baseline'] = cpu_baseline()
     print(json.dumps(line))
@@ -275,6 +372,7 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-serve', action='store_true', help='skip the served-versus-plain request-stream measurement')
     ap.add_argument('--profile-small', action='store_true',
                     help='one untimed step over a 16x16-chunk corner of each region (a small case for ncu captures)')
     args = ap.parse_args()

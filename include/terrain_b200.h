@@ -107,6 +107,40 @@ tg_status tg_generate_batch(struct tg_generator* gen, const tg_request* requests
  * cpu/src/terrain.cpp:152-176). */
 tg_status tg_biome_lookup(struct tg_generator* gen, const int64_t* seeds, const int32_t* xyz, int32_t n, uint8_t* out);
 
+/* ---- serving: continuous batching ---------------------------------------------------
+ * A server owns its generator (which then rejects direct calls until the server is
+ * destroyed). A worker thread admits submitted requests while the chunks in flight stay
+ * within the HBM-derived limit, cuts device batches across all admitted requests (seeds
+ * and request sizes mixed), and copies each batch out on a second stream while the next
+ * one computes; per-seed tables stay resident on the device. Results are byte-identical
+ * to tg_generate for the same seed and chunks, alone or in any mix.
+ * No counterpart in the reference (it has no serving form). */
+typedef struct tg_server_config {
+    int32_t batch_chunks;       /* chunks per device batch (<= max_batch_chunks); 0 = max_batch_chunks */
+    int64_t hbm_budget_bytes;   /* output bytes admitted but not yet issued; 0 = 8 batches */
+    int32_t reserved;
+} tg_server_config;
+
+typedef struct tg_server_stats {
+    int64_t completed_requests, completed_chunks;
+    double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> last byte on the host */
+    double chunks_per_s;                     /* completed chunks / (first submit -> last completion) */
+    int32_t batches, queued_requests, active_requests;
+} tg_server_stats;
+
+tg_status tg_server_create(struct tg_generator* gen, const tg_server_config* config, struct tg_server** out);
+/* Queues a request; blocks_out (count * 16 * 16 * height u16) and biomes_out (may be NULL)
+ * are host buffers that must stay valid until the request completes. Non-blocking. */
+tg_status tg_server_submit(struct tg_server* srv, int64_t seed, const tg_chunk_xz* chunks, int32_t count, uint16_t* blocks_out, uint8_t* biomes_out,
+                           uint64_t* ticket);
+/* *done = 1 once the request's outputs are on the host (the ticket is then released);
+ * timeout_ms: 0 polls, < 0 waits without limit. */
+tg_status tg_server_wait(struct tg_server* srv, uint64_t ticket, int32_t timeout_ms, int32_t* done);
+tg_status tg_server_get_stats(struct tg_server* srv, tg_server_stats* stats);
+tg_status tg_server_reset_stats(struct tg_server* srv);
+/* Finishes the work in flight, then stops the worker. */
+tg_status tg_server_destroy(struct tg_server* srv);
+
 /* Pinned host memory for outputs. reference: alloc_pinned / free_pinned
  * (cuda/include/mccuda_cuda/terrain_gpu.h:62-63) */
 void* tg_alloc_pinned(size_t bytes);

@@ -79,7 +79,7 @@ constexpr unsigned long long kEmpty = ~0ull;
 struct Batch {
     DevModel M;
     const DevSeed* seeds;
-    int32_t n;                        // chunks in the batch
+    const int32_t* n_dev;             // chunks in the batch (device memory, so one graph serves any size)
     const int32_t* cx;                // chunk coordinates, seed slot
     const int32_t* cz;
     const int32_t* cseed;

@@ -1,30 +1,40 @@
-// TERRAIN step on sm_100a: kernels, the batch pipeline and the C ABI of
-// include/terrain_b200.h.
+// TERRAIN step on sm_100a: kernels, the batch pipeline, the continuous-batching server
+// and the C ABI of include/terrain_b200.h.
 //
 // Pipeline of one batch (all on one stream, all positions deduplicated on the device
 // through hash tables, so nothing returns to the host until the outputs):
 //   biome stage    neighbourhood union -> climate columns -> climate + first minimal
 //                  leaf per quart -> last-result chain per biome chunk
-//   noise stage    corner-column union -> hoisted y = 0 values -> 4x8 channel corners
+//   noise stage    corner-column union -> hoisted y = 0 values -> 4x8 channel corners,
+//                  zoom fiddle table
 //   aquifer stage  surface-level quart union (volume / point) -> find_top_surface ->
 //                  aquifer cell locations and fluid status, skip heights
 //   fill           per 8-block cell column: channels, final density, substance, heights
-//   surface        per column: eroded badlands + frozen-ocean dry run, then the rule
-//                  walk and the frozen-ocean extension
-// Reference: cuda/src/terrain.cu:1259-1332 (run_batch) and cpu/src/terrain.cpp:750-810.
+//   surface        eroded badlands + frozen-ocean dry run per column, the walk state per
+//                  column, the rule tree per block, the frozen-ocean extension per column
+// The batch size lives in device memory and every kernel is a grid-stride loop, so the
+// whole batch is captured once as a CUDA graph per output buffer and replayed for any
+// batch size up to the capacity. Outputs are double-buffered: the copy stream drains
+// batch k while batch k + 1 computes.
+// Reference: cuda/src/terrain.cu:1259-1417 (run_batch / generate) and
+// cpu/src/terrain.cpp:750-810.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <climits>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <fstream>
 #include <memory>
 #include <mutex>
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -48,6 +58,8 @@ void ck(cudaError_t e, const char* what) {
     }
 }
 
+double now_ms() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
+
 // ---- kernels: grid-stride loops over the bodies --------------------------------------------------
 // Minimum resident 256-thread blocks per SM for the register-heavy kernels (caps registers).
 #ifndef TB_MINB_SURFACE2
@@ -63,8 +75,10 @@ void ck(cudaError_t e, const char* what) {
 #define TB_MINB_QUART 2
 #endif
 
-template <void (*F)(const Batch&, int), int MINB = 1>
-__global__ void __launch_bounds__(256, MINB) k_items(const __grid_constant__ Batch B, int n) {
+// item count = chunks in the batch * MUL
+template <void (*F)(const Batch&, int), int MUL, int MINB = 1>
+__global__ void __launch_bounds__(256, MINB) k_items(const __grid_constant__ Batch B) {
+    const int n = *B.n_dev * MUL;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) F(B, i);
 }
 
@@ -75,20 +89,23 @@ __global__ void __launch_bounds__(256, MINB) k_dyn(const __grid_constant__ Batch
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) F(B, i);
 }
 
-__global__ void k_fill_i32(int32_t* p, int32_t v, int n) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+__global__ void k_init_heights(const __grid_constant__ Batch B) {
+    const int n = *B.n_dev * 256;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) B.h0[i] = tbm::kMinY;
 }
 
-__global__ void k_split_chunks(const tg_chunk_xz* ch, int n, int32_t slot, int32_t* cx, int32_t* cz, int32_t* cs) {
+__global__ void k_split_chunks(const tg_chunk_xz* ch, int n, int32_t slot, int32_t* cx, int32_t* cz, int32_t* cs, int32_t* n_dev) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         cx[i] = ch[i].x;
         cz[i] = ch[i].z;
         cs[i] = slot;
     }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n_dev = n;
 }
 
 // one lookup position per item: the zoomed biome from its chunk's neighbourhood
-__global__ void k_biome_lookup(const __grid_constant__ Batch B, const int32_t* xyz, uint8_t* out, int n) {
+__global__ void k_biome_lookup(const __grid_constant__ Batch B, const int32_t* xyz, uint8_t* out) {
+    const int n = *B.n_dev;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
         out[i] = static_cast<uint8_t>(zoom_biome(B, i, B.seeds[B.cseed[i]].zoom_seed, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
 }
@@ -96,12 +113,12 @@ __global__ void k_biome_lookup(const __grid_constant__ Batch B, const int32_t* x
 int g_sm_count = 148;
 thread_local int g_launches = 0;
 
+// grid for a grid-stride kernel: enough blocks for the items, at most 8 per SM
 template <typename K, typename... Args>
-void launch(K kernel, cudaStream_t s, int items_hint, Args... args) {
+void launch(K kernel, cudaStream_t s, long items_hint, Args... args) {
     const int threads = 256;
-    long blocks = (static_cast<long>(items_hint) + threads - 1) / threads;
-    const long cap = static_cast<long>(g_sm_count) * 8;
-    blocks = std::max(1L, std::min(blocks, cap));
+    long blocks = (items_hint + threads - 1) / threads;
+    blocks = std::max(1L, std::min(blocks, static_cast<long>(g_sm_count) * 8));
     kernel<<<static_cast<unsigned>(blocks), threads, 0, s>>>(args...);
     ++g_launches;
 }
@@ -112,7 +129,7 @@ uint32_t pow2_at_least(uint64_t v) {
     return p;
 }
 
-// ---- device memory ---------------------------------------------------------------------------------
+// ---- device and pinned memory -------------------------------------------------------------------
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -127,6 +144,25 @@ struct DevBuf {
         p = nullptr;
         bytes = b;
         if (b) ck(cudaMalloc(&p, b), "cudaMalloc");
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+};
+
+struct PinBuf {
+    void* p = nullptr;
+    PinBuf() = default;
+    PinBuf(const PinBuf&) = delete;
+    PinBuf& operator=(const PinBuf&) = delete;
+    ~PinBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    void alloc(size_t b) {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        if (b) ck(cudaMallocHost(&p, b), "cudaMallocHost");
     }
     template <class T>
     T* as() const {
@@ -151,7 +187,7 @@ struct TableBufs {
     }
 };
 
-constexpr int kMaxSlots = 512;
+constexpr int kMaxSlots = 512;   // resident seeds (the 9-bit seed field of the position keys)
 
 struct SeedSlot {
     int64_t seed = 0;
@@ -160,31 +196,45 @@ struct SeedSlot {
     DevBuf off, perm, layers;
 };
 
+// one output buffer set (the pipeline's outputs are double-buffered)
+struct OutSlot {
+    DevBuf blocks, biomes, aquifer;
+    PinBuf coords;             // staged cx | cz | cs | n of the batch
+    cudaEvent_t computed = nullptr, drained = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    bool graph_aquifer = false;
+    cudaStream_t graph_stream = nullptr;
+    bool busy = false;         // outputs not yet drained to the host
+};
+
 }  // namespace
 
 // ---- the generator ----------------------------------------------------------------------------------
 struct Generator {
     int device = 0;
     int max_batch = 2048;
-    cudaStream_t stream = nullptr;      // the stream all work runs on
+    cudaStream_t stream = nullptr;      // compute stream (the caller's, when set)
     cudaStream_t own_stream = nullptr;
+    cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev[8] = {};
+    bool use_graphs = true;
+    std::atomic<bool> served{false};    // owned by a server's worker thread
     // model
     DevBuf d_boxes, d_tree, d_children, d_leaf_biome, d_leaf_node, d_leaf_rank, d_flags, d_btemp, d_bfrozen;
     DevModel model{};
     int tree_depth = 0;
     // seeds
     std::unique_ptr<SeedSlot[]> slots;
-    DevBuf d_seeds;                 // kMaxSlots DevSeed
-    std::vector<DevSeed> h_seeds;
+    DevBuf d_seeds;
     uint64_t use_clock = 0;
     int current_slot = -1;
-    // batch buffers
-    DevBuf d_chunks, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_loc,
-        d_aq_status, d_aq_skip, d_blocks, d_h0, d_h1, d_h2, d_biomes, d_aqcopy, d_zoom, d_walk, d_colrec;
+    // batch buffers (shared by both output slots: the kernels of one batch at a time use them)
+    DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_loc, d_aq_status,
+        d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_walk, d_colrec;
     TableBufs tb_b, tb_c, tb_s;
-    // pinned staging
-    tg_chunk_xz* h_chunks = nullptr;
+    OutSlot out[2];
+    int next_out = 0;
+    int graph_launches = 0;
 
     Generator(int dev, int batch) : device(dev), max_batch(batch) {
         ck(cudaSetDevice(device), "cudaSetDevice");
@@ -192,21 +242,29 @@ struct Generator {
         ck(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
         g_sm_count = prop.multiProcessorCount;
         ck(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
         stream = own_stream;
         for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
-        // generated evaluators and the rule tree use deep inlined frames
-        ck(cudaDeviceSetLimit(cudaLimitStackSize, 16384), "cudaDeviceSetLimit");
+        for (auto& o : out) {
+            ck(cudaEventCreateWithFlags(&o.computed, cudaEventDisableTiming), "cudaEventCreate");
+            ck(cudaEventCreateWithFlags(&o.drained, cudaEventDisableTiming), "cudaEventCreate");
+        }
         upload_model();
         slots.reset(new SeedSlot[kMaxSlots]);
-        h_seeds.resize(kMaxSlots);
         d_seeds.alloc(sizeof(DevSeed) * kMaxSlots);
         alloc_batch(max_batch);
-        ck(cudaMallocHost(reinterpret_cast<void**>(&h_chunks), sizeof(tg_chunk_xz) * max_batch), "cudaMallocHost");
     }
     ~Generator() {
-        if (h_chunks) cudaFreeHost(h_chunks);
+        cudaSetDevice(device);
+        cudaDeviceSynchronize();
+        for (auto& o : out) {
+            if (o.graph) cudaGraphExecDestroy(o.graph);
+            if (o.computed) cudaEventDestroy(o.computed);
+            if (o.drained) cudaEventDestroy(o.drained);
+        }
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 
@@ -225,12 +283,9 @@ struct Generator {
         upload(d_leaf_biome, m.leaf_biome);
         upload(d_leaf_node, m.leaf_node);
         upload(d_leaf_rank, m.leaf_rank);
-        std::vector<uint8_t> flags(tbm::kBlockFlags, tbm::kBlockFlags + tbm::kPaletteSize);
-        upload(d_flags, flags);
-        std::vector<float> bt(tbm::kBiomeTemp, tbm::kBiomeTemp + tbm::kNumBiomes);
-        upload(d_btemp, bt);
-        std::vector<uint8_t> bf(tbm::kBiomeFrozen, tbm::kBiomeFrozen + tbm::kNumBiomes);
-        upload(d_bfrozen, bf);
+        upload(d_flags, std::vector<uint8_t>(tbm::kBlockFlags, tbm::kBlockFlags + tbm::kPaletteSize));
+        upload(d_btemp, std::vector<float>(tbm::kBiomeTemp, tbm::kBiomeTemp + tbm::kNumBiomes));
+        upload(d_bfrozen, std::vector<uint8_t>(tbm::kBiomeFrozen, tbm::kBiomeFrozen + tbm::kNumBiomes));
         if (m.depth >= kSearchStack) throw Error(TG_ERR_INTERNAL, "climate tree deeper than the search stack");
         tree_depth = m.depth;
         model.boxes = m.boxes.empty() ? nullptr : d_boxes.as<RBox>();
@@ -255,7 +310,7 @@ struct Generator {
 
     void alloc_batch(int n) {
         const size_t N = static_cast<size_t>(n);
-        d_chunks.alloc(sizeof(tg_chunk_xz) * N);
+        d_n.alloc(sizeof(int32_t));
         d_cx.alloc(4 * N);
         d_cz.alloc(4 * N);
         d_cs.alloc(4 * N);
@@ -277,18 +332,22 @@ struct Generator {
         d_aq_loc.alloc(sizeof(int32_t) * N * kAqCells * 3);
         d_aq_status.alloc(sizeof(int32_t) * N * kAqCells * 2);
         d_aq_skip.alloc(4 * N);
-        d_blocks.alloc(sizeof(uint16_t) * N * kBlocksPerChunk);
         d_h0.alloc(4 * 256 * N);
         d_h1.alloc(4 * 256 * N);
         d_h2.alloc(4 * 256 * N);
-        d_biomes.alloc(N * kQuartsPerChunk);
         d_zoom.alloc(sizeof(uint32_t) * N * kZoomVerts);
         d_walk.alloc(sizeof(uint32_t) * N * kBlocksPerChunk);
         d_colrec.alloc(sizeof(ColumnRec) * N * 256);
+        for (auto& o : out) {
+            o.blocks.alloc(sizeof(uint16_t) * N * kBlocksPerChunk);
+            o.biomes.alloc(N * kQuartsPerChunk);
+            o.coords.alloc(sizeof(int32_t) * (3 * N + 1));
+        }
     }
 
-    // Resident per-seed tables: returns the slot, building and uploading on a miss.
-    int seed_slot(int64_t seed, const std::vector<int>& pinned_slots = {}) {
+    // Resident per-seed tables: the slot of a seed, built and uploaded on a miss; slots
+    // listed in `keep` are not evicted.
+    int seed_slot(int64_t seed, const std::vector<int>& keep = {}) {
         ++use_clock;
         int free_slot = -1, lru = -1;
         for (int i = 0; i < kMaxSlots; ++i) {
@@ -301,7 +360,7 @@ struct Generator {
         int s = free_slot;
         if (s < 0) {
             for (int i = 0; i < kMaxSlots; ++i) {
-                if (std::find(pinned_slots.begin(), pinned_slots.end(), i) != pinned_slots.end()) continue;
+                if (std::find(keep.begin(), keep.end(), i) != keep.end()) continue;
                 if (lru < 0 || slots[i].last_use < slots[lru].last_use) lru = i;
             }
             s = lru;
@@ -309,6 +368,8 @@ struct Generator {
         if (s < 0) throw Error(TG_ERR_INTERNAL, "no free seed slot");
         SeedHost h;
         build_seed_host(seed, h);
+        // queued work may still read the tables this slot held
+        if (slots[s].valid) ck(cudaDeviceSynchronize(), "sync");
         SeedSlot& sl = slots[s];
         upload(sl.off, h.off);
         upload(sl.perm, h.perm);
@@ -321,7 +382,6 @@ struct Generator {
         for (size_t k = 0; k < h.gradient.size(); ++k) d.gradient[k] = h.gradient[k];
         d.zoom_seed = h.zoom_seed;
         std::memcpy(d.clay, h.clay, sizeof d.clay);
-        h_seeds[s] = d;
         ck(cudaMemcpy(d_seeds.as<DevSeed>() + s, &d, sizeof(DevSeed), cudaMemcpyHostToDevice), "seed upload");
         sl.seed = seed;
         sl.valid = true;
@@ -329,16 +389,16 @@ struct Generator {
         return s;
     }
 
-    Batch batch_view(int n) const {
+    Batch batch_view(const OutSlot* o) const {
         Batch B{};
         B.M = model;
         B.seeds = d_seeds.as<DevSeed>();
-        B.n = n;
+        B.n_dev = d_n.as<int32_t>();
         B.cx = d_cx.as<int32_t>();
         B.cz = d_cz.as<int32_t>();
         B.cseed = d_cs.as<int32_t>();
         B.hb = tb_b.view();
-        B.nb_cap = 9 * n;
+        B.nb_cap = 9 * max_batch;
         B.nb9 = d_nb9.as<int32_t>();
         B.bcol = d_bcol.as<float>();
         B.tgt = d_tgt.as<long long>();
@@ -346,89 +406,137 @@ struct Generator {
         B.mdist = d_mdist.as<long long>();
         B.qbiome = d_qbiome.as<uint8_t>();
         B.hc = tb_c.view();
-        B.cc_cap = 25 * n;
+        B.cc_cap = 25 * max_batch;
         B.c25 = d_c25.as<int32_t>();
         B.ccol = d_ccol.as<float>();
         B.corners = d_corners.as<float>();
         B.hs = tb_s.view();
-        B.sg_cap = kGrid * n;
+        B.sg_cap = kGrid * max_batch;
         B.g513 = d_g513.as<int32_t>();
         B.sfts = d_sfts.as<float>();
         B.aq_loc = d_aq_loc.as<int32_t>();
         B.aq_status = d_aq_status.as<int32_t>();
         B.aq_skip = d_aq_skip.as<int32_t>();
-        B.blocks = d_blocks.as<uint16_t>();
+        B.blocks = o ? o->blocks.as<uint16_t>() : nullptr;
         B.h0 = d_h0.as<int32_t>();
         B.h1 = d_h1.as<int32_t>();
         B.h2 = d_h2.as<int32_t>();
-        B.biomes_out = d_biomes.as<uint8_t>();
+        B.biomes_out = o ? o->biomes.as<uint8_t>() : nullptr;
         B.zoom_tab = d_zoom.as<uint32_t>();
         B.walk = d_walk.as<uint32_t>();
         B.colrec = d_colrec.as<ColumnRec>();
         return B;
     }
 
-    // biome stage only (shared by the TERRAIN step and biome lookups)
-    void run_biomes(const Batch& B, int n) {
-        cudaStream_t s = stream;
+    // biome stage (shared by the TERRAIN step and biome lookups); nmax sizes the grids
+    void enqueue_biomes(const Batch& B, cudaStream_t s, long nmax) {
+        const int32_t* cnt_b = tb_b.count.as<int32_t>();
         tb_b.reset(s);
-        launch(k_items<body_nb_insert>, s, 9 * n, B, 9 * n);
-        launch(k_items<body_nb_resolve>, s, 9 * n, B, 9 * n);
-        launch(k_dyn<body_climate_col, 16>, s, n * 16 * 2, B, static_cast<const int32_t*>(tb_b.count.as<int32_t>()));
-        launch(k_dyn<body_climate_quart, 16 * kRuns, TB_MINB_QUART>, s, n * 16 * kRuns * 2, B, static_cast<const int32_t*>(tb_b.count.as<int32_t>()));
-        launch(k_dyn<body_chain, 1>, s, n * 2, B, static_cast<const int32_t*>(tb_b.count.as<int32_t>()));
+        launch(k_items<body_nb_insert, 9>, s, 9 * nmax, B);
+        launch(k_items<body_nb_resolve, 9>, s, 9 * nmax, B);
+        launch(k_dyn<body_climate_col, 16>, s, nmax * 16 * 2, B, cnt_b);
+        launch(k_dyn<body_climate_quart, 16 * kRuns, TB_MINB_QUART>, s, nmax * 16 * kRuns * 2, B, cnt_b);
+        launch(k_dyn<body_chain, 1>, s, nmax * 2, B, cnt_b);
     }
 
-    // One device batch of n chunks whose coordinates are already in d_cx/d_cz/d_cs.
-    void run_batch(int n, tg_timing* t) {
-        cudaStream_t s = stream;
-        const Batch B = batch_view(n);
+    // every kernel of one batch; with timed set, events split the stages
+    void enqueue_batch(const Batch& B, cudaStream_t s, long nmax, uint16_t* aquifer_dev, bool timed) {
+        auto mark = [&](int i) {
+            if (timed) ck(cudaEventRecord(ev[i], s), "event");
+        };
         const int32_t* cnt_c = tb_c.count.as<int32_t>();
         const int32_t* cnt_s = tb_s.count.as<int32_t>();
-        ck(cudaEventRecord(ev[0], s), "event");
-        run_biomes(B, n);
-        ck(cudaEventRecord(ev[1], s), "event");
-        // noise stage
+        mark(0);
+        enqueue_biomes(B, s, nmax);
+        mark(1);
         tb_c.reset(s);
-        launch(k_items<body_cc_insert>, s, 25 * n, B, 25 * n);
-        launch(k_items<body_cc_resolve>, s, 25 * n, B, 25 * n);
-        launch(k_dyn<body_corner_col, 1>, s, 16 * n, B, cnt_c);
-        launch(k_dyn<body_corner, kRows, TB_MINB_CORNER>, s, 16 * n * kRows, B, cnt_c);
-        launch(k_items<body_zoom_table>, s, kZoomVerts * n, B, kZoomVerts * n);
-        ck(cudaEventRecord(ev[2], s), "event");
-        // aquifer stage
+        launch(k_items<body_cc_insert, 25>, s, 25 * nmax, B);
+        launch(k_items<body_cc_resolve, 25>, s, 25 * nmax, B);
+        launch(k_dyn<body_corner_col, 1>, s, 16 * nmax, B, cnt_c);
+        launch(k_dyn<body_corner, kRows, TB_MINB_CORNER>, s, 16 * nmax * kRows, B, cnt_c);
+        launch(k_items<body_zoom_table, kZoomVerts>, s, kZoomVerts * nmax, B);
+        mark(2);
         tb_s.reset(s);
-        launch(k_items<body_sg_insert>, s, kGrid * n, B, kGrid * n);
-        launch(k_items<body_sg_resolve>, s, kGrid * n, B, kGrid * n);
-        launch(k_dyn<body_surface_level, 1>, s, 2 * n * 100, B, cnt_s);
-        launch(k_items<body_aquifer_cell>, s, kAqCells * n, B, kAqCells * n);
-        launch(k_items<body_aquifer_skip>, s, n, B, n);
-        ck(cudaEventRecord(ev[3], s), "event");
-        // fill
-        launch(k_fill_i32, s, 256 * n, B.h0, static_cast<int32_t>(tbm::kMinY), 256 * n);
-        launch(k_items<body_fill, TB_MINB_FILL>, s, 256 * kCellsY * n, B, 256 * kCellsY * n);
-        ck(cudaEventRecord(ev[4], s), "event");
-        // surface
-        launch(k_items<body_surface1>, s, 256 * n, B, 256 * n);
-        launch(k_items<body_surface_walk>, s, 256 * n, B, 256 * n);
-        launch(k_items<body_surface_rules, TB_MINB_SURFACE2>, s, kBlocksPerChunk * n, B, kBlocksPerChunk * n);
-        launch(k_items<body_surface_frozen>, s, 256 * n, B, 256 * n);
-        launch(k_items<body_gather>, s, kQuartsPerChunk * n, B, kQuartsPerChunk * n);
-        ck(cudaEventRecord(ev[5], s), "event");
-        ck(cudaGetLastError(), "kernel launch");
+        launch(k_items<body_sg_insert, kGrid>, s, kGrid * nmax, B);
+        launch(k_items<body_sg_resolve, kGrid>, s, kGrid * nmax, B);
+        launch(k_dyn<body_surface_level, 1>, s, 2 * nmax * 100, B, cnt_s);
+        launch(k_items<body_aquifer_cell, kAqCells>, s, kAqCells * nmax, B);
+        launch(k_items<body_aquifer_skip, 1>, s, nmax, B);
+        mark(3);
+        launch(k_init_heights, s, 256 * nmax, B);
+        launch(k_items<body_fill, 256 * kCellsY, TB_MINB_FILL>, s, 256L * kCellsY * nmax, B);
+        if (aquifer_dev)
+            ck(cudaMemcpyAsync(aquifer_dev, B.blocks, sizeof(uint16_t) * static_cast<size_t>(max_batch) * kBlocksPerChunk, cudaMemcpyDeviceToDevice, s),
+               "d2d");
+        mark(4);
+        launch(k_items<body_surface1, 256>, s, 256 * nmax, B);
+        launch(k_items<body_surface_walk, 256>, s, 256 * nmax, B);
+        launch(k_items<body_surface_rules, kBlocksPerChunk, TB_MINB_SURFACE2>, s, static_cast<long>(kBlocksPerChunk) * nmax, B);
+        launch(k_items<body_surface_frozen, 256>, s, 256 * nmax, B);
+        launch(k_items<body_gather, kQuartsPerChunk>, s, static_cast<long>(kQuartsPerChunk) * nmax, B);
+        mark(5);
+    }
+
+    void add_stage_times(tg_timing* t) {
+        ck(cudaEventSynchronize(ev[5]), "sync");
+        float ms[5];
+        for (int i = 0; i < 5; ++i) ck(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]), "elapsed");
+        t->biome_ms += ms[0];
+        t->noise_ms += ms[1];
+        t->aquifer_ms += ms[2];
+        t->fill_ms += ms[3];
+        t->surface_ms += ms[4];
+        t->kernel_ms += ms[0] + ms[1] + ms[2] + ms[3] + ms[4];
+        t->batches += 1;
+    }
+
+    // Runs one batch whose staged coordinates sit in o.coords into output slot o.
+    void run_batch(OutSlot& o, int n, tg_timing* t, bool want_aquifer) {
+        cudaStream_t s = stream;
+        if (o.busy) ck(cudaStreamWaitEvent(s, o.drained, 0), "wait");   // the slot's previous outputs are copied out
+        const int32_t* h = o.coords.as<int32_t>();
+        ck(cudaMemcpyAsync(d_cx.p, h, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(d_cz.p, h + max_batch, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(d_cs.p, h + 2 * max_batch, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
+        if (want_aquifer && !o.aquifer.p) o.aquifer.alloc(sizeof(uint16_t) * static_cast<size_t>(max_batch) * kBlocksPerChunk);
+        const Batch B = batch_view(&o);
+        uint16_t* aq = want_aquifer ? o.aquifer.as<uint16_t>() : nullptr;
         if (t) {
-            ck(cudaEventSynchronize(ev[5]), "sync");
-            float ms[5];
-            for (int i = 0; i < 5; ++i) ck(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]), "elapsed");
-            t->biome_ms += ms[0];
-            t->noise_ms += ms[1];
-            t->aquifer_ms += ms[2];
-            t->fill_ms += ms[3];
-            t->surface_ms += ms[4];
-            t->kernel_ms += ms[0] + ms[1] + ms[2] + ms[3] + ms[4];
-            t->batches += 1;
-            t->launches = g_launches;
+            enqueue_batch(B, s, max_batch, aq, true);
+            add_stage_times(t);
+        } else if (use_graphs) {
+            if (!o.graph || o.graph_aquifer != want_aquifer || o.graph_stream != s) {
+                if (o.graph) cudaGraphExecDestroy(o.graph);
+                o.graph = nullptr;
+                cudaGraph_t g;
+                ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
+                const int before = g_launches;
+                enqueue_batch(B, s, max_batch, aq, false);
+                ck(cudaStreamEndCapture(s, &g), "capture");
+                ck(cudaGraphInstantiate(&o.graph, g, 0), "graph instantiate");
+                cudaGraphDestroy(g);
+                graph_launches = g_launches - before;
+                g_launches = before;
+                o.graph_aquifer = want_aquifer;
+                o.graph_stream = s;
+            }
+            ck(cudaGraphLaunch(o.graph, s), "graph launch");
+            g_launches += graph_launches;
+        } else {
+            enqueue_batch(B, s, max_batch, aq, false);
         }
+        ck(cudaGetLastError(), "kernel launch");
+        ck(cudaEventRecord(o.computed, s), "event");
+    }
+
+    void stage(OutSlot& o, int n, const int32_t* cx, const int32_t* cz, const int32_t* cs) {
+        if (o.busy) ck(cudaEventSynchronize(o.computed), "sync");   // the slot's staged coordinates were consumed
+        int32_t* h = o.coords.as<int32_t>();
+        std::memcpy(h, cx, 4 * static_cast<size_t>(n));
+        std::memcpy(h + max_batch, cz, 4 * static_cast<size_t>(n));
+        std::memcpy(h + 2 * max_batch, cs, 4 * static_cast<size_t>(n));
+        h[3 * max_batch] = n;
     }
 
     void check_chunks(const tg_chunk_xz* c, int n) {
@@ -437,46 +545,87 @@ struct Generator {
             if (c[i].x <= -lim || c[i].x >= lim || c[i].z <= -lim || c[i].z >= lim) throw Error(TG_ERR_RANGE, "chunk coordinate outside |c| < 2^23");
     }
 
+    struct Piece {
+        uint16_t* blocks;
+        uint8_t* biomes;
+        uint16_t* aquifer;
+        int first, count;      // position in the batch
+    };
+
+    // copies of a computed batch to host buffers, on the copy stream
+    void drain(OutSlot& o, const std::vector<Piece>& pieces) {
+        ck(cudaStreamWaitEvent(copy_stream, o.computed, 0), "wait");
+        for (const Piece& p : pieces) {
+            ck(cudaMemcpyAsync(p.blocks, o.blocks.as<uint16_t>() + static_cast<size_t>(p.first) * kBlocksPerChunk,
+                               sizeof(uint16_t) * p.count * kBlocksPerChunk, cudaMemcpyDeviceToHost, copy_stream),
+               "d2h");
+            if (p.biomes)
+                ck(cudaMemcpyAsync(p.biomes, o.biomes.as<uint8_t>() + static_cast<size_t>(p.first) * kQuartsPerChunk,
+                                   static_cast<size_t>(p.count) * kQuartsPerChunk, cudaMemcpyDeviceToHost, copy_stream),
+                   "d2h");
+            if (p.aquifer)
+                ck(cudaMemcpyAsync(p.aquifer, o.aquifer.as<uint16_t>() + static_cast<size_t>(p.first) * kBlocksPerChunk,
+                                   sizeof(uint16_t) * p.count * kBlocksPerChunk, cudaMemcpyDeviceToHost, copy_stream),
+                   "d2h");
+        }
+        ck(cudaEventRecord(o.drained, copy_stream), "event");
+        o.busy = true;
+    }
+
+    void finish() {
+        for (auto& o : out)
+            if (o.busy) {
+                ck(cudaEventSynchronize(o.drained), "sync");
+                o.busy = false;
+            }
+        ck(cudaStreamSynchronize(stream), "sync");
+    }
+
     void generate(const tg_chunk_xz* chunks, int count, uint16_t* blocks, uint8_t* biomes, uint16_t* aquifer, tg_timing* t) {
         if (current_slot < 0) throw Error(TG_ERR_NO_SEED, "tg_set_seed has not been called");
         check_chunks(chunks, count);
+        std::vector<int32_t> cx(max_batch), cz(max_batch), cs(max_batch, current_slot);
         for (int off = 0; off < count; off += max_batch) {
             const int n = std::min(max_batch, count - off);
-            std::memcpy(h_chunks, chunks + off, sizeof(tg_chunk_xz) * n);
-            ck(cudaMemcpyAsync(d_chunks.p, h_chunks, sizeof(tg_chunk_xz) * n, cudaMemcpyHostToDevice, stream), "h2d");
-            launch(k_split_chunks, stream, n, d_chunks.as<tg_chunk_xz>(), n, static_cast<int32_t>(current_slot), d_cx.as<int32_t>(), d_cz.as<int32_t>(),
-                   d_cs.as<int32_t>());
-            run_batch(n, t);
-            if (aquifer) throw Error(TG_ERR_INVALID_ARGUMENT, "aquifer_out is not supported yet");
-            ck(cudaMemcpyAsync(blocks + static_cast<size_t>(off) * kBlocksPerChunk, d_blocks.p, sizeof(uint16_t) * n * kBlocksPerChunk,
-                               cudaMemcpyDeviceToHost, stream),
-               "d2h");
-            if (biomes)
-                ck(cudaMemcpyAsync(biomes + static_cast<size_t>(off) * kQuartsPerChunk, d_biomes.p, static_cast<size_t>(n) * kQuartsPerChunk,
-                                   cudaMemcpyDeviceToHost, stream),
-                   "d2h");
-            ck(cudaStreamSynchronize(stream), "sync");
+            for (int i = 0; i < n; ++i) {
+                cx[i] = chunks[off + i].x;
+                cz[i] = chunks[off + i].z;
+            }
+            OutSlot& o = out[next_out];
+            next_out ^= 1;
+            stage(o, n, cx.data(), cz.data(), cs.data());
+            run_batch(o, n, t, aquifer != nullptr);
+            drain(o, {Piece{blocks + static_cast<size_t>(off) * kBlocksPerChunk, biomes ? biomes + static_cast<size_t>(off) * kQuartsPerChunk : nullptr,
+                            aquifer ? aquifer + static_cast<size_t>(off) * kBlocksPerChunk : nullptr, 0, n}});
         }
+        finish();
     }
 
     void generate_device(const tg_chunk_xz* chunks_dev, int count, uint16_t* blocks_dev, uint8_t* biomes_dev, tg_timing* t) {
         if (current_slot < 0) throw Error(TG_ERR_NO_SEED, "tg_set_seed has not been called");
         if (count > max_batch) throw Error(TG_ERR_INVALID_ARGUMENT, "count exceeds max_batch_chunks");
-        launch(k_split_chunks, stream, count, chunks_dev, count, static_cast<int32_t>(current_slot), d_cx.as<int32_t>(), d_cz.as<int32_t>(),
-               d_cs.as<int32_t>());
-        run_batch(count, t);
-        ck(cudaMemcpyAsync(blocks_dev, d_blocks.p, sizeof(uint16_t) * count * kBlocksPerChunk, cudaMemcpyDeviceToDevice, stream), "d2d");
-        if (biomes_dev) ck(cudaMemcpyAsync(biomes_dev, d_biomes.p, static_cast<size_t>(count) * kQuartsPerChunk, cudaMemcpyDeviceToDevice, stream), "d2d");
-        ck(cudaStreamSynchronize(stream), "sync");
+        finish();
+        OutSlot& o = out[0];
+        cudaStream_t s = stream;
+        launch(k_split_chunks, s, count, chunks_dev, count, static_cast<int32_t>(current_slot), d_cx.as<int32_t>(), d_cz.as<int32_t>(), d_cs.as<int32_t>(),
+               d_n.as<int32_t>());
+        const Batch B = batch_view(&o);
+        enqueue_batch(B, s, max_batch, nullptr, t != nullptr);
+        if (t) add_stage_times(t);
+        ck(cudaMemcpyAsync(blocks_dev, o.blocks.p, sizeof(uint16_t) * count * kBlocksPerChunk, cudaMemcpyDeviceToDevice, s), "d2d");
+        if (biomes_dev) ck(cudaMemcpyAsync(biomes_dev, o.biomes.p, static_cast<size_t>(count) * kQuartsPerChunk, cudaMemcpyDeviceToDevice, s), "d2d");
+        ck(cudaGetLastError(), "kernel launch");
+        ck(cudaStreamSynchronize(s), "sync");
     }
 
-    void biome_lookup(const int64_t* seeds, const int32_t* xyz, int n, uint8_t* out) {
-        std::vector<int32_t> cx, cz, cs, pos;
+    void biome_lookup(const int64_t* seeds, const int32_t* xyz, int n, uint8_t* res) {
+        std::vector<int32_t> cx(max_batch), cz(max_batch), cs(max_batch);
+        DevBuf d_xyz, d_res;
+        d_xyz.alloc(sizeof(int32_t) * 3 * max_batch);
+        d_res.alloc(max_batch);
+        finish();
         for (int off = 0; off < n; off += max_batch) {
             const int m = std::min(max_batch, n - off);
-            cx.resize(m);
-            cz.resize(m);
-            cs.resize(m);
             std::vector<int> used;
             for (int i = 0; i < m; ++i) {
                 const int32_t* p = xyz + 3 * (off + i);
@@ -484,52 +633,42 @@ struct Generator {
                 cz[i] = p[2] >> 4;
                 if (cx[i] <= -(1 << 23) || cx[i] >= (1 << 23) || cz[i] <= -(1 << 23) || cz[i] >= (1 << 23)) throw Error(TG_ERR_RANGE, "position out of range");
                 cs[i] = seed_slot(seeds[off + i], used);
-                used.push_back(cs[i]);
+                if (std::find(used.begin(), used.end(), cs[i]) == used.end()) used.push_back(cs[i]);
             }
-            DevBuf d_xyz, d_out;
-            d_xyz.alloc(sizeof(int32_t) * 3 * m);
-            d_out.alloc(m);
-            ck(cudaMemcpyAsync(d_xyz.p, xyz + 3 * off, sizeof(int32_t) * 3 * m, cudaMemcpyHostToDevice, stream), "h2d");
-            ck(cudaMemcpyAsync(d_cx.p, cx.data(), 4 * m, cudaMemcpyHostToDevice, stream), "h2d");
-            ck(cudaMemcpyAsync(d_cz.p, cz.data(), 4 * m, cudaMemcpyHostToDevice, stream), "h2d");
-            ck(cudaMemcpyAsync(d_cs.p, cs.data(), 4 * m, cudaMemcpyHostToDevice, stream), "h2d");
-            const Batch B = batch_view(m);
-            run_biomes(B, m);
-            launch(k_biome_lookup, stream, m, B, d_xyz.as<int32_t>(), d_out.as<uint8_t>(), m);
-            ck(cudaMemcpyAsync(out + off, d_out.p, m, cudaMemcpyDeviceToHost, stream), "d2h");
-            ck(cudaStreamSynchronize(stream), "sync");
+            OutSlot& o = out[0];
+            stage(o, m, cx.data(), cz.data(), cs.data());
+            const int32_t* h = o.coords.as<int32_t>();
+            cudaStream_t s = stream;
+            ck(cudaMemcpyAsync(d_cx.p, h, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
+            ck(cudaMemcpyAsync(d_cz.p, h + max_batch, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
+            ck(cudaMemcpyAsync(d_cs.p, h + 2 * max_batch, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
+            ck(cudaMemcpyAsync(d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
+            ck(cudaMemcpyAsync(d_xyz.p, xyz + 3 * off, sizeof(int32_t) * 3 * m, cudaMemcpyHostToDevice, s), "h2d");
+            const Batch B = batch_view(nullptr);
+            enqueue_biomes(B, s, m);
+            launch(k_biome_lookup, s, m, B, d_xyz.as<int32_t>(), d_res.as<uint8_t>());
+            ck(cudaMemcpyAsync(res + off, d_res.p, m, cudaMemcpyDeviceToHost, s), "d2h");
+            ck(cudaStreamSynchronize(s), "sync");
         }
     }
 
+    // Multi-seed batch: requests are cut into device batches; a batch mixes seeds.
     void generate_batch(const tg_request* req, int n, tg_timing* t) {
-        // flatten requests into device batches; each request's seed gets a resident slot
+        for (int r = 0; r < n; ++r) {
+            if (req[r].count < 0 || (req[r].count > 0 && (!req[r].chunks || !req[r].blocks_out))) throw Error(TG_ERR_INVALID_ARGUMENT, "bad request");
+            check_chunks(req[r].chunks, req[r].count);
+        }
         std::vector<int32_t> cx, cz, cs;
-        struct Piece {
-            int req, first, count;
-        };
         std::vector<Piece> pieces;
         std::vector<int> used;
         auto flush = [&]() {
             const int m = static_cast<int>(cx.size());
             if (!m) return;
-            ck(cudaMemcpyAsync(d_cx.p, cx.data(), 4 * m, cudaMemcpyHostToDevice, stream), "h2d");
-            ck(cudaMemcpyAsync(d_cz.p, cz.data(), 4 * m, cudaMemcpyHostToDevice, stream), "h2d");
-            ck(cudaMemcpyAsync(d_cs.p, cs.data(), 4 * m, cudaMemcpyHostToDevice, stream), "h2d");
-            run_batch(m, t);
-            int at = 0;
-            for (const Piece& p : pieces) {
-                ck(cudaMemcpyAsync(req[p.req].blocks_out + static_cast<size_t>(p.first) * kBlocksPerChunk,
-                                   d_blocks.as<uint16_t>() + static_cast<size_t>(at) * kBlocksPerChunk, sizeof(uint16_t) * p.count * kBlocksPerChunk,
-                                   cudaMemcpyDeviceToHost, stream),
-                   "d2h");
-                if (req[p.req].biomes_out)
-                    ck(cudaMemcpyAsync(req[p.req].biomes_out + static_cast<size_t>(p.first) * kQuartsPerChunk,
-                                       d_biomes.as<uint8_t>() + static_cast<size_t>(at) * kQuartsPerChunk, static_cast<size_t>(p.count) * kQuartsPerChunk,
-                                       cudaMemcpyDeviceToHost, stream),
-                       "d2h");
-                at += p.count;
-            }
-            ck(cudaStreamSynchronize(stream), "sync");
+            OutSlot& o = out[next_out];
+            next_out ^= 1;
+            stage(o, m, cx.data(), cz.data(), cs.data());
+            run_batch(o, m, t, false);
+            drain(o, pieces);
             cx.clear();
             cz.clear();
             cs.clear();
@@ -537,15 +676,15 @@ struct Generator {
             used.clear();
         };
         for (int r = 0; r < n; ++r) {
-            if (!req[r].chunks || !req[r].blocks_out || req[r].count < 0) throw Error(TG_ERR_INVALID_ARGUMENT, "bad request");
-            check_chunks(req[r].chunks, req[r].count);
             int done = 0;
             while (done < req[r].count) {
-                if (static_cast<int>(cx.size()) == max_batch || static_cast<int>(used.size()) >= kMaxSlots) flush();
+                if (static_cast<int>(cx.size()) == max_batch) flush();
                 const int slot = seed_slot(req[r].seed, used);
                 if (std::find(used.begin(), used.end(), slot) == used.end()) used.push_back(slot);
                 const int take = std::min(req[r].count - done, max_batch - static_cast<int>(cx.size()));
-                pieces.push_back({r, done, take});
+                pieces.push_back(Piece{req[r].blocks_out + static_cast<size_t>(done) * kBlocksPerChunk,
+                                       req[r].biomes_out ? req[r].biomes_out + static_cast<size_t>(done) * kQuartsPerChunk : nullptr, nullptr,
+                                       static_cast<int>(cx.size()), take});
                 for (int i = 0; i < take; ++i) {
                     cx.push_back(req[r].chunks[done + i].x);
                     cz.push_back(req[r].chunks[done + i].z);
@@ -555,8 +694,257 @@ struct Generator {
             }
         }
         flush();
+        finish();
     }
 };
+
+// ---- continuous-batching server ---------------------------------------------------------------------
+// A worker thread owns the generator. Requests (seed, chunk list, host output buffers)
+// queue on submit; the worker admits them into an active set while the chunks in flight
+// stay within the HBM-derived limit, cuts device batches across all active requests
+// (mixing seeds and request sizes), and drains each batch's outputs on the copy stream
+// while the next batch computes. A request completes when its last chunk is copied out.
+struct Server {
+    struct Req {
+        uint64_t id = 0;
+        int64_t seed = 0;
+        std::vector<tg_chunk_xz> chunks;
+        uint16_t* blocks = nullptr;
+        uint8_t* biomes = nullptr;
+        int issued = 0, finished = 0;
+        double t_submit = 0, t_done = 0;
+        bool complete = false;
+        int slot = -1;
+    };
+    struct InFlight {
+        int out = 0;
+        std::vector<std::pair<Req*, int>> parts;   // request, chunks
+    };
+
+    Generator* g;
+    int batch_chunks;
+    long max_active_chunks;
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Req*> queue;
+    std::vector<Req*> active;
+    std::unordered_map<uint64_t, std::unique_ptr<Req>> reqs;
+    uint64_t next_id = 1;
+    bool stop = false;
+    tg_status failure = TG_OK;
+    std::string failure_msg;
+    // statistics
+    std::vector<double> lat;
+    long chunks_done = 0;
+    double t_first = -1, t_last = 0;
+    int batches = 0;
+
+    Server(Generator* gen, const tg_server_config* cfg) : g(gen) {
+        batch_chunks = cfg && cfg->batch_chunks > 0 ? std::min(cfg->batch_chunks, g->max_batch) : g->max_batch;
+        const double per_chunk = static_cast<double>(kBlocksPerChunk) * 2 + kQuartsPerChunk;
+        const long budget_chunks = cfg && cfg->hbm_budget_bytes > 0 ? static_cast<long>(static_cast<double>(cfg->hbm_budget_bytes) / per_chunk) : 8L * g->max_batch;
+        max_active_chunks = std::max<long>(batch_chunks, budget_chunks);
+        g->served = true;
+        worker = std::thread([this] { run(); });
+    }
+    ~Server() {
+        {
+            std::lock_guard<std::mutex> l(mu);
+            stop = true;
+        }
+        cv_work.notify_all();
+        if (worker.joinable()) worker.join();
+        g->served = false;
+    }
+
+    uint64_t submit(int64_t seed, const tg_chunk_xz* chunks, int count, uint16_t* blocks, uint8_t* biomes) {
+        g->check_chunks(chunks, count);
+        auto r = std::make_unique<Req>();
+        r->seed = seed;
+        r->chunks.assign(chunks, chunks + count);
+        r->blocks = blocks;
+        r->biomes = biomes;
+        r->t_submit = now_ms();
+        std::lock_guard<std::mutex> l(mu);
+        if (failure != TG_OK) throw Error(failure, failure_msg);
+        r->id = next_id++;
+        const uint64_t id = r->id;
+        if (t_first < 0) t_first = r->t_submit;
+        if (count == 0) {
+            r->complete = true;
+            r->t_done = r->t_submit;
+        } else {
+            queue.push_back(r.get());
+        }
+        reqs.emplace(id, std::move(r));
+        cv_work.notify_one();
+        return id;
+    }
+
+    // 1 = done (the ticket is released), 0 = pending
+    int poll(uint64_t id, int wait_ms) {
+        std::unique_lock<std::mutex> l(mu);
+        auto it = reqs.find(id);
+        if (it == reqs.end()) throw Error(TG_ERR_INVALID_ARGUMENT, "unknown ticket");
+        Req* r = it->second.get();
+        auto pred = [&] { return r->complete || failure != TG_OK; };
+        if (wait_ms < 0) cv_done.wait(l, pred);
+        else if (wait_ms > 0) cv_done.wait_for(l, std::chrono::milliseconds(wait_ms), pred);
+        if (failure != TG_OK && !r->complete) throw Error(failure, failure_msg);
+        if (!r->complete) return 0;
+        reqs.erase(it);
+        return 1;
+    }
+
+    void stats(tg_server_stats* s) {
+        std::lock_guard<std::mutex> l(mu);
+        std::memset(s, 0, sizeof *s);
+        s->completed_requests = static_cast<int64_t>(lat.size());
+        s->completed_chunks = chunks_done;
+        s->batches = batches;
+        if (!lat.empty()) {
+            std::vector<double> v = lat;
+            std::sort(v.begin(), v.end());
+            auto pct = [&](double q) { return v[std::min(v.size() - 1, static_cast<size_t>(q * static_cast<double>(v.size() - 1) + 0.5))]; };
+            s->p50_ms = pct(0.50);
+            s->p99_ms = pct(0.99);
+            s->max_ms = v.back();
+            double sum = 0;
+            for (double x : v) sum += x;
+            s->mean_ms = sum / static_cast<double>(v.size());
+        }
+        if (t_first >= 0 && t_last > t_first) s->chunks_per_s = static_cast<double>(chunks_done) / ((t_last - t_first) / 1000.0);
+        s->queued_requests = static_cast<int32_t>(queue.size());
+        s->active_requests = static_cast<int32_t>(active.size());
+    }
+
+    void reset_stats() {
+        std::lock_guard<std::mutex> l(mu);
+        lat.clear();
+        chunks_done = 0;
+        t_first = -1;
+        t_last = 0;
+        batches = 0;
+    }
+
+    void complete_batch(InFlight& f) {
+        ck(cudaEventSynchronize(g->out[f.out].drained), "sync");
+        g->out[f.out].busy = false;
+        const double t = now_ms();
+        std::lock_guard<std::mutex> l(mu);
+        for (auto& part : f.parts) {
+            Req* r = part.first;
+            r->finished += part.second;
+            chunks_done += part.second;
+            if (r->finished == static_cast<int>(r->chunks.size())) {
+                r->complete = true;
+                r->t_done = t;
+                lat.push_back(t - r->t_submit);
+                active.erase(std::find(active.begin(), active.end(), r));
+            }
+        }
+        t_last = t;
+        ++batches;
+        cv_done.notify_all();
+    }
+
+    void run() {
+        try {
+            ck(cudaSetDevice(g->device), "cudaSetDevice");
+            std::deque<InFlight> flight;
+            std::vector<int32_t> cx(g->max_batch), cz(g->max_batch), cs(g->max_batch);
+            for (;;) {
+                std::vector<Req*> admitted;
+                {
+                    std::unique_lock<std::mutex> l(mu);
+                    cv_work.wait(l, [&] { return stop || !queue.empty() || !flight.empty() || !active.empty(); });
+                    if (stop && flight.empty()) break;
+                    // admission: chunks still to issue across the active set stay within the limit
+                    long pending = 0;
+                    for (Req* r : active) pending += static_cast<long>(r->chunks.size()) - r->issued;
+                    while (!queue.empty() && (active.empty() || pending + static_cast<long>(queue.front()->chunks.size()) <= max_active_chunks)) {
+                        Req* r = queue.front();
+                        queue.pop_front();
+                        active.push_back(r);
+                        admitted.push_back(r);
+                        pending += static_cast<long>(r->chunks.size());
+                    }
+                }
+                // per-seed tables stay resident; none is evicted while an active request uses it
+                if (!admitted.empty()) {
+                    std::vector<int> keep;
+                    {
+                        std::lock_guard<std::mutex> l(mu);
+                        for (Req* r : active)
+                            if (r->slot >= 0) keep.push_back(r->slot);
+                    }
+                    for (Req* r : admitted) {
+                        const int slot = g->seed_slot(r->seed, keep);
+                        keep.push_back(slot);
+                        std::lock_guard<std::mutex> l(mu);
+                        r->slot = slot;
+                    }
+                }
+                // cut one batch across the active requests, oldest first
+                InFlight f;
+                int n = 0;
+                std::vector<Generator::Piece> pieces;
+                {
+                    std::lock_guard<std::mutex> l(mu);
+                    for (Req* r : active) {
+                        if (n == batch_chunks) break;
+                        const int left = static_cast<int>(r->chunks.size()) - r->issued;
+                        if (left <= 0 || r->slot < 0) continue;
+                        const int take = std::min(left, batch_chunks - n);
+                        for (int i = 0; i < take; ++i) {
+                            cx[n + i] = r->chunks[r->issued + i].x;
+                            cz[n + i] = r->chunks[r->issued + i].z;
+                            cs[n + i] = r->slot;
+                        }
+                        pieces.push_back(Generator::Piece{r->blocks + static_cast<size_t>(r->issued) * kBlocksPerChunk,
+                                                          r->biomes ? r->biomes + static_cast<size_t>(r->issued) * kQuartsPerChunk : nullptr, nullptr, n, take});
+                        f.parts.push_back({r, take});
+                        r->issued += take;
+                        n += take;
+                    }
+                }
+                if (n > 0) {
+                    const int oi = g->next_out;
+                    g->next_out ^= 1;
+                    OutSlot& o = g->out[oi];
+                    if (o.busy) {
+                        // the slot's previous batch completes before its buffers are reused
+                        complete_batch(flight.front());
+                        flight.pop_front();
+                    }
+                    g->stage(o, n, cx.data(), cz.data(), cs.data());
+                    g->run_batch(o, n, nullptr, false);
+                    g->drain(o, pieces);
+                    f.out = oi;
+                    flight.push_back(std::move(f));
+                    continue;
+                }
+                if (!flight.empty()) {
+                    complete_batch(flight.front());
+                    flight.pop_front();
+                }
+            }
+        } catch (const Error& e) {
+            std::lock_guard<std::mutex> l(mu);
+            failure = e.code;
+            failure_msg = e.what();
+            cv_done.notify_all();
+        } catch (const std::exception& e) {
+            std::lock_guard<std::mutex> l(mu);
+            failure = TG_ERR_INTERNAL;
+            failure_msg = e.what();
+            cv_done.notify_all();
+        }
+    }
+};
+
+namespace {
 
 std::string read_file(const char* path) {
     std::ifstream f(path, std::ios::binary);
@@ -584,11 +972,24 @@ tg_status guarded(F&& f) {
     }
 }
 
+}  // namespace
 }  // namespace tb
 
 struct tg_generator {
     std::unique_ptr<tb::Generator> g;
 };
+
+struct tg_server {
+    std::unique_ptr<tb::Server> s;
+};
+
+namespace {
+void usable(tg_generator* gen) {
+    if (!gen) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "gen is null");
+    if (gen->g->served) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "the generator is owned by a server");
+    tb::ck(cudaSetDevice(gen->g->device), "cudaSetDevice");
+}
+}  // namespace
 
 extern "C" {
 
@@ -600,35 +1001,34 @@ tg_status tg_create(const char* ir_json_path, const char* terrain_json_path, con
             throw tb::Error(TG_ERR_MODEL_MISMATCH, "IR file differs from the compiled model");
         if (terrain_json_path && tb::sha256_hex(tb::read_file(terrain_json_path)) != tbm::kModelTerrainSha256)
             throw tb::Error(TG_ERR_MODEL_MISMATCH, "terrain model file differs from the compiled model");
-        int batch = config && config->max_batch_chunks > 0 ? config->max_batch_chunks : 2048;
+        const int batch = config && config->max_batch_chunks > 0 ? config->max_batch_chunks : 2048;
         if (batch > (1 << 16)) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "max_batch_chunks too large");
+        if (config && (config->pipeline_slots < 0 || config->pipeline_slots > 2)) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "pipeline_slots must be 0, 1 or 2");
         const int dev = config ? config->device : 0;
-        auto* h = new tg_generator;
-        try {
-            h->g = std::make_unique<tb::Generator>(dev, batch);
-        } catch (...) {
-            delete h;
-            throw;
-        }
-        *out = h;
+        auto h = std::make_unique<tg_generator>();
+        h->g = std::make_unique<tb::Generator>(dev, batch);
+        *out = h.release();
     });
 }
 
 tg_status tg_destroy(tg_generator* gen) {
-    return tb::guarded([&] { delete gen; });
+    return tb::guarded([&] {
+        if (gen && gen->g->served) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "destroy the server first");
+        delete gen;
+    });
 }
 
 tg_status tg_set_stream(tg_generator* gen, void* cuda_stream) {
     return tb::guarded([&] {
-        if (!gen) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "gen is null");
+        usable(gen);
+        gen->g->finish();
         gen->g->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : gen->g->own_stream;
     });
 }
 
 tg_status tg_set_seed(tg_generator* gen, int64_t seed) {
     return tb::guarded([&] {
-        if (!gen) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "gen is null");
-        tb::ck(cudaSetDevice(gen->g->device), "cudaSetDevice");
+        usable(gen);
         gen->g->current_slot = gen->g->seed_slot(seed);
     });
 }
@@ -636,21 +1036,23 @@ tg_status tg_set_seed(tg_generator* gen, int64_t seed) {
 tg_status tg_generate(tg_generator* gen, const tg_chunk_xz* chunks, int32_t count, uint16_t* blocks_out, uint8_t* biomes_out, uint16_t* aquifer_out,
                       tg_timing* timing) {
     return tb::guarded([&] {
-        if (!gen || (count > 0 && (!chunks || !blocks_out)) || count < 0) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
-        tb::ck(cudaSetDevice(gen->g->device), "cudaSetDevice");
+        usable(gen);
+        if ((count > 0 && (!chunks || !blocks_out)) || count < 0) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
         const auto t0 = std::chrono::steady_clock::now();
         if (timing) std::memset(timing, 0, sizeof *timing);
         tb::g_launches = 0;
         gen->g->generate(chunks, count, blocks_out, biomes_out, aquifer_out, timing);
-        if (timing) timing->launches = tb::g_launches;
-        if (timing) timing->wall_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (timing) {
+            timing->launches = tb::g_launches;
+            timing->wall_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
     });
 }
 
 tg_status tg_generate_device(tg_generator* gen, const tg_chunk_xz* chunks_dev, int32_t count, uint16_t* blocks_dev, uint8_t* biomes_dev, tg_timing* timing) {
     return tb::guarded([&] {
-        if (!gen || count <= 0 || !chunks_dev || !blocks_dev) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
-        tb::ck(cudaSetDevice(gen->g->device), "cudaSetDevice");
+        usable(gen);
+        if (count <= 0 || !chunks_dev || !blocks_dev) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
         if (timing) std::memset(timing, 0, sizeof *timing);
         tb::g_launches = 0;
         gen->g->generate_device(chunks_dev, count, blocks_dev, biomes_dev, timing);
@@ -660,23 +1062,69 @@ tg_status tg_generate_device(tg_generator* gen, const tg_chunk_xz* chunks_dev, i
 
 tg_status tg_generate_batch(tg_generator* gen, const tg_request* requests, int32_t n, tg_timing* timing) {
     return tb::guarded([&] {
-        if (!gen || n < 0 || (n > 0 && !requests)) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
-        tb::ck(cudaSetDevice(gen->g->device), "cudaSetDevice");
+        usable(gen);
+        if (n < 0 || (n > 0 && !requests)) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
         const auto t0 = std::chrono::steady_clock::now();
         if (timing) std::memset(timing, 0, sizeof *timing);
         tb::g_launches = 0;
         gen->g->generate_batch(requests, n, timing);
-        if (timing) timing->launches = tb::g_launches;
-        if (timing) timing->wall_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (timing) {
+            timing->launches = tb::g_launches;
+            timing->wall_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
     });
 }
 
 tg_status tg_biome_lookup(tg_generator* gen, const int64_t* seeds, const int32_t* xyz, int32_t n, uint8_t* out) {
     return tb::guarded([&] {
-        if (!gen || n < 0 || (n > 0 && (!seeds || !xyz || !out))) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
-        tb::ck(cudaSetDevice(gen->g->device), "cudaSetDevice");
+        usable(gen);
+        if (n < 0 || (n > 0 && (!seeds || !xyz || !out))) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
         gen->g->biome_lookup(seeds, xyz, n, out);
     });
+}
+
+tg_status tg_server_create(tg_generator* gen, const tg_server_config* config, tg_server** out) {
+    return tb::guarded([&] {
+        usable(gen);
+        if (!out) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "out is null");
+        gen->g->finish();
+        auto h = std::make_unique<tg_server>();
+        h->s = std::make_unique<tb::Server>(gen->g.get(), config);
+        *out = h.release();
+    });
+}
+
+tg_status tg_server_submit(tg_server* srv, int64_t seed, const tg_chunk_xz* chunks, int32_t count, uint16_t* blocks_out, uint8_t* biomes_out,
+                           uint64_t* ticket) {
+    return tb::guarded([&] {
+        if (!srv || !ticket || count < 0 || (count > 0 && (!chunks || !blocks_out))) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        *ticket = srv->s->submit(seed, chunks, count, blocks_out, biomes_out);
+    });
+}
+
+tg_status tg_server_wait(tg_server* srv, uint64_t ticket, int32_t timeout_ms, int32_t* done) {
+    return tb::guarded([&] {
+        if (!srv || !done) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        *done = srv->s->poll(ticket, timeout_ms);
+    });
+}
+
+tg_status tg_server_get_stats(tg_server* srv, tg_server_stats* stats) {
+    return tb::guarded([&] {
+        if (!srv || !stats) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        srv->s->stats(stats);
+    });
+}
+
+tg_status tg_server_reset_stats(tg_server* srv) {
+    return tb::guarded([&] {
+        if (!srv) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        srv->s->reset_stats();
+    });
+}
+
+tg_status tg_server_destroy(tg_server* srv) {
+    return tb::guarded([&] { delete srv; });
 }
 
 void* tg_alloc_pinned(size_t bytes) {

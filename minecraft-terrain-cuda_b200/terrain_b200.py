@@ -40,7 +40,21 @@ class TgRequest(ctypes.Structure):
                 ('blocks_out', ctypes.POINTER(ctypes.c_uint16)), ('biomes_out', ctypes.POINTER(ctypes.c_uint8))]
 
 
+class TgServerConfig(ctypes.Structure):
+    _fields_ = [('batch_chunks', ctypes.c_int32), ('hbm_budget_bytes', ctypes.c_int64), ('reserved', ctypes.c_int32)]
+
+
+class TgServerStats(ctypes.Structure):
+    _fields_ = [('completed_requests', ctypes.c_int64), ('completed_chunks', ctypes.c_int64)] + \
+               [(k, ctypes.c_double) for k in ('p50_ms', 'p99_ms', 'mean_ms', 'max_ms', 'chunks_per_s')] + \
+               [(k, ctypes.c_int32) for k in ('batches', 'queued_requests', 'active_requests')]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+           'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
            'tg_alloc_pinned', 'tg_free_pinned', 'tg_model_info', 'tg_last_error_string']
 
 
@@ -69,12 +83,19 @@ def load(path=LIB_PATH):
     L.tg_generate_device.argtypes = [vp, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(TgTiming)]
     L.tg_generate_batch.argtypes = [vp, ctypes.POINTER(TgRequest), ctypes.c_int32, ctypes.POINTER(TgTiming)]
     L.tg_biome_lookup.argtypes = [vp, vp, vp, ctypes.c_int32, vp]
+    L.tg_server_create.argtypes = [vp, ctypes.POINTER(TgServerConfig), ctypes.POINTER(vp)]
+    L.tg_server_submit.argtypes = [vp, ctypes.c_int64, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.tg_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    L.tg_server_get_stats.argtypes = [vp, ctypes.POINTER(TgServerStats)]
+    L.tg_server_reset_stats.argtypes = [vp]
+    L.tg_server_destroy.argtypes = [vp]
     L.tg_alloc_pinned.argtypes = [ctypes.c_size_t]
     L.tg_alloc_pinned.restype = vp
     L.tg_free_pinned.argtypes = [vp]
     L.tg_model_info.argtypes = [ctypes.POINTER(ctypes.c_int32)] * 5
     L.tg_last_error_string.restype = ctypes.c_char_p
     for f in ('tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+              'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
               'tg_model_info'):
         getattr(L, f).restype = ctypes.c_int
     _lib = L
@@ -175,3 +196,60 @@ class TerrainGenerator:
         out = np.empty(xyz.shape[0], np.uint8)
         self._check(self.L.tg_biome_lookup(self.h, _ptr(seeds), _ptr(xyz), xyz.shape[0], _ptr(out)))
         return out
+
+
+class TerrainServer:
+    """Continuous-batching server over one generator (tg_server_*).
+
+        srv = TerrainServer(gen, batch_chunks=512)
+        t = srv.submit(seed, chunks)          # returns a ticket; outputs allocated here
+        blocks, biomes = srv.wait(t)
+    """
+
+    def __init__(self, gen, batch_chunks=0, hbm_budget_bytes=0):
+        self.gen = gen
+        self.L = gen.L
+        self.h = ctypes.c_void_p()
+        cfg = TgServerConfig(batch_chunks, hbm_budget_bytes, 0)
+        gen._check(self.L.tg_server_create(gen.h, ctypes.byref(cfg), ctypes.byref(self.h)))
+        self.pending = {}
+
+    def submit(self, seed, chunks, blocks_out=None, biomes_out=None):
+        a = chunk_array(chunks)
+        n = a.shape[0]
+        g = self.gen
+        blocks = blocks_out if blocks_out is not None else np.empty((n, g.height, 16, 16), np.uint16)
+        biomes = biomes_out if biomes_out is not None else np.empty((n, g.qper), np.uint8)
+        t = ctypes.c_uint64()
+        g._check(self.L.tg_server_submit(self.h, int(seed), _ptr(a), n, _ptr(blocks), _ptr(biomes), ctypes.byref(t)))
+        self.pending[t.value] = (a, blocks, biomes)
+        return t.value
+
+    def poll(self, ticket, timeout_ms=0):
+        done = ctypes.c_int32()
+        self.gen._check(self.L.tg_server_wait(self.h, ctypes.c_uint64(ticket), int(timeout_ms), ctypes.byref(done)))
+        return bool(done.value)
+
+    def wait(self, ticket):
+        self.poll(ticket, -1)
+        _, blocks, biomes = self.pending.pop(ticket)
+        return blocks, biomes
+
+    def stats(self):
+        st = TgServerStats()
+        self.gen._check(self.L.tg_server_get_stats(self.h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self):
+        self.gen._check(self.L.tg_server_reset_stats(self.h))
+
+    def close(self):
+        if self.h:
+            self.L.tg_server_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -104,7 +104,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     Batch B{};
     B.M = R.M;
     B.seeds = &R.D;
-    B.n = n;
+    B.n_dev = &n;
     B.cx = vcx.data();
     B.cz = vcz.data();
     B.cseed = vcs.data();

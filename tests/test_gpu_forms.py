@@ -1,0 +1,110 @@
+"""GPU: the batched multi-seed form, the continuous-batching server, biome lookups,
+the aquifer-fill output and argument errors, each checked against the reference port
+or against the plain form. Integer outputs, zero tolerance.
+"""
+import numpy as np
+import pytest
+
+import terrain_b200
+
+pytestmark = pytest.mark.gpu
+
+
+def test_aquifer_output_matches_reference(gpu_gen, ref_model):
+    chunks = [(0, 0), (5, -3), (1874999, 1874999), (-4000, 1600)]
+    gpu_gen.set_seed(99)
+    blocks, biomes, aq = gpu_gen.generate(chunks, aquifer=True)
+    rb, rq, raq = ref_model.seed(99).generate(chunks, aquifer=True)
+    assert (aq == raq).all() and (blocks == rb).all() and (biomes == rq).all()
+
+
+def test_batch_mixes_seeds_and_sizes(gpu_gen, ref_model):
+    rng = np.random.default_rng(3)
+    reqs = []
+    for seed, n in [(11, 1), (-5, 7), (11, 3), (2 ** 40, 20), (-5, 2)]:
+        base = rng.integers(-50000, 50000, 2)
+        reqs.append((seed, [(int(base[0] + i % 5), int(base[1] + i // 5)) for i in range(n)]))
+    outs = gpu_gen.generate_batch(reqs)
+    for (seed, chunks), (b, q) in zip(reqs, outs):
+        rb, rq = ref_model.seed(seed).generate(chunks)
+        assert (b == rb).all() and (q == rq).all(), 'seed %d' % seed
+
+
+def test_batch_larger_than_one_device_batch(ref_model):
+    g = terrain_b200.TerrainGenerator(max_batch_chunks=8)
+    try:
+        chunks = [(x, z) for z in range(3) for x in range(5)]
+        outs = g.generate_batch([(1234, chunks), (4321, chunks[:4])])
+        rb, rq = ref_model.seed(1234).generate(chunks)
+        assert (outs[0][0] == rb).all() and (outs[0][1] == rq).all()
+        rb, rq = ref_model.seed(4321).generate(chunks[:4])
+        assert (outs[1][0] == rb).all() and (outs[1][1] == rq).all()
+        g.set_seed(1234)
+        b2, q2 = g.generate(chunks)            # the plain form splits the list the same way
+        assert (b2 == outs[0][0]).all() and (q2 == outs[0][1]).all()
+    finally:
+        g.close()
+
+
+def test_server_alone_equals_mixed(ref_model):
+    """Each served result is byte-identical alone and in a mix of concurrent requests."""
+    g = terrain_b200.TerrainGenerator(max_batch_chunks=64)
+    try:
+        rng = np.random.default_rng(7)
+        reqs = []
+        for k in range(12):
+            r = int(rng.integers(0, 3))
+            cx, cz = (int(v) for v in rng.integers(-100000, 100000, 2))
+            reqs.append((int(rng.choice([1, 2, 3])), [(cx + dx, cz + dz) for dz in range(-r, r + 1) for dx in range(-r, r + 1)]))
+        alone = []
+        for seed, chunks in reqs:
+            g.set_seed(seed)
+            alone.append(g.generate(chunks))
+        with terrain_b200.TerrainServer(g, batch_chunks=40) as srv:
+            tickets = [srv.submit(seed, chunks) for seed, chunks in reqs]
+            mixed = [srv.wait(t) for t in tickets]
+            st = srv.stats()
+        assert st['completed_requests'] == len(reqs)
+        for (a_b, a_q), (m_b, m_q) in zip(alone, mixed):
+            assert (a_b == m_b).all() and (a_q == m_q).all()
+        seed, chunks = reqs[0]
+        rb, rq = ref_model.seed(seed).generate(chunks)
+        assert (mixed[0][0] == rb).all() and (mixed[0][1] == rq).all()
+    finally:
+        g.close()
+
+
+def test_biome_lookup_matches_reference(gpu_gen, ref_model):
+    rng = np.random.default_rng(5)
+    n = 3000
+    xyz = np.stack([rng.integers(-1874999, 1874999, n), rng.integers(-64, 320, n), rng.integers(-1874999, 1874999, n)], 1).astype(np.int32)
+    seeds = rng.choice(np.array([0, 77, -3, 2 ** 62], np.int64), n)
+    got = gpu_gen.biome_lookup(seeds, xyz)
+    for s in np.unique(seeds):
+        sel = seeds == s
+        want = ref_model.seed(int(s)).biome_lookup(xyz[sel])
+        assert (got[sel] == want).all(), 'seed %d' % s
+
+
+def test_errors_are_status_codes(gpu_gen):
+    with pytest.raises(terrain_b200.TerrainError) as e:
+        gpu_gen.generate([(1 << 23, 0)])
+    assert e.value.status == 5
+    g = terrain_b200.TerrainGenerator(max_batch_chunks=4)
+    try:
+        with pytest.raises(terrain_b200.TerrainError) as e:
+            g.generate([(0, 0)])
+        assert e.value.status == 6
+    finally:
+        g.close()
+    with pytest.raises(terrain_b200.TerrainError) as e:
+        terrain_b200.TerrainGenerator(max_batch_chunks=4, ir_path=__file__)
+    assert e.value.status == 2
+
+
+def test_repeatable(gpu_gen):
+    gpu_gen.set_seed(31337)
+    chunks = [(x, 0) for x in range(6)]
+    a = gpu_gen.generate(chunks)
+    b = gpu_gen.generate(chunks[::-1])
+    assert (a[0] == b[0][::-1]).all() and (a[1] == b[1][::-1]).all()
