@@ -156,6 +156,17 @@ def run_reference(args, rank):
     print(json.dumps(line))
 
 
+def max_over_ranks(value, world, device=None):
+    """The step time every rank reports: the maximum over ranks (all_reduce MAX)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], device=device) if device is not None else torch.tensor([float(value)])
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def serving_requests(n, rng):
     """View-distance requests: a (2r+1)^2 square or the ring of radius r (r in 2..12) around a
     uniform centre within +/-117,187 chunks; seeds from a pool of 64."""
@@ -294,12 +305,7 @@ def run_ours(args, rank, world, local_rank):
     ms = e0.elapsed_time(e1)
     barrier()
     torch.cuda.synchronize()
-    ms_max = ms
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, 'cuda')
     chunks_total = n * nreg * args.steps * world
     value = chunks_total / (ms_max / 1000.0)
 
@@ -322,12 +328,7 @@ def run_ours(args, rank, world, local_rank):
         step_e2e()
     e3.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e2.elapsed_time(e3)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms_e2e], device='cuda')
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3), world, 'cuda')
     e2e_value = chunks_total / (ms_e2e / 1000.0)
 
     if rank != 0:

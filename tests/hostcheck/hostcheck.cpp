@@ -303,3 +303,34 @@ int hc_tree_info(int32_t* out3) {
     return 0;
 }
 }
+
+extern "C" {
+// Java-semantics helpers and random sources of the product, for known-answer tests.
+int32_t hc_d2i(double v) { return d2i(v); }
+int32_t hc_jfloor(double v) { return jfloor(v); }
+int32_t hc_fdiv(int32_t a, int32_t b) { return fdiv(a, b); }
+int32_t hc_fmod(int32_t a, int32_t b) { return fmod_i(a, b); }
+float hc_jmin(float a, float b) { return jmin(a, b); }
+float hc_jmax(float a, float b) { return jmax(a, b); }
+float hc_fabs(float a) { return fabs_j(a); }
+int64_t hc_f2l(float v) { return f2l(v); }
+double hc_nwrap(double v) { return nwrap(v); }
+float hc_grad(int32_t h, int32_t c) { return c == 0 ? gx_of(static_cast<uint32_t>(h)) : (c == 1 ? gy_of(static_cast<uint32_t>(h)) : gz_of(static_cast<uint32_t>(h))); }
+int64_t hc_pos_seed(int32_t x, int32_t y, int32_t z) { return pos_seed(x, y, z); }
+int hc_xoroshiro_longs(int64_t seed, int32_t n, int64_t* out) {
+    Xoro r = Xoro::from_seed(seed);
+    for (int i = 0; i < n; ++i) out[i] = static_cast<int64_t>(r.next());
+    return n;
+}
+int hc_xoroshiro_ints(int64_t seed, int32_t bound, int32_t n, int32_t* out) {
+    Xoro r = Xoro::from_seed(seed);
+    for (int i = 0; i < n; ++i) out[i] = r.next_int(bound);
+    return n;
+}
+double hc_stream_sum(const double* v, int32_t n) { return java_stream_sum(std::vector<double>(v, v + n)); }
+int64_t hc_zoom_seed(int64_t seed) {
+    SeedHost s;
+    build_seed_host(seed, s);
+    return s.zoom_seed;
+}
+}

@@ -1,0 +1,86 @@
+"""ctypes access to the host twin of the kernel bodies (lib/libterrain_b200_hostcheck.so).
+
+The twin compiles csrc/tb_pipeline.cuh and the generated evaluators for the host, so the
+CPU test suite can compare the device code's arithmetic with the reference port without
+a GPU. It is test infrastructure; the product never loads it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+PATH = os.path.join(REPO, 'minecraft-terrain-cuda_b200', 'lib', 'libterrain_b200_hostcheck.so')
+_L = None
+
+
+def available():
+    return os.path.exists(PATH)
+
+
+def lib():
+    global _L
+    if _L is None:
+        L = ctypes.CDLL(PATH)
+        vp = ctypes.c_void_p
+        L.hc_generate.argtypes = [ctypes.c_int64, vp, vp, ctypes.c_int32, vp, vp, vp]
+        L.hc_point.argtypes = [ctypes.c_int64, ctypes.c_int32, vp, ctypes.c_int32, vp]
+        L.hc_climate.argtypes = [ctypes.c_int64, vp, ctypes.c_int32, vp]
+        L.hc_corners.argtypes = [ctypes.c_int64, vp, ctypes.c_int32, vp]
+        L.hc_seed_scalars.argtypes = [ctypes.c_int64, vp, vp]
+        L.hc_noise_layers.argtypes = [ctypes.c_int64, ctypes.c_int32, vp, vp, vp, vp]
+        _L = L
+    return _L
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def generate(seed, chunks, aquifer=False):
+    a = np.ascontiguousarray(np.asarray(chunks, np.int32).reshape(-1, 2))
+    n = a.shape[0]
+    cx, cz = np.ascontiguousarray(a[:, 0]), np.ascontiguousarray(a[:, 1])
+    b = np.empty((n, 384, 16, 16), np.uint16)
+    q = np.empty((n, 1536), np.uint8)
+    aq = np.empty((n, 384, 16, 16), np.uint16) if aquifer else None
+    lib().hc_generate(int(seed), _p(cx), _p(cz), n, _p(b), _p(q), _p(aq) if aquifer else None)
+    return (b, q, aq) if aquifer else (b, q)
+
+
+def point(seed, root, xyz):
+    xyz = np.ascontiguousarray(np.asarray(xyz, np.int32).reshape(-1, 3))
+    out = np.empty(xyz.shape[0], np.float32)
+    assert lib().hc_point(int(seed), root, _p(xyz), xyz.shape[0], _p(out)) == 0
+    return out
+
+
+def climate(seed, xyz):
+    xyz = np.ascontiguousarray(np.asarray(xyz, np.int32).reshape(-1, 3))
+    out = np.empty((xyz.shape[0], 6), np.float32)
+    lib().hc_climate(int(seed), _p(xyz), xyz.shape[0], _p(out))
+    return out
+
+
+def corners(seed, xyz):
+    xyz = np.ascontiguousarray(np.asarray(xyz, np.int32).reshape(-1, 3))
+    nch = lib().hc_num_channels()
+    out = np.empty((xyz.shape[0], nch), np.float32)
+    lib().hc_corners(int(seed), _p(xyz), xyz.shape[0], _p(out))
+    return out
+
+
+def seed_scalars(seed):
+    a = np.zeros(7, np.int64)
+    clay = np.zeros(192, np.int32)
+    lib().hc_seed_scalars(int(seed), _p(a), _p(clay))
+    return a, clay
+
+
+def noise_layers(seed, key_index):
+    f = np.zeros(128)
+    amp = np.zeros(128, np.float32)
+    offs = np.zeros(384)
+    perms = np.zeros(128 * 256, np.uint8)
+    n = lib().hc_noise_layers(int(seed), key_index, _p(f), _p(amp), _p(offs), _p(perms))
+    return f[:n], amp[:n], offs[:3 * n].reshape(-1, 3), perms[:256 * n].reshape(-1, 256)
