@@ -107,6 +107,18 @@ tg_status tg_generate_batch(struct tg_generator* gen, const tg_request* requests
  * cpu/src/terrain.cpp:152-176). */
 tg_status tg_biome_lookup(struct tg_generator* gen, const int64_t* seeds, const int32_t* xyz, int32_t n, uint8_t* out);
 
+/* Biome lookups for the seed of tg_set_seed that allocate nothing: for callers that cannot
+ * allocate device memory (a tick thread running lookups while batches are in flight, where
+ * cudaFree would synchronise the device; a process whose HBM budget is fully reserved).
+ * Positions and results pass through one fixed device scratch array of 53,504 bytes, so
+ * n <= 4,096 and n <= max_batch_chunks; larger n returns TG_ERR_INVALID_ARGUMENT. xyz
+ * (3 x n int32) and out (n u8) are host memory. The first call on a device resolves the
+ * scratch address; make it before any stream capture begins. Every call on a device
+ * shares the array: calls that overlap on the GPU race (each call waits for its own
+ * copies before it returns). Results equal tg_biome_lookup with every seed = the current
+ * seed. No counterpart in the reference. */
+tg_status tg_biome_lookup_noalloc(struct tg_generator* gen, const int32_t* xyz, int32_t n, uint8_t* out);
+
 /* ---- serving: continuous batching ---------------------------------------------------
  * A server owns its generator (which then rejects direct calls until the server is
  * destroyed). A worker thread admits submitted requests while the chunks in flight stay

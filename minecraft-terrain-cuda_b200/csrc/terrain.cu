@@ -110,6 +110,59 @@ __global__ void k_biome_lookup(const __grid_constant__ Batch B, const int32_t* x
         out[i] = static_cast<uint8_t>(zoom_biome(B, i, B.seeds[B.cseed[i]].zoom_seed, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
 }
 
+// ---- scratch of the no-allocation biome lookup ---------------------------------------------------
+// tg_biome_lookup_noalloc stages its positions and results in this fixed device array
+// instead of device buffers allocated per call. Callers that cannot allocate device
+// memory use it: a game-server tick thread that runs lookups while the generator's
+// batches are in flight (cudaFree synchronises the whole device, so a per-call
+// allocation would stall those batches and the tick), and a process whose HBM budget is
+// fully reserved for generator and server buffers (an allocation there could fail in the
+// middle of a tick). Layout: [0, 256) header, the u32 count of finished positions at
+// offset 0, which must start at zero and is cleared by every call; then 3 x int32
+// positions; then the u8 biomes. At most 4,096 positions per call: 53,504 bytes.
+// Every call on a device shares this one array, so calls that overlap on the GPU race;
+// each call waits for its own copies before it returns.
+constexpr int kNoAllocMaxLookups = 4096;
+constexpr size_t kNoAllocXyzOff = 256;
+constexpr size_t kNoAllocOutOff = kNoAllocXyzOff + sizeof(int32_t) * 3 * kNoAllocMaxLookups;
+constexpr size_t kNoAllocBytes = kNoAllocOutOff + kNoAllocMaxLookups;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// k_biome_lookup with its positions and results in the no-allocation scratch; counts the
+// positions it finished into the scratch header.
+__global__ void k_biome_lookup_scratch(const __grid_constant__ Batch B, unsigned char* scratch) {
+    const int n = *B.n_dev;
+    const int32_t* xyz = reinterpret_cast<const int32_t*>(scratch + kNoAllocXyzOff);
+    uint8_t* out = scratch + kNoAllocOutOff;
+    unsigned int finished = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        out[i] = static_cast<uint8_t>(zoom_biome(B, i, B.seeds[B.cseed[i]].zoom_seed, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+        ++finished;
+    }
+    if (finished) atomicAdd(reinterpret_cast<unsigned int*>(scratch), finished);
+}
+
+// Device address of the scratch array on `device`, resolved once per device with that
+// device current. The first call on a device does this set-up; make it before any
+// stream capture begins.
+unsigned char* noalloc_scratch(int device) {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static unsigned char* addr[kMaxDevices] = {};
+    if (device < 0 || device >= kMaxDevices) throw Error(TG_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        int current = -1;
+        ck(cudaGetDevice(&current), "cudaGetDevice");
+        if (current != device) ck(cudaSetDevice(device), "cudaSetDevice");
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) throw Error(TG_ERR_CUDA, std::string("cudaGetSymbolAddress(no-allocation scratch): ") + cudaGetErrorString(e));
+        addr[device] = static_cast<unsigned char*>(p);
+    }
+    return addr[device];
+}
+
 int g_sm_count = 148;
 thread_local int g_launches = 0;
 
@@ -652,6 +705,48 @@ struct Generator {
         }
     }
 
+    // Biome lookups for the current seed that allocate nothing: positions and results pass
+    // through the fixed scratch array (g_noalloc_scratch), the chunk list through the
+    // generator's own pinned staging and batch buffers, built at tg_create.
+    void biome_lookup_noalloc(const int32_t* xyz, int n, uint8_t* res) {
+        if (current_slot < 0) throw Error(TG_ERR_NO_SEED, "tg_set_seed has not been called");
+        const int cap = std::min(kNoAllocMaxLookups, max_batch);
+        if (n > cap)
+            throw Error(TG_ERR_INVALID_ARGUMENT, "n = " + std::to_string(n) + " exceeds the no-allocation lookup limit of " + std::to_string(cap) +
+                                                     " positions (4,096 per call, and at most max_batch_chunks)");
+        for (int i = 0; i < n; ++i) {
+            const int32_t cx = xyz[3 * i] >> 4, cz = xyz[3 * i + 2] >> 4;
+            if (cx <= -(1 << 23) || cx >= (1 << 23) || cz <= -(1 << 23) || cz >= (1 << 23)) throw Error(TG_ERR_RANGE, "position out of range");
+        }
+        if (n == 0) return;
+        unsigned char* scratch = noalloc_scratch(device);
+        finish();
+        int32_t* h = out[0].coords.as<int32_t>();
+        for (int i = 0; i < n; ++i) {
+            h[i] = xyz[3 * i] >> 4;
+            h[max_batch + i] = xyz[3 * i + 2] >> 4;
+            h[2 * max_batch + i] = current_slot;
+        }
+        h[3 * max_batch] = n;
+        cudaStream_t s = stream;
+        ck(cudaMemsetAsync(scratch, 0, sizeof(unsigned int), s), "memset");   // the finished count starts at zero
+        ck(cudaMemcpyAsync(d_cx.p, h, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(d_cz.p, h + max_batch, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(d_cs.p, h + 2 * max_batch, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(scratch + kNoAllocXyzOff, xyz, sizeof(int32_t) * 3 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
+        const Batch B = batch_view(nullptr);
+        enqueue_biomes(B, s, n);
+        launch(k_biome_lookup_scratch, s, n, B, scratch);
+        ck(cudaGetLastError(), "kernel launch");
+        unsigned int finished = 0;
+        ck(cudaMemcpyAsync(res, scratch + kNoAllocOutOff, static_cast<size_t>(n), cudaMemcpyDeviceToHost, s), "d2h");
+        ck(cudaMemcpyAsync(&finished, scratch, sizeof finished, cudaMemcpyDeviceToHost, s), "d2h");
+        ck(cudaStreamSynchronize(s), "sync");
+        if (finished != static_cast<unsigned int>(n))
+            throw Error(TG_ERR_INTERNAL, "no-allocation lookup finished " + std::to_string(finished) + " of " + std::to_string(n) + " positions");
+    }
+
     // Multi-seed batch: requests are cut into device batches; a batch mixes seeds.
     void generate_batch(const tg_request* req, int n, tg_timing* t) {
         for (int r = 0; r < n; ++r) {
@@ -1080,6 +1175,14 @@ tg_status tg_biome_lookup(tg_generator* gen, const int64_t* seeds, const int32_t
         usable(gen);
         if (n < 0 || (n > 0 && (!seeds || !xyz || !out))) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
         gen->g->biome_lookup(seeds, xyz, n, out);
+    });
+}
+
+tg_status tg_biome_lookup_noalloc(tg_generator* gen, const int32_t* xyz, int32_t n, uint8_t* out) {
+    return tb::guarded([&] {
+        usable(gen);
+        if (n < 0 || (n > 0 && (!xyz || !out))) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        gen->g->biome_lookup_noalloc(xyz, n, out);
     });
 }
 

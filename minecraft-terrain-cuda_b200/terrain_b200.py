@@ -54,6 +54,7 @@ class TgServerStats(ctypes.Structure):
 
 
 EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+           'tg_biome_lookup_noalloc',
            'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
            'tg_alloc_pinned', 'tg_free_pinned', 'tg_model_info', 'tg_last_error_string']
 
@@ -83,6 +84,7 @@ def load(path=LIB_PATH):
     L.tg_generate_device.argtypes = [vp, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(TgTiming)]
     L.tg_generate_batch.argtypes = [vp, ctypes.POINTER(TgRequest), ctypes.c_int32, ctypes.POINTER(TgTiming)]
     L.tg_biome_lookup.argtypes = [vp, vp, vp, ctypes.c_int32, vp]
+    L.tg_biome_lookup_noalloc.argtypes = [vp, vp, ctypes.c_int32, vp]
     L.tg_server_create.argtypes = [vp, ctypes.POINTER(TgServerConfig), ctypes.POINTER(vp)]
     L.tg_server_submit.argtypes = [vp, ctypes.c_int64, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
     L.tg_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
@@ -195,6 +197,13 @@ class TerrainGenerator:
         seeds = np.ascontiguousarray(np.broadcast_to(np.asarray(seeds, np.int64), (xyz.shape[0],)))
         out = np.empty(xyz.shape[0], np.uint8)
         self._check(self.L.tg_biome_lookup(self.h, _ptr(seeds), _ptr(xyz), xyz.shape[0], _ptr(out)))
+        return out
+
+    def biome_lookup_noalloc(self, xyz):
+        """Lookups for the current seed through the fixed device scratch (at most 4,096)."""
+        xyz = np.ascontiguousarray(np.asarray(xyz, np.int32).reshape(-1, 3))
+        out = np.empty(xyz.shape[0], np.uint8)
+        self._check(self.L.tg_biome_lookup_noalloc(self.h, _ptr(xyz), xyz.shape[0], _ptr(out)))
         return out
 
 
