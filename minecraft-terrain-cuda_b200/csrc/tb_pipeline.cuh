@@ -116,6 +116,7 @@ struct Batch {
     uint8_t* biomes_out;              // n * kQuartsPerChunk
     uint32_t* zoom_tab;               // n * kZoomVerts packed fiddle draws per quart vertex
     uint32_t* walk;                   // n * kBlocksPerChunk packed column-walk state per block
+    uint8_t* bbiome;                  // n * kBlocksPerChunk zoomed biome per block up to the column height
     struct ColumnRec* colrec;         // n * 256 per-column surface context
 };
 
@@ -734,6 +735,16 @@ TB_HD TB_FI uint32_t zoom_fiddles(int64_t seed, int qx, int qy, int qz) {
 
 // BiomeManager.getBiome: the quart whose fiddled corner is nearest (first on ties), then
 // its stored biome from the chunk's 3x3 neighbourhood (qy clamped to the world).
+TB_HD TB_FI int zoom_stored(const Batch& B, int c, int best, int px, int py, int pz) {
+    const int qx = (best & 4) == 0 ? px : px + 1;
+    const int qy = (best & 2) == 0 ? py : py + 1;
+    const int qz = (best & 1) == 0 ? pz : pz + 1;
+    const int dcx = (qx >> 2) - B.cx[c], dcz = (qz >> 2) - B.cz[c];
+    constexpr int qmin = tbm::kMinY >> 2, qh = tbm::kHeight / 4;
+    const int cqy = (qy < qmin ? qmin : (qy > qmin + qh - 1 ? qmin + qh - 1 : qy)) - qmin;
+    const int b = B.nb9[static_cast<size_t>(c) * 9 + (dcz + 1) * 3 + dcx + 1];
+    return B.qbiome[static_cast<size_t>(b) * kQuartsPerChunk + (cqy * 4 + (qz & 3)) * 4 + (qx & 3)];
+}
 template <class Fiddles>
 TB_HD TB_FI int zoom_pick(const Batch& B, int c, int x, int y, int z, Fiddles fid) {
     const int ax = x - 2, ay = y - 2, az = z - 2;
@@ -755,14 +766,7 @@ TB_HD TB_FI int zoom_pick(const Batch& B, int c, int x, int y, int z, Fiddles fi
             best_d = d;
         }
     }
-    const int qx = (best & 4) == 0 ? px : px + 1;
-    const int qy = (best & 2) == 0 ? py : py + 1;
-    const int qz = (best & 1) == 0 ? pz : pz + 1;
-    const int dcx = (qx >> 2) - B.cx[c], dcz = (qz >> 2) - B.cz[c];
-    constexpr int qmin = tbm::kMinY >> 2, qh = tbm::kHeight / 4;
-    const int cqy = (qy < qmin ? qmin : (qy > qmin + qh - 1 ? qmin + qh - 1 : qy)) - qmin;
-    const int b = B.nb9[static_cast<size_t>(c) * 9 + (dcz + 1) * 3 + dcx + 1];
-    return B.qbiome[static_cast<size_t>(b) * kQuartsPerChunk + (cqy * 4 + (qz & 3)) * 4 + (qx & 3)];
+    return zoom_stored(B, c, best, px, py, pz);
 }
 
 // any position (biome lookups): the LCG chains computed in place
@@ -782,6 +786,60 @@ TB_HD inline void body_zoom_table(const Batch& B, int it) {
     const int c = it / kZoomVerts, v = it % kZoomVerts;
     const int qx = B.cx[c] * 4 - 1 + v % 6, qz = B.cz[c] * 4 - 1 + (v / 6) % 6, qy = kZoomQyMin + v / 36;
     B.zoom_tab[it] = zoom_fiddles(B.seeds[B.cseed[c]].zoom_seed, qx, qy, qz);
+}
+
+// Zoomed biomes of the blocks under the surface, for the rule tree. Blocks y = 4 py + 2 ..
+// 4 py + 5 share py = (y - 2) >> 2 and so the 8 candidate vertices: their fiddles and the
+// x and z distance terms are computed once per group, and each block adds its own y term
+// in zoom_pick's order ((z term + y term) + x term), so every value is zoom_pick's.
+constexpr int kZoomPyMin = (tbm::kMinY - 2) >> 2;
+constexpr int kZoomGroups = ((kMaxY - 2) >> 2) - kZoomPyMin + 1;
+
+// item = (chunk * kZoomGroups + group) * 256 + z * 16 + x; blocks up to the column height
+TB_HD inline void body_block_biome(const Batch& B, int it) {
+    const int col = it & 255, g = (it >> 8) % kZoomGroups, c = (it >> 8) / kZoomGroups;
+    const int lx = col & 15, lz = col >> 4;
+    const int py = kZoomPyMin + g;
+    const int top = B.h1[(static_cast<size_t>(c) << 8) | (lx << 4) | lz];
+    const int ylo = 4 * py + 2 < tbm::kMinY ? tbm::kMinY : 4 * py + 2;
+    int yhi = 4 * py + 5 > kMaxY ? kMaxY : 4 * py + 5;
+    if (yhi > top) yhi = top;
+    if (ylo > yhi) return;
+    const int x = B.cx[c] * 16 + lx, z = B.cz[c] * 16 + lz;
+    const int ax = x - 2, az = z - 2, px = ax >> 2, pz = az >> 2;
+    const double fx = static_cast<double>(ax & 3) / 4.0, fz = static_cast<double>(az & 3) / 4.0;
+    const uint32_t* tab = B.zoom_tab + static_cast<size_t>(c) * kZoomVerts;
+    const int qx0 = B.cx[c] * 4 - 1, qz0 = B.cz[c] * 4 - 1;
+    double sx[8], sz[8], oy[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const bool xe = (i & 4) == 0, ye = (i & 2) == 0, ze = (i & 1) == 0;
+        const int qx = xe ? px : px + 1, qy = ye ? py : py + 1, qz = ze ? pz : pz + 1;
+        const uint32_t m = tab[((qy - kZoomQyMin) * 6 + (qz - qz0)) * 6 + (qx - qx0)];
+        const double ox = zoom_fiddle(static_cast<int32_t>(m & 1023u));
+        oy[i] = zoom_fiddle(static_cast<int32_t>((m >> 10) & 1023u));
+        const double oz = zoom_fiddle(static_cast<int32_t>(m >> 20));
+        const double dx = xe ? fx : fx - 1.0, dz = ze ? fz : fz - 1.0;
+        sz[i] = (dz + oz) * (dz + oz);
+        sx[i] = (dx + ox) * (dx + ox);
+    }
+    uint8_t* out = B.bbiome + static_cast<size_t>(c) * kBlocksPerChunk;
+    for (int y = ylo; y <= yhi; ++y) {
+        const double fy = static_cast<double>((y - 2) & 3) / 4.0;
+        int best = 0;
+        double best_d = 0.0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const double dy = (i & 2) == 0 ? fy : fy - 1.0;
+            const double sy = (dy + oy[i]) * (dy + oy[i]);
+            const double d = sz[i] + sy + sx[i];
+            if (i == 0 || best_d > d) {
+                best = i;
+                best_d = d;
+            }
+        }
+        out[((y - tbm::kMinY) * 16 + lz) * 16 + lx] = static_cast<uint8_t>(zoom_stored(B, c, best, px, py, pz));
+    }
 }
 
 TB_HD TB_NOINLINE inline float biome_temperature(const DevModel& M, int biome, int x, int y, int z) {
@@ -920,6 +978,46 @@ TB_HD TB_FI float prelim_surface(const Batch& B, int c, int lx, int lz) {
     return a0 + step * 0.0f;
 }
 
+// Channel values of one block on first use: the generated ore functions read a channel
+// only under the guards that need it (a vein's y range, for one). Each value is the
+// cell's a0 plus the step added once per block above the cell floor, as in the fill.
+struct LazyChannels {
+    const Batch* B;
+    int c, lx, lz, y;
+    mutable bool set;
+    mutable float ch[tbm::kNumChannels];
+    TB_HD TB_FI float operator[](int k) const {
+        if (!set) {
+            CellInterp ci;
+            const int cell_y = (y - tbm::kMinY) >> 3, yi = (y - tbm::kMinY) & 7;
+            cell_interp(*B, c, lx, lz, cell_y, ci);
+            for (int j = 0; j < tbm::kNumChannels; ++j) {
+                float v = ci.a0[j];
+                for (int q = 0; q < yi; ++q) v += ci.step[j];
+                ch[j] = v;
+            }
+            set = true;
+        }
+        return ch[k];
+    }
+};
+
+// OreVeinRule for one block: density and richness on the volume path (channel values),
+// the filler gap on the point path. Takes its inputs by value so that the rule context
+// of the caller stays in registers.
+TB_HD TB_NOINLINE inline int ore_vein_at(const Batch& B, int c, int lx, int lz, int bx, int y, int bz, const DevSeed& S, int k, int ore, int raw,
+                                         int filler, float chance) {
+    const NoiseTables& T = S.nt;
+    const LazyChannels ch{&B, c, lx, lz, y, false, {}};
+    const float density = tbgen::gen_ore_density(k, T, bx, y, bz, ch);
+    if (density <= 0.0f) return -1;
+    Xoro r = S.ore.at(bx, y, bz);
+    if (r.next_float() > density) return -1;
+    const float richness = tbgen::gen_ore_richness(k, T, bx, y, bz, ch);
+    if (r.next_float() < richness && tbgen::gen_ore_gap(k, T, bx, y, bz) < 0.0f) return r.next_float() < chance ? raw : ore;
+    return filler;
+}
+
 // Block context handed to the generated rule tree (MaterialSystem's per-block state).
 struct RuleCtx {
     Column* col;
@@ -933,13 +1031,12 @@ struct RuleCtx {
     float prelim;
     // block
     int y, stone_above, stone_below, water_height;
-    bool biome_set, ch_set;
+    bool biome_set;
     int biome_v;
-    float ch[tbm::kNumChannels];
 
     TB_HD TB_FI int biome() {
         if (!biome_set) {
-            biome_v = zoom_biome_tab(*B, c, col->bx, y, col->bz);
+            biome_v = B->bbiome[static_cast<size_t>(c) * kBlocksPerChunk + col->idx(y)];
             biome_set = true;
         }
         return biome_v;
@@ -978,33 +1075,10 @@ struct RuleCtx {
         const int off = jround(static_cast<float>(col->noise<tbm::kNoise_clay_bands_offset>(col->bx, 0.0, col->bz)) * 4.0f);
         return col->S->clay[(y + off + 192) % 192];
     }
-    TB_HD TB_NOINLINE void channels() {
-        if (ch_set) return;
-        CellInterp ci;
-        const int cell_y = (y - tbm::kMinY) >> 3, yi = (y - tbm::kMinY) & 7;
-        cell_interp(*B, c, col->lx, col->lz, cell_y, ci);
-        for (int k = 0; k < tbm::kNumChannels; ++k) {
-            float v = ci.a0[k];
-            for (int q = 0; q < yi; ++q) v += ci.step[k];
-            ch[k] = v;
-        }
-        ch_set = true;
+    TB_HD TB_FI int ore_vein(int k, int ore, int raw, int filler, float chance) const {
+        return ore_vein_at(*B, c, col->lx, col->lz, col->bx, y, col->bz, *col->S, k, ore, raw, filler, chance);
     }
-    TB_HD TB_NOINLINE int ore_vein(int k, int ore, int raw, int filler, float chance);
 };
-
-// OreVeinRule: density and richness on the volume path, the filler gap on the point path.
-TB_HD TB_NOINLINE int RuleCtx::ore_vein(int k, int ore, int raw, int filler, float chance) {
-    channels();
-    const NoiseTables& T = col->S->nt;
-    const float density = tbgen::gen_ore_density(k, T, col->bx, y, col->bz, ch);
-    if (density <= 0.0f) return -1;
-    Xoro r = col->S->ore.at(col->bx, y, col->bz);
-    if (r.next_float() > density) return -1;
-    const float richness = tbgen::gen_ore_richness(k, T, col->bx, y, col->bz, ch);
-    if (r.next_float() < richness && tbgen::gen_ore_gap(k, T, col->bx, y, col->bz) < 0.0f) return r.next_float() < chance ? raw : ore;
-    return filler;
-}
 
 // pass 1 (item = chunk * 256 + z * 16 + x): eroded badlands (writes), heights after it
 // and after a dry run of the frozen-ocean extension
@@ -1111,7 +1185,6 @@ TB_HD inline void body_surface_rules(const Batch& B, int it) {
     const uint32_t wh = w >> 20;
     R.water_height = wh == 1023u ? INT_MIN : static_cast<int>(wh) + tbm::kMinY;
     R.biome_set = false;
-    R.ch_set = false;
     const int state = tbgen::apply_rules(R);
     if (state >= 0) C.blocks[b] = static_cast<uint16_t>(state);
 }

@@ -63,7 +63,7 @@ double now_ms() { return std::chrono::duration<double, std::milli>(std::chrono::
 // ---- kernels: grid-stride loops over the bodies --------------------------------------------------
 // Minimum resident 256-thread blocks per SM for the register-heavy kernels (caps registers).
 #ifndef TB_MINB_SURFACE2
-#define TB_MINB_SURFACE2 3
+#define TB_MINB_SURFACE2 4
 #endif
 #ifndef TB_MINB_FILL
 #define TB_MINB_FILL 1
@@ -283,7 +283,7 @@ struct Generator {
     int current_slot = -1;
     // batch buffers (shared by both output slots: the kernels of one batch at a time use them)
     DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_loc, d_aq_status,
-        d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_walk, d_colrec;
+        d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_walk, d_bbiome, d_colrec;
     TableBufs tb_b, tb_c, tb_s;
     OutSlot out[2];
     int next_out = 0;
@@ -390,6 +390,7 @@ struct Generator {
         d_h2.alloc(4 * 256 * N);
         d_zoom.alloc(sizeof(uint32_t) * N * kZoomVerts);
         d_walk.alloc(sizeof(uint32_t) * N * kBlocksPerChunk);
+        d_bbiome.alloc(N * kBlocksPerChunk);
         d_colrec.alloc(sizeof(ColumnRec) * N * 256);
         for (auto& o : out) {
             o.blocks.alloc(sizeof(uint16_t) * N * kBlocksPerChunk);
@@ -477,6 +478,7 @@ struct Generator {
         B.biomes_out = o ? o->biomes.as<uint8_t>() : nullptr;
         B.zoom_tab = d_zoom.as<uint32_t>();
         B.walk = d_walk.as<uint32_t>();
+        B.bbiome = d_bbiome.as<uint8_t>();
         B.colrec = d_colrec.as<ColumnRec>();
         return B;
     }
@@ -523,6 +525,7 @@ struct Generator {
                "d2d");
         mark(4);
         launch(k_items<body_surface1, 256>, s, 256 * nmax, B);
+        launch(k_items<body_block_biome, 256 * kZoomGroups>, s, 256L * kZoomGroups * nmax, B);
         launch(k_items<body_surface_walk, 256>, s, 256 * nmax, B);
         launch(k_items<body_surface_rules, kBlocksPerChunk, TB_MINB_SURFACE2>, s, static_cast<long>(kBlocksPerChunk) * nmax, B);
         launch(k_items<body_surface_frozen, 256>, s, 256 * nmax, B);

@@ -100,6 +100,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     std::vector<uint8_t> qbiome(nb * kQuartsPerChunk), bout(N * kQuartsPerChunk);
     std::vector<uint16_t> bl(N * kBlocksPerChunk);
     std::vector<uint32_t> ztab(N * kZoomVerts), walk(N * kBlocksPerChunk);
+    std::vector<uint8_t> bbiome(N * kBlocksPerChunk);
     std::vector<ColumnRec> colrec(N * 256);
     Batch B{};
     B.M = R.M;
@@ -135,6 +136,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     B.biomes_out = bout.data();
     B.zoom_tab = ztab.data();
     B.walk = walk.data();
+    B.bbiome = bbiome.data();
     B.colrec = colrec.data();
     each(9 * n, [&](int i) { body_nb_insert(B, i); });
     each(9 * n, [&](int i) { body_nb_resolve(B, i); });
@@ -154,6 +156,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     each(256 * kCellsY * n, [&](int i) { body_fill(B, i); });
     if (aquifer) std::memcpy(aquifer, bl.data(), sizeof(uint16_t) * bl.size());
     each(256 * n, [&](int i) { body_surface1(B, i); });
+    each(256 * kZoomGroups * n, [&](int i) { body_block_biome(B, i); });
     each(256 * n, [&](int i) { body_surface_walk(B, i); });
     each(kBlocksPerChunk * n, [&](int i) { body_surface_rules(B, i); });
     each(256 * n, [&](int i) { body_surface_frozen(B, i); });
