@@ -375,7 +375,7 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-serve', action='store_true', help='skip the served-versus-plain request-stream measurement')
     ap.add_argument('--profile-small', action='store_true',
-                    help='one untimed step over a 16x16-chunk corner of each region (a small case for ncu captures)')
+                    help='one untimed step over a 32x32-chunk corner of each region, 1,024-chunk batches (a small case for ncu captures)')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
@@ -385,10 +385,10 @@ def main():
         return
     if args.profile_small:
         import terrain_b200
-        g = terrain_b200.TerrainGenerator(max_batch_chunks=256)
+        g = terrain_b200.TerrainGenerator(max_batch_chunks=1024)
         g.set_seed(SEED)
         for _, x0, z0 in REGIONS:
-            g.generate(region_chunks(x0, z0, 16))
+            g.generate(region_chunks(x0, z0, 32))
         g.close()
         return
     if world > 1:

@@ -127,6 +127,9 @@ struct ColumnRec {
     int32_t surface_biome, start_h;
 };
 constexpr uint32_t kNoWalk = 0xFFFFFFFFu;
+#ifndef TB_FUSED_WALK
+#define TB_FUSED_WALK 1     // rule tree inside the column walk (1) or a per-block pass after it (0)
+#endif
 
 // ---- atomics (device) / plain operations (host test build) --------------------------------------
 TB_HD TB_FI unsigned long long cas64(unsigned long long* p, unsigned long long cmp, unsigned long long val) {
@@ -1187,6 +1190,74 @@ TB_HD inline void body_surface_rules(const Batch& B, int it) {
     R.biome_set = false;
     const int state = tbgen::apply_rules(R);
     if (state >= 0) C.blocks[b] = static_cast<uint16_t>(state);
+}
+
+// pass 2 fused (item = chunk * 256 + z * 16 + x): the column context and the top-down walk,
+// applying the rule tree to each solid block as the walk reaches it (the blocks below it,
+// which the walk still reads, are untouched; the rules never turn a block into air or a
+// fluid). A warp holds 32 columns of one chunk at the same y, as the per-block pass does.
+TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
+    const int c = it >> 8, lz = (it >> 4) & 15, lx = it & 15;
+    const int ci = (c << 8) | (lx << 4) | lz;   // x * 16 + z column index
+    const size_t hb = static_cast<size_t>(c) * 256;
+    Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
+             B.h1[ci]};
+    auto H = [&](int x, int z) -> int {
+        if (x == lx && z == lz) return B.h1[hb + x * 16 + z] - 1;
+        const bool done = x < lx || (x == lx && z < lz);
+        return (done ? B.h2[hb + x * 16 + z] : B.h0[hb + x * 16 + z]) - 1;
+    };
+    ColumnRec r;
+    r.start_h = B.h0[ci];
+    r.surface_biome = zoom_biome_tab(B, c, C.bx, r.start_h, C.bz);
+    r.grad_x = H(lx + 1 < 15 ? lx + 1 : 15, lz) - H(lx - 1 > 0 ? lx - 1 : 0, lz);
+    r.grad_z = H(lx, lz + 1 < 15 ? lz + 1 : 15) - H(lx, lz - 1 > 0 ? lz - 1 : 0);
+    const double n = C.noise<tbm::kNoise_surface>(C.bx, 0.0, C.bz);
+    const double rr = C.S->random.at(C.bx, 0, C.bz).next_double();
+    r.surface_depth = d2i(n * 2.75 + 3.0 + rr * 0.25);
+    r.min_surface = jfloor(static_cast<double>(prelim_surface(B, c, lx, lz))) + r.surface_depth - 8;
+    r.secondary = C.noise<tbm::kNoise_surface_secondary>(C.bx, 0.0, C.bz);
+    B.colrec[ci] = r;
+    RuleCtx R{};
+    R.col = &C;
+    R.B = &B;
+    R.c = c;
+    R.surface_depth = r.surface_depth;
+    R.grad_x = r.grad_x;
+    R.grad_z = r.grad_z;
+    R.min_set = true;
+    R.min_surf = r.min_surface;
+    R.sec_set = true;
+    R.secondary = r.secondary;
+    const int height = C.hm;
+    int stone_above = 0, water_height = INT_MIN, next_ceiling = INT_MAX;
+    for (int y = height > kMaxY ? kMaxY : height; y >= tbm::kMinY; --y) {
+        const uint8_t f = C.flags(C.get(y));
+        if (f & 1) {
+            stone_above = 0;
+            water_height = INT_MIN;
+        } else if (f & 8) {
+            if (water_height == INT_MIN) water_height = y + 1;
+        } else {
+            if (next_ceiling >= y) {
+                next_ceiling = kWayBelowMinY;
+                for (int la = y - 1; la >= tbm::kMinY - 1; --la) {
+                    if (C.flags(C.get(la)) & 9) {
+                        next_ceiling = la + 1;
+                        break;
+                    }
+                }
+            }
+            ++stone_above;
+            R.y = y;
+            R.stone_above = stone_above;
+            R.stone_below = y - next_ceiling + 1;
+            R.water_height = water_height;
+            R.biome_set = false;
+            const int state = tbgen::apply_rules(R);
+            if (state >= 0) C.blocks[C.idx(y)] = static_cast<uint16_t>(state);
+        }
+    }
 }
 
 // pass 2c (item = chunk * 256 + z * 16 + x): the frozen-ocean extension after the rules

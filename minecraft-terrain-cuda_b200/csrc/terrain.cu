@@ -62,6 +62,12 @@ double now_ms() { return std::chrono::duration<double, std::milli>(std::chrono::
 
 // ---- kernels: grid-stride loops over the bodies --------------------------------------------------
 // Minimum resident 256-thread blocks per SM for the register-heavy kernels (caps registers).
+#ifndef TB_MINB_WALK
+#define TB_MINB_WALK 4
+#endif
+#ifndef TB_CHAIN_WARP
+#define TB_CHAIN_WARP 1     // last-result chain with one warp per biome chunk
+#endif
 #ifndef TB_MINB_SURFACE2
 #define TB_MINB_SURFACE2 4
 #endif
@@ -101,6 +107,63 @@ __global__ void k_split_chunks(const tg_chunk_xz* ch, int n, int32_t slot, int32
         cs[i] = slot;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *n_dev = n;
+}
+
+// The last-result chain of body_chain with one warp per biome chunk. Lane k of a block of
+// 32 quarts p first assumes the chain entered p holding L*(p - 1) (the previous quart's
+// first minimal leaf; for lane 0 the true previous result) and decides whether that leaf is
+// kept (it differs from L*(p) and reaches the minimum distance of p). While the assumption
+// holds the block resolves from those decisions; a leaf that is carried past its own quart
+// is tested against the following quarts of the block in one parallel round. Every result
+// equals body_chain's.
+__device__ void chain_warp(const Batch& B, int b, int lane) {
+    const size_t base = static_cast<size_t>(b) * kQuartsPerChunk;
+    const unsigned full = 0xFFFFFFFFu;
+    int last = -1;
+    for (int p0 = 0; p0 < kQuartsPerChunk; p0 += 32) {
+        const size_t q = base + p0 + lane;
+        const int ls = B.lstar[q];
+        const long long md = B.mdist[q];
+        const long long* t = B.tgt + q * 6;
+        int prev = __shfl_up_sync(full, ls, 1);
+        if (lane == 0) prev = last;
+        const bool keep = prev >= 0 && prev != ls && param_dist(B.M.tree[B.M.leaf_node[prev]], t) == md;
+        const unsigned keeps = __ballot_sync(full, keep);
+        int r = ls;                 // this lane's result
+        int v = last;               // chain value entering position pos (warp-uniform)
+        int pos = 0;
+        while (pos < 32) {
+            const int spec = pos == 0 ? last : __shfl_sync(full, ls, pos - 1);
+            if (v == spec) {
+                const unsigned m = keeps & (full << pos);
+                if (!m) {
+                    pos = 32;
+                    break;
+                }
+                const int j = __ffs(m) - 1;
+                if (lane == j) r = prev;
+                v = __shfl_sync(full, prev, j);
+                pos = j + 1;
+            } else {
+                const bool carry = lane >= pos && v != ls && param_dist(B.M.tree[B.M.leaf_node[v]], t) == md;
+                const unsigned run = __ballot_sync(full, carry) | ~(full << pos);
+                const int j = (~run) ? __ffs(~run) - 1 : 32;   // first lane at or after pos that does not keep v
+                if (lane >= pos && lane < j) r = v;
+                if (j < 32) v = __shfl_sync(full, ls, j);
+                pos = j + 1;
+            }
+        }
+        last = __shfl_sync(full, r, 31);
+        int qx, qy, qz;
+        chain_quart(p0 + lane, qx, qy, qz);
+        B.qbiome[base + (qy * 4 + qz) * 4 + qx] = static_cast<uint8_t>(B.M.leaf_biome[r]);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_chain_warp(const __grid_constant__ Batch B, const int32_t* count) {
+    const int n = *count, lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) chain_warp(B, w, lane);
 }
 
 // one lookup position per item: the zoomed biome from its chunk's neighbourhood
@@ -389,7 +452,7 @@ struct Generator {
         d_h1.alloc(4 * 256 * N);
         d_h2.alloc(4 * 256 * N);
         d_zoom.alloc(sizeof(uint32_t) * N * kZoomVerts);
-        d_walk.alloc(sizeof(uint32_t) * N * kBlocksPerChunk);
+        if (!TB_FUSED_WALK) d_walk.alloc(sizeof(uint32_t) * N * kBlocksPerChunk);   // per-block walk states of the split pass
         d_bbiome.alloc(N * kBlocksPerChunk);
         d_colrec.alloc(sizeof(ColumnRec) * N * 256);
         for (auto& o : out) {
@@ -491,7 +554,11 @@ struct Generator {
         launch(k_items<body_nb_resolve, 9>, s, 9 * nmax, B);
         launch(k_dyn<body_climate_col, 16>, s, nmax * 16 * 2, B, cnt_b);
         launch(k_dyn<body_climate_quart, 16 * kRuns, TB_MINB_QUART>, s, nmax * 16 * kRuns * 2, B, cnt_b);
+#if TB_CHAIN_WARP
+        launch(k_chain_warp, s, nmax * 2 * 32, B, cnt_b);
+#else
         launch(k_dyn<body_chain, 1>, s, nmax * 2, B, cnt_b);
+#endif
     }
 
     // every kernel of one batch; with timed set, events split the stages
@@ -526,8 +593,12 @@ struct Generator {
         mark(4);
         launch(k_items<body_surface1, 256>, s, 256 * nmax, B);
         launch(k_items<body_block_biome, 256 * kZoomGroups>, s, 256L * kZoomGroups * nmax, B);
+#if TB_FUSED_WALK
+        launch(k_items<body_surface_walk_rules, 256, TB_MINB_WALK>, s, 256 * nmax, B);
+#else
         launch(k_items<body_surface_walk, 256>, s, 256 * nmax, B);
         launch(k_items<body_surface_rules, kBlocksPerChunk, TB_MINB_SURFACE2>, s, static_cast<long>(kBlocksPerChunk) * nmax, B);
+#endif
         launch(k_items<body_surface_frozen, 256>, s, 256 * nmax, B);
         launch(k_items<body_gather, kQuartsPerChunk>, s, static_cast<long>(kQuartsPerChunk) * nmax, B);
         mark(5);

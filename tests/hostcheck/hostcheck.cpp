@@ -157,8 +157,12 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     if (aquifer) std::memcpy(aquifer, bl.data(), sizeof(uint16_t) * bl.size());
     each(256 * n, [&](int i) { body_surface1(B, i); });
     each(256 * kZoomGroups * n, [&](int i) { body_block_biome(B, i); });
+#if TB_FUSED_WALK
+    each(256 * n, [&](int i) { body_surface_walk_rules(B, i); });
+#else
     each(256 * n, [&](int i) { body_surface_walk(B, i); });
     each(kBlocksPerChunk * n, [&](int i) { body_surface_rules(B, i); });
+#endif
     each(256 * n, [&](int i) { body_surface_frozen(B, i); });
     each(kQuartsPerChunk * n, [&](int i) { body_gather(B, i); });
     std::memcpy(blocks, bl.data(), sizeof(uint16_t) * bl.size());
