@@ -522,15 +522,34 @@ void build_model_host(ModelHost& m) {
             if (r.mn[d] > r.mx[d] || r.mn[d] < -kBox32Limit || r.mx[d] > kBox32Limit) fits = false;
     }
     if (fits) {
-        m.boxes.resize(m.nodes.size());
-        for (size_t i = 0; i < m.nodes.size(); ++i) {
-            const RNode& r = m.nodes[i];
+        // breadth first from the root, so that the children of a node are consecutive boxes
+        std::vector<int> order{m.root};
+        std::vector<int32_t> box_of(m.nodes.size(), -1);
+        box_of[m.root] = 0;
+        for (size_t h = 0; h < order.size(); ++h) {
+            const RNode& r = m.nodes[order[h]];
+            if (r.leaf >= 0) continue;
+            for (int k = 0; k < r.child_count; ++k) {
+                const int ch = m.children[r.first_child + k];
+                box_of[ch] = static_cast<int32_t>(order.size());
+                order.push_back(ch);
+            }
+        }
+        m.boxes.resize(order.size());
+        m.box_leaf.assign(tbm::kNumParams, -1);
+        for (size_t i = 0; i < order.size(); ++i) {
+            const RNode& r = m.nodes[order[i]];
             RBox& b = m.boxes[i];
             for (int d = 0; d < 7; ++d) {
                 b.mn[d] = static_cast<int32_t>(r.mn[d]);
                 b.mx[d] = static_cast<int32_t>(r.mx[d]);
             }
-            b.info = !reachable[i] ? 0 : (r.leaf >= 0 ? ~r.leaf : ((r.first_child << 5) | r.child_count));
+            if (r.leaf >= 0) {
+                b.info = ~r.leaf;
+                m.box_leaf[r.leaf] = static_cast<int32_t>(i);
+            } else {
+                b.info = (box_of[m.children[r.first_child]] << 5) | r.child_count;
+            }
             b.rank = r.rank;
         }
     }

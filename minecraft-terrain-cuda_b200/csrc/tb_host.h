@@ -36,9 +36,10 @@ struct RNode {                 // flattened R-tree node (device layout)
     int32_t rank;              // depth-first rank of the first leaf in the subtree
 };
 
-// The same node as 16 int32 (64 bytes), used when every box bound fits in +/-2^29:
-// info = ~leaf for leaves, (first_child << 5) | child_count otherwise.
-struct RBox {
+// The same node as 16 int32 (64 bytes), used when every box bound fits in +/-2^29. The
+// boxes are stored breadth first from the root (box 0), the children of a node
+// consecutive: info = ~leaf for leaves, (first child box << 5) | child_count otherwise.
+struct alignas(16) RBox {
     int32_t mn[7], mx[7];
     int32_t info, rank;
 };
@@ -47,6 +48,7 @@ constexpr int32_t kBox32Limit = 1 << 29;
 struct ModelHost {
     std::vector<RNode> nodes;
     std::vector<RBox> boxes;       // empty unless every bound fits the 32-bit search
+    std::vector<int32_t> box_leaf; // parameter index -> box index
     std::vector<int32_t> children;
     std::vector<int32_t> leaf_biome;   // per parameter index
     std::vector<int32_t> leaf_node;    // parameter index -> node index

@@ -42,7 +42,8 @@ static_assert(tbm::kHeight % 16 == 0 && tbm::kMinY % 16 == 0, "world height must
 
 // ---- device-resident model and per-seed tables -------------------------------------------------
 struct DevModel {
-    const RBox* boxes;              // null when the 32-bit search does not apply
+    const RBox* boxes;              // null when the 32-bit search does not apply; root is box 0
+    const int32_t* box_leaf;        // parameter index -> box index
     const RNode* tree;
     const int32_t* children;
     const int32_t* leaf_biome;
@@ -322,10 +323,10 @@ TB_HD TB_FI long long box_dist32(const RBox& n, const int32_t* t) {
 TB_HD inline int tree_first_min32(const DevModel& M, const int32_t* t, int start_leaf, long long& best_d) {
     int best = start_leaf;
     int best_rank = M.leaf_rank[start_leaf];
-    best_d = box_dist32(M.boxes[M.leaf_node[start_leaf]], t);
+    best_d = box_dist32(M.boxes[M.box_leaf[start_leaf]], t);
     int stack_node[kSearchStack], stack_next[kSearchStack];
     int sp = 1;
-    stack_node[0] = M.root;
+    stack_node[0] = 0;
     stack_next[0] = 0;
     while (sp > 0) {
         const int info = M.boxes[stack_node[sp - 1]].info;
@@ -335,7 +336,7 @@ TB_HD inline int tree_first_min32(const DevModel& M, const int32_t* t, int start
             continue;
         }
         stack_next[sp - 1] = k + 1;
-        const int ci = M.children[(info >> 5) + k];
+        const int ci = (info >> 5) + k;
         const RBox ch = M.boxes[ci];
         const long long d = box_dist32(ch, t);
         if (d < best_d || (d == best_d && ch.rank < best_rank)) {

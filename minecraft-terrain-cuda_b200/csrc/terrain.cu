@@ -327,6 +327,7 @@ struct OutSlot {
 
 // ---- the generator ----------------------------------------------------------------------------------
 struct Generator {
+    static constexpr int kTailMin = 512;   // smallest batch the tail split of generate() makes
     int device = 0;
     int max_batch = 2048;
     cudaStream_t stream = nullptr;      // compute stream (the caller's, when set)
@@ -336,7 +337,7 @@ struct Generator {
     bool use_graphs = true;
     std::atomic<bool> served{false};    // owned by a server's worker thread
     // model
-    DevBuf d_boxes, d_tree, d_children, d_leaf_biome, d_leaf_node, d_leaf_rank, d_flags, d_btemp, d_bfrozen;
+    DevBuf d_boxes, d_box_leaf, d_tree, d_children, d_leaf_biome, d_leaf_node, d_leaf_rank, d_flags, d_btemp, d_bfrozen;
     DevModel model{};
     int tree_depth = 0;
     // seeds
@@ -394,7 +395,10 @@ struct Generator {
         ModelHost m;
         build_model_host(m);
         upload(d_tree, m.nodes);
-        if (!m.boxes.empty()) upload(d_boxes, m.boxes);
+        if (!m.boxes.empty()) {
+            upload(d_boxes, m.boxes);
+            upload(d_box_leaf, m.box_leaf);
+        }
         upload(d_children, m.children);
         upload(d_leaf_biome, m.leaf_biome);
         upload(d_leaf_node, m.leaf_node);
@@ -405,6 +409,7 @@ struct Generator {
         if (m.depth >= kSearchStack) throw Error(TG_ERR_INTERNAL, "climate tree deeper than the search stack");
         tree_depth = m.depth;
         model.boxes = m.boxes.empty() ? nullptr : d_boxes.as<RBox>();
+        model.box_leaf = m.boxes.empty() ? nullptr : d_box_leaf.as<int32_t>();
         model.tree = d_tree.as<RNode>();
         model.children = d_children.as<int32_t>();
         model.leaf_biome = d_leaf_biome.as<int32_t>();
@@ -712,8 +717,11 @@ struct Generator {
         if (current_slot < 0) throw Error(TG_ERR_NO_SEED, "tg_set_seed has not been called");
         check_chunks(chunks, count);
         std::vector<int32_t> cx(max_batch), cz(max_batch), cs(max_batch, current_slot);
-        for (int off = 0; off < count; off += max_batch) {
-            const int n = std::min(max_batch, count - off);
+        for (int off = 0; off < count;) {
+            // The copy of the last batch is the one no compute hides: within the last two
+            // batches' worth, halve the batches (down to kTailMin chunks) so that it is short.
+            const int rem = count - off;
+            const int n = rem > 2 * max_batch ? max_batch : std::min(max_batch, std::max((rem + 1) / 2, std::min(rem, kTailMin)));
             for (int i = 0; i < n; ++i) {
                 cx[i] = chunks[off + i].x;
                 cz[i] = chunks[off + i].z;
@@ -724,6 +732,7 @@ struct Generator {
             run_batch(o, n, t, aquifer != nullptr);
             drain(o, {Piece{blocks + static_cast<size_t>(off) * kBlocksPerChunk, biomes ? biomes + static_cast<size_t>(off) * kQuartsPerChunk : nullptr,
                             aquifer ? aquifer + static_cast<size_t>(off) * kBlocksPerChunk : nullptr, 0, n}});
+            off += n;
         }
         finish();
     }

@@ -31,6 +31,7 @@ struct HostRun {
         btemp.assign(tbm::kBiomeTemp, tbm::kBiomeTemp + tbm::kNumBiomes);
         bfrozen.assign(tbm::kBiomeFrozen, tbm::kBiomeFrozen + tbm::kNumBiomes);
         M.boxes = m.boxes.empty() ? nullptr : m.boxes.data();
+        M.box_leaf = m.box_leaf.empty() ? nullptr : m.box_leaf.data();
         M.tree = m.nodes.data();
         M.children = m.children.data();
         M.leaf_biome = m.leaf_biome.data();
