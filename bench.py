@@ -10,8 +10,9 @@ material rules, u16 block states and u8 quart biomes out.
              (tg_generate_device), device time from CUDA events on the launching stream
   e2e        chunks/s through tg_generate with host buffers: the chunk list is copied
              in and every block/biome byte copied out to pinned memory inside the step
-  roofline   the dominant stage's output bytes (198,144 B per chunk: u16 blocks + u8
-             biomes) over its device time, against the measured HBM copy peak
+  roofline   the dominant kernel (the column walk with the rule tree, timed by its own
+             CUDA events): 294,912 B per chunk (u16 blocks + u8 per-block biomes, each read
+             once) over its launch time, against the measured HBM copy peak
   cpu_baseline  the reference's own C++ port (oracle/_ref) on this host's cores, on a
              bounded sample of the same regions
 
@@ -35,6 +36,10 @@ SEED = 0x5445525241494E31   # "TERRAIN1"
 REGIONS = [('origin', 0, 0), ('negative', -62500, -62500), ('border', 117124, 117124)]
 SIDE = 64
 BYTES_PER_CHUNK = 98304 * 2 + 1536
+WALK_BYTES_PER_CHUNK = 98304 * 2 + 98304
+# dram__bytes_read.sum + dram__bytes_write.sum of one 4,096-chunk launch of the walk-rules
+# kernel in this workload (596.56 MB + 238.69 MB), from profiles/walk_rules_traffic.md
+WALK_TRAFFIC_PER_LAUNCH = 835250000
 METRIC = 'bit-exact TERRAIN chunks/s on 1 B200, served vs plain; p50/p99 request latency'
 
 
@@ -335,10 +340,10 @@ def run_ours(args, rank, world, local_rank):
         return
     stage = {k: sum(t[k] for t in stats) for k in ('biome_ms', 'noise_ms', 'aquifer_ms', 'fill_ms', 'surface_ms', 'kernel_ms')}
     launches = sum(t['launches'] for t in stats)
-    dom = max(('biome_ms', 'noise_ms', 'aquifer_ms', 'fill_ms', 'surface_ms'), key=lambda k: stage[k])
+    # dominant kernel: the column walk with the rule tree, timed by its own CUDA events
     calls = len(stats)
-    per_launch_ms = stage[dom] / calls
-    algo_bytes = BYTES_PER_CHUNK * n
+    per_launch_ms = sum(t['walk_rules_ms'] for t in stats) / calls
+    algo_bytes = WALK_BYTES_PER_CHUNK * n
     achieved = algo_bytes / (per_launch_ms / 1000.0) / 1e9
     peak, peak_kind = peaks()
     line = {
@@ -349,10 +354,13 @@ def run_ours(args, rank, world, local_rank):
                    'seed': SEED, 'chunks_per_step': n * nreg, 'batch_chunks': n, 'l2': 'outputs (2.4 GB per step) larger than L2',
                    'parallelism': 'replicas: each GPU runs the full workload' if world > 1 else 'single GPU'},
         'stage_ms_per_step': {k: round(v / args.steps, 3) for k, v in stage.items()},
-        'roofline': {'bound': 'hbm', 'kernel': dom.replace('_ms', ''), 'achieved': round(achieved, 2), 'peak': peak, 'unit': 'GB/s',
-                     'frac': round(achieved / peak, 5), 'traffic': None, 'peak_source': peak_kind,
-                     'note': 'algorithmic bytes = 198,144 B per chunk (u16 blocks + u8 biomes) x 4,096 chunks per launch; the stages are '
-                             'FP32/FP64/INT pipe bound, so the HBM fraction is small by design'},
+        'roofline': {'bound': 'hbm', 'kernel': 'surface_walk_rules', 'achieved': round(achieved, 2), 'peak': peak, 'unit': 'GB/s',
+                     'frac': round(achieved / peak, 5), 'traffic': WALK_TRAFFIC_PER_LAUNCH, 'peak_source': peak_kind,
+                     'launch_ms': round(per_launch_ms, 3), 'share_of_step': round(per_launch_ms * calls / stage['kernel_ms'], 3),
+                     'note': 'algorithmic bytes = 294,912 B per chunk (the u16 block column read once, the u8 per-block biome read once) x '
+                             '4,096 chunks per launch; traffic = dram read + write bytes of one 4,096-chunk launch (ncu, '
+                             'profiles/walk_rules_traffic.md). The kernel is issue- and latency-bound (integer and FP64 rule '
+                             'arithmetic), so its HBM fraction is small'},
         'e2e': {'value': round(e2e_value, 1), 'unit': 'chunks/s', 'h2d_bytes_per_step': int(n * nreg * 8),
                 'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK)},
         'gpu_launches': int(launches),

@@ -598,12 +598,14 @@ struct Generator {
         mark(4);
         launch(k_items<body_surface1, 256>, s, 256 * nmax, B);
         launch(k_items<body_block_biome, 256 * kZoomGroups>, s, 256L * kZoomGroups * nmax, B);
+        mark(6);
 #if TB_FUSED_WALK
         launch(k_items<body_surface_walk_rules, 256, TB_MINB_WALK>, s, 256 * nmax, B);
 #else
         launch(k_items<body_surface_walk, 256>, s, 256 * nmax, B);
         launch(k_items<body_surface_rules, kBlocksPerChunk, TB_MINB_SURFACE2>, s, static_cast<long>(kBlocksPerChunk) * nmax, B);
 #endif
+        mark(7);
         launch(k_items<body_surface_frozen, 256>, s, 256 * nmax, B);
         launch(k_items<body_gather, kQuartsPerChunk>, s, static_cast<long>(kQuartsPerChunk) * nmax, B);
         mark(5);
@@ -619,6 +621,9 @@ struct Generator {
         t->fill_ms += ms[3];
         t->surface_ms += ms[4];
         t->kernel_ms += ms[0] + ms[1] + ms[2] + ms[3] + ms[4];
+        float rules = 0.0f;
+        ck(cudaEventElapsedTime(&rules, ev[6], ev[7]), "elapsed");
+        t->walk_rules_ms += rules;
         t->batches += 1;
     }
 

@@ -29,7 +29,7 @@ class TgConfig(ctypes.Structure):
 
 class TgTiming(ctypes.Structure):
     _fields_ = [(k, ctypes.c_float) for k in ('h2d_ms', 'biome_ms', 'noise_ms', 'aquifer_ms', 'fill_ms', 'surface_ms', 'd2h_ms', 'kernel_ms',
-                                               'wall_ms')] + [('batches', ctypes.c_int32), ('launches', ctypes.c_int32)]
+                                               'wall_ms')] + [('batches', ctypes.c_int32), ('launches', ctypes.c_int32), ('walk_rules_ms', ctypes.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
