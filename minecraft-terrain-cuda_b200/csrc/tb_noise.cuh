@@ -48,6 +48,25 @@ TB_HD TB_FI float gx_of(uint32_t h) { return grad_axis(h, kGxNz, kGxNeg); }
 TB_HD TB_FI float gy_of(uint32_t h) { return grad_axis(h, kGyNz, kGyNeg); }
 TB_HD TB_FI float gz_of(uint32_t h) { return grad_axis(h, kGzNz, kGzNeg); }
 
+// GRADIENT[h & 15] . (dx, dy, dz) as the sum of its two non-zero terms. Each of the 16
+// vectors has exactly two components of +-1 and one of 0: the first term is dx for h < 8
+// and dy otherwise, the second dy for h < 4, dx for h = 12 and 14, dz otherwise; bits 0 and
+// 1 of h negate them. The zero component's product is a signed zero, and adding it to the
+// other two (in either association order, IEEE addition being commutative) changes at
+// most the sign of a zero sum. Through the trilinear lerps a zero's sign reaches only the
+// sign of a zero result, and every octave value is accumulated onto a stack sum that
+// starts at +0 (x + -0 = x, +0 + -0 = +0), so stack values are bit-identical to the
+// three-product forms of the reference.
+TB_HD TB_FI float grad_pair(uint32_t h, float dx, float dy, float dz) {
+    h &= 15u;
+    const float u = h < 8u ? dx : dy;
+    const float v = h < 4u ? dy : ((h == 12u || h == 14u) ? dx : dz);
+    return bitsf(fbits(u) ^ ((h & 1u) << 31)) + bitsf(fbits(v) ^ ((h & 2u) << 30));
+}
+#ifndef TB_GRAD_PAIR
+#define TB_GRAD_PAIR 1
+#endif
+
 constexpr double kWrapLimit = 0x1.fffffffffffffp+23;   // largest double below 2^24
 
 // GradientNoise.wrap: values inside [-L, L) pass unchanged; the rest fold by 2^25.
@@ -86,8 +105,12 @@ TB_HD TB_FI float cell_point(const CellHash& c, float rx, float ry, float rz, fl
         const float dx = (k & 1) ? rx - 1.0f : rx;
         const float dy = (k & 2) ? ry - 1.0f : ry;
         const float dz = (k & 4) ? rz - 1.0f : rz;
+#if TB_GRAD_PAIR
+        d[k] = grad_pair(c.h[k], dx, dy, dz);
+#else
         const float xy = gx_of(c.h[k]) * dx + gy_of(c.h[k]) * dy;
         d[k] = xy + gz_of(c.h[k]) * dz;
+#endif
     }
     return lerp3f(smoothf(rx), smoothf(wy), smoothf(rz), d[0], d[1], d[2], d[3], d[4], d[5], d[6], d[7]);
 }
@@ -100,8 +123,12 @@ TB_HD TB_FI float cell_volume(const CellHash& c, float rx, float rz, float ry, f
         const float dx = (k & 1) ? rx - 1.0f : rx;
         const float dz = (k & 4) ? rz - 1.0f : rz;
         const float dy = (k & 2) ? ry - 1.0f : ry;
+#if TB_GRAD_PAIR
+        d[k] = grad_pair(c.h[k], dx, dy, dz);
+#else
         const float xz = gx_of(c.h[k]) * dx + gz_of(c.h[k]) * dz;
         d[k] = xz + gy_of(c.h[k]) * dy;
+#endif
     }
     return lerp3f(ax, ay, az, d[0], d[1], d[2], d[3], d[4], d[5], d[6], d[7]);
 }
