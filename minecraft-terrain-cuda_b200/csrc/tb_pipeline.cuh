@@ -50,6 +50,7 @@ struct DevModel {
     const int32_t* leaf_node;
     const int32_t* leaf_rank;
     int32_t root;
+    int32_t depth;                  // levels of the climate tree (root = 1)
     const uint8_t* block_flags;     // 1 air, 2 water, 4 lava, 8 fluid
     const float* biome_temp;
     const uint8_t* biome_frozen;
@@ -354,6 +355,39 @@ TB_HD inline int tree_first_min32(const DevModel& M, const int32_t* t, int start
     return best;
 }
 
+// The same search with the descent as nested loops over the tree levels (children of a box
+// are consecutive boxes), for trees of at most kRecDepth levels: the loop state of every
+// level stays in registers instead of a stack in local memory. Same visiting order.
+constexpr int kRecDepth = 6;
+template <int L>
+TB_HD TB_FI void search_level32(const DevModel& M, const int32_t* t, int node, int& best, int& best_rank, long long& best_d) {
+    const int info = M.boxes[node].info;
+    const int first = info >> 5, cnt = info & 31;
+    for (int k = 0; k < cnt; ++k) {
+        const RBox ch = M.boxes[first + k];
+        const long long d = box_dist32(ch, t);
+        if (d < best_d || (d == best_d && ch.rank < best_rank)) {
+            if (ch.info < 0) {
+                best = ~ch.info;
+                best_rank = ch.rank;
+                best_d = d;
+            } else if constexpr (L > 1) {
+                search_level32<L - 1>(M, t, first + k, best, best_rank, best_d);
+            }
+        }
+    }
+}
+TB_HD inline int tree_first_min32_levels(const DevModel& M, const int32_t* t, int start_leaf, long long& best_d) {
+    int best = start_leaf;
+    int best_rank = M.leaf_rank[start_leaf];
+    best_d = box_dist32(M.boxes[M.box_leaf[start_leaf]], t);
+    search_level32<kRecDepth - 1>(M, t, 0, best, best_rank, best_d);
+    return best;
+}
+#ifndef TB_SEARCH_LEVELS
+#define TB_SEARCH_LEVELS 1
+#endif
+
 // One quart column run: climate per quart, quantized targets, first minimal leaf.
 // item = run * (biome chunks * 16) + biome chunk * 16 + column; a run is kRun
 // consecutive quarts in y. A warp holds 32 neighbouring columns at the same heights,
@@ -388,7 +422,9 @@ TB_HD inline void body_climate_quart(const Batch& B, int it) {
             small = small && t[k] >= -kBox32Limit && t[k] <= kBox32Limit;
             t32[k] = static_cast<int32_t>(t[k]);
         }
-        const int leaf = small ? tree_first_min32(B.M, t32, prev, md) : tree_first_min(B.M, t, prev, md);
+        const int leaf = !small                                     ? tree_first_min(B.M, t, prev, md)
+                         : (TB_SEARCH_LEVELS && B.M.depth <= kRecDepth) ? tree_first_min32_levels(B.M, t32, prev, md)
+                                                                        : tree_first_min32(B.M, t32, prev, md);
         prev = leaf;
         const size_t p = static_cast<size_t>(b) * kQuartsPerChunk + chain_pos(qx, qy, qz);
         for (int k = 0; k < 6; ++k) B.tgt[p * 6 + k] = t[k];

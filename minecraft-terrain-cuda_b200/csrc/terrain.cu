@@ -416,6 +416,7 @@ struct Generator {
         model.leaf_node = d_leaf_node.as<int32_t>();
         model.leaf_rank = d_leaf_rank.as<int32_t>();
         model.root = m.root;
+        model.depth = m.depth;
         model.block_flags = d_flags.as<uint8_t>();
         model.biome_temp = d_btemp.as<float>();
         model.biome_frozen = d_bfrozen.as<uint8_t>();

@@ -38,6 +38,7 @@ struct HostRun {
         M.leaf_node = m.leaf_node.data();
         M.leaf_rank = m.leaf_rank.data();
         M.root = m.root;
+        M.depth = m.depth;
         M.block_flags = flags.data();
         M.biome_temp = btemp.data();
         M.biome_frozen = bfrozen.data();
