@@ -1018,41 +1018,49 @@ TB_HD TB_FI float prelim_surface(const Batch& B, int c, int lx, int lz) {
     return a0 + step * 0.0f;
 }
 
+// The 8 channel values of one block: the cell's a0 plus the step added once per block
+// above the cell floor, as in the fill. Out of line, returned in registers.
+struct ChannelValues {
+    float v[tbm::kNumChannels];
+};
+TB_HD TB_NOINLINE inline ChannelValues block_channels(const Batch& B, int c, int lx, int lz, int y) {
+    CellInterp ci;
+    const int cell_y = (y - tbm::kMinY) >> 3, yi = (y - tbm::kMinY) & 7;
+    cell_interp(B, c, lx, lz, cell_y, ci);
+    ChannelValues out;
+    for (int j = 0; j < tbm::kNumChannels; ++j) {
+        float v = ci.a0[j];
+        for (int q = 0; q < yi; ++q) v += ci.step[j];
+        out.v[j] = v;
+    }
+    return out;
+}
+
 // Channel values of one block on first use: the generated ore functions read a channel
-// only under the guards that need it (a vein's y range, for one). Each value is the
-// cell's a0 plus the step added once per block above the cell floor, as in the fill.
+// only under the guards that need it (a vein's y range, for one).
 struct LazyChannels {
     const Batch* B;
     int c, lx, lz, y;
     mutable bool set;
-    mutable float ch[tbm::kNumChannels];
+    mutable ChannelValues cv;
     TB_HD TB_FI float operator[](int k) const {
         if (!set) {
-            CellInterp ci;
-            const int cell_y = (y - tbm::kMinY) >> 3, yi = (y - tbm::kMinY) & 7;
-            cell_interp(*B, c, lx, lz, cell_y, ci);
-            for (int j = 0; j < tbm::kNumChannels; ++j) {
-                float v = ci.a0[j];
-                for (int q = 0; q < yi; ++q) v += ci.step[j];
-                ch[j] = v;
-            }
+            cv = block_channels(*B, c, lx, lz, y);
             set = true;
         }
-        return ch[k];
+        return cv.v[k];
     }
 };
 
-// OreVeinRule for one block: density and richness on the volume path (channel values),
-// the filler gap on the point path. Takes its inputs by value so that the rule context
-// of the caller stays in registers.
-TB_HD TB_NOINLINE inline int ore_vein_at(const Batch& B, int c, int lx, int lz, int bx, int y, int bz, const DevSeed& S, int k, int ore, int raw,
-                                         int filler, float chance) {
+// OreVeinRule past its density test (density > 0): the positional draw, richness on the
+// volume path (channel values), the filler gap on the point path. Inputs by value, so
+// that the rule context of the caller stays in registers.
+TB_HD TB_NOINLINE inline int ore_vein_hit(const Batch& B, int c, int lx, int lz, int bx, int y, int bz, const DevSeed& S, int k, int ore, int raw,
+                                          int filler, float chance, float density) {
     const NoiseTables& T = S.nt;
-    const LazyChannels ch{&B, c, lx, lz, y, false, {}};
-    const float density = tbgen::gen_ore_density(k, T, bx, y, bz, ch);
-    if (density <= 0.0f) return -1;
     Xoro r = S.ore.at(bx, y, bz);
     if (r.next_float() > density) return -1;
+    const LazyChannels ch{&B, c, lx, lz, y, false, {}};
     const float richness = tbgen::gen_ore_richness(k, T, bx, y, bz, ch);
     if (r.next_float() < richness && tbgen::gen_ore_gap(k, T, bx, y, bz) < 0.0f) return r.next_float() < chance ? raw : ore;
     return filler;
@@ -1115,8 +1123,13 @@ struct RuleCtx {
         const int off = jround(static_cast<float>(col->noise<tbm::kNoise_clay_bands_offset>(col->bx, 0.0, col->bz)) * 4.0f);
         return col->S->clay[(y + off + 192) % 192];
     }
+    // OreVeinRule: the density inline (its guards usually end it after a y test), the rest
+    // out of line
     TB_HD TB_FI int ore_vein(int k, int ore, int raw, int filler, float chance) const {
-        return ore_vein_at(*B, c, col->lx, col->lz, col->bx, y, col->bz, *col->S, k, ore, raw, filler, chance);
+        const LazyChannels ch{B, c, col->lx, col->lz, y, false, {}};
+        const float density = tbgen::gen_ore_density(k, col->S->nt, col->bx, y, col->bz, ch);
+        if (density <= 0.0f) return -1;
+        return ore_vein_hit(*B, c, col->lx, col->lz, col->bx, y, col->bz, *col->S, k, ore, raw, filler, chance, density);
     }
 };
 
