@@ -75,10 +75,10 @@ double now_ms() { return std::chrono::duration<double, std::milli>(std::chrono::
 #define TB_MINB_FILL 1
 #endif
 #ifndef TB_MINB_CORNER
-#define TB_MINB_CORNER 1
+#define TB_MINB_CORNER 3
 #endif
 #ifndef TB_MINB_QUART
-#define TB_MINB_QUART 2
+#define TB_MINB_QUART 4
 #endif
 
 // item count = chunks in the batch * MUL
@@ -297,7 +297,7 @@ struct TableBufs {
         count.alloc(sizeof(int32_t));
     }
     HashTab view() const { return HashTab{keys.as<unsigned long long>(), vals.as<int32_t>(), uniq.as<unsigned long long>(), count.as<int32_t>(), cap - 1}; }
-    void reset(cudaStream_t s) {
+    void reset(cudaStream_t s) const {
         ck(cudaMemsetAsync(keys.p, 0xFF, keys.bytes, s), "memset");
         ck(cudaMemsetAsync(count.p, 0, sizeof(int32_t), s), "memset");
     }
@@ -321,6 +321,48 @@ struct OutSlot {
     bool graph_aquifer = false;
     cudaStream_t graph_stream = nullptr;
     bool busy = false;         // outputs not yet drained to the host
+    int lane = 0;              // working buffers and stream its batches use
+};
+
+// The working buffers of one batch in flight (tables, climate, corners, aquifer, heights,
+// per-block biomes). A generator holds one set per lane; two lanes let the batches of the
+// two output slots run concurrently on two streams.
+struct Work {
+    DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_loc, d_aq_status,
+        d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_walk, d_bbiome, d_colrec;
+    TableBufs tb_b, tb_c, tb_s;
+    void alloc(int n) {
+        const size_t N = static_cast<size_t>(n);
+        d_n.alloc(sizeof(int32_t));
+        d_cx.alloc(4 * N);
+        d_cz.alloc(4 * N);
+        d_cs.alloc(4 * N);
+        tb_b.alloc(9 * N);
+        tb_c.alloc(25 * N);
+        tb_s.alloc(static_cast<uint64_t>(kGrid) * N);
+        const size_t nb = 9 * N, cc = 25 * N, sg = static_cast<size_t>(kGrid) * N;
+        d_nb9.alloc(4 * 9 * N);
+        d_bcol.alloc(sizeof(float) * nb * 16 * tbm::kClimateCols);
+        d_tgt.alloc(sizeof(long long) * nb * kQuartsPerChunk * 6);
+        d_lstar.alloc(sizeof(int32_t) * nb * kQuartsPerChunk);
+        d_mdist.alloc(sizeof(long long) * nb * kQuartsPerChunk);
+        d_qbiome.alloc(nb * kQuartsPerChunk);
+        d_c25.alloc(4 * 25 * N);
+        d_ccol.alloc(sizeof(float) * cc * tbm::kCornerCols);
+        d_corners.alloc(sizeof(float) * cc * kRows * tbm::kNumChannels);
+        d_g513.alloc(4 * sg);
+        d_sfts.alloc(sizeof(float) * sg);
+        d_aq_loc.alloc(sizeof(int32_t) * N * kAqCells * 3);
+        d_aq_status.alloc(sizeof(int32_t) * N * kAqCells * 2);
+        d_aq_skip.alloc(4 * N);
+        d_h0.alloc(4 * 256 * N);
+        d_h1.alloc(4 * 256 * N);
+        d_h2.alloc(4 * 256 * N);
+        d_zoom.alloc(sizeof(uint32_t) * N * kZoomVerts);
+        if (!TB_FUSED_WALK) d_walk.alloc(sizeof(uint32_t) * N * kBlocksPerChunk);   // per-block walk states of the split pass
+        d_bbiome.alloc(N * kBlocksPerChunk);
+        d_colrec.alloc(sizeof(ColumnRec) * N * 256);
+    }
 };
 
 }  // namespace
@@ -345,22 +387,26 @@ struct Generator {
     DevBuf d_seeds;
     uint64_t use_clock = 0;
     int current_slot = -1;
-    // batch buffers (shared by both output slots: the kernels of one batch at a time use them)
-    DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_loc, d_aq_status,
-        d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_walk, d_bbiome, d_colrec;
-    TableBufs tb_b, tb_c, tb_s;
+    // working buffers per lane: lane 0 runs on `stream`, lane 1 on lane_stream
+    Work work[2];
+    int lanes = 2;
+    cudaStream_t lane_stream = nullptr;
+    cudaEvent_t ev_entry = nullptr;
     OutSlot out[2];
     int next_out = 0;
     int graph_launches = 0;
 
-    Generator(int dev, int batch) : device(dev), max_batch(batch) {
+    Generator(int dev, int batch, int pipeline_slots) : device(dev), max_batch(batch), lanes(pipeline_slots == 1 ? 1 : 2) {
         ck(cudaSetDevice(device), "cudaSetDevice");
         cudaDeviceProp prop{};
         ck(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
         g_sm_count = prop.multiProcessorCount;
         ck(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
         ck(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaStreamCreateWithFlags(&lane_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaEventCreateWithFlags(&ev_entry, cudaEventDisableTiming), "cudaEventCreate");
         stream = own_stream;
+        out[1].lane = lanes == 2 ? 1 : 0;
         for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
         for (auto& o : out) {
             ck(cudaEventCreateWithFlags(&o.computed, cudaEventDisableTiming), "cudaEventCreate");
@@ -381,6 +427,8 @@ struct Generator {
         }
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        if (ev_entry) cudaEventDestroy(ev_entry);
+        if (lane_stream) cudaStreamDestroy(lane_stream);
         if (copy_stream) cudaStreamDestroy(copy_stream);
         if (own_stream) cudaStreamDestroy(own_stream);
     }
@@ -432,35 +480,7 @@ struct Generator {
 
     void alloc_batch(int n) {
         const size_t N = static_cast<size_t>(n);
-        d_n.alloc(sizeof(int32_t));
-        d_cx.alloc(4 * N);
-        d_cz.alloc(4 * N);
-        d_cs.alloc(4 * N);
-        tb_b.alloc(9 * N);
-        tb_c.alloc(25 * N);
-        tb_s.alloc(static_cast<uint64_t>(kGrid) * N);
-        const size_t nb = 9 * N, cc = 25 * N, sg = static_cast<size_t>(kGrid) * N;
-        d_nb9.alloc(4 * 9 * N);
-        d_bcol.alloc(sizeof(float) * nb * 16 * tbm::kClimateCols);
-        d_tgt.alloc(sizeof(long long) * nb * kQuartsPerChunk * 6);
-        d_lstar.alloc(sizeof(int32_t) * nb * kQuartsPerChunk);
-        d_mdist.alloc(sizeof(long long) * nb * kQuartsPerChunk);
-        d_qbiome.alloc(nb * kQuartsPerChunk);
-        d_c25.alloc(4 * 25 * N);
-        d_ccol.alloc(sizeof(float) * cc * tbm::kCornerCols);
-        d_corners.alloc(sizeof(float) * cc * kRows * tbm::kNumChannels);
-        d_g513.alloc(4 * sg);
-        d_sfts.alloc(sizeof(float) * sg);
-        d_aq_loc.alloc(sizeof(int32_t) * N * kAqCells * 3);
-        d_aq_status.alloc(sizeof(int32_t) * N * kAqCells * 2);
-        d_aq_skip.alloc(4 * N);
-        d_h0.alloc(4 * 256 * N);
-        d_h1.alloc(4 * 256 * N);
-        d_h2.alloc(4 * 256 * N);
-        d_zoom.alloc(sizeof(uint32_t) * N * kZoomVerts);
-        if (!TB_FUSED_WALK) d_walk.alloc(sizeof(uint32_t) * N * kBlocksPerChunk);   // per-block walk states of the split pass
-        d_bbiome.alloc(N * kBlocksPerChunk);
-        d_colrec.alloc(sizeof(ColumnRec) * N * 256);
+        for (int l = 0; l < lanes; ++l) work[l].alloc(n);
         for (auto& o : out) {
             o.blocks.alloc(sizeof(uint16_t) * N * kBlocksPerChunk);
             o.biomes.alloc(N * kQuartsPerChunk);
@@ -512,50 +532,50 @@ struct Generator {
         return s;
     }
 
-    Batch batch_view(const OutSlot* o) const {
+    Batch batch_view(const Work& W, const OutSlot* o) const {
         Batch B{};
         B.M = model;
         B.seeds = d_seeds.as<DevSeed>();
-        B.n_dev = d_n.as<int32_t>();
-        B.cx = d_cx.as<int32_t>();
-        B.cz = d_cz.as<int32_t>();
-        B.cseed = d_cs.as<int32_t>();
-        B.hb = tb_b.view();
+        B.n_dev = W.d_n.as<int32_t>();
+        B.cx = W.d_cx.as<int32_t>();
+        B.cz = W.d_cz.as<int32_t>();
+        B.cseed = W.d_cs.as<int32_t>();
+        B.hb = W.tb_b.view();
         B.nb_cap = 9 * max_batch;
-        B.nb9 = d_nb9.as<int32_t>();
-        B.bcol = d_bcol.as<float>();
-        B.tgt = d_tgt.as<long long>();
-        B.lstar = d_lstar.as<int32_t>();
-        B.mdist = d_mdist.as<long long>();
-        B.qbiome = d_qbiome.as<uint8_t>();
-        B.hc = tb_c.view();
+        B.nb9 = W.d_nb9.as<int32_t>();
+        B.bcol = W.d_bcol.as<float>();
+        B.tgt = W.d_tgt.as<long long>();
+        B.lstar = W.d_lstar.as<int32_t>();
+        B.mdist = W.d_mdist.as<long long>();
+        B.qbiome = W.d_qbiome.as<uint8_t>();
+        B.hc = W.tb_c.view();
         B.cc_cap = 25 * max_batch;
-        B.c25 = d_c25.as<int32_t>();
-        B.ccol = d_ccol.as<float>();
-        B.corners = d_corners.as<float>();
-        B.hs = tb_s.view();
+        B.c25 = W.d_c25.as<int32_t>();
+        B.ccol = W.d_ccol.as<float>();
+        B.corners = W.d_corners.as<float>();
+        B.hs = W.tb_s.view();
         B.sg_cap = kGrid * max_batch;
-        B.g513 = d_g513.as<int32_t>();
-        B.sfts = d_sfts.as<float>();
-        B.aq_loc = d_aq_loc.as<int32_t>();
-        B.aq_status = d_aq_status.as<int32_t>();
-        B.aq_skip = d_aq_skip.as<int32_t>();
+        B.g513 = W.d_g513.as<int32_t>();
+        B.sfts = W.d_sfts.as<float>();
+        B.aq_loc = W.d_aq_loc.as<int32_t>();
+        B.aq_status = W.d_aq_status.as<int32_t>();
+        B.aq_skip = W.d_aq_skip.as<int32_t>();
         B.blocks = o ? o->blocks.as<uint16_t>() : nullptr;
-        B.h0 = d_h0.as<int32_t>();
-        B.h1 = d_h1.as<int32_t>();
-        B.h2 = d_h2.as<int32_t>();
+        B.h0 = W.d_h0.as<int32_t>();
+        B.h1 = W.d_h1.as<int32_t>();
+        B.h2 = W.d_h2.as<int32_t>();
         B.biomes_out = o ? o->biomes.as<uint8_t>() : nullptr;
-        B.zoom_tab = d_zoom.as<uint32_t>();
-        B.walk = d_walk.as<uint32_t>();
-        B.bbiome = d_bbiome.as<uint8_t>();
-        B.colrec = d_colrec.as<ColumnRec>();
+        B.zoom_tab = W.d_zoom.as<uint32_t>();
+        B.walk = W.d_walk.as<uint32_t>();
+        B.bbiome = W.d_bbiome.as<uint8_t>();
+        B.colrec = W.d_colrec.as<ColumnRec>();
         return B;
     }
 
     // biome stage (shared by the TERRAIN step and biome lookups); nmax sizes the grids
-    void enqueue_biomes(const Batch& B, cudaStream_t s, long nmax) {
-        const int32_t* cnt_b = tb_b.count.as<int32_t>();
-        tb_b.reset(s);
+    void enqueue_biomes(const Work& W, const Batch& B, cudaStream_t s, long nmax) {
+        const int32_t* cnt_b = W.tb_b.count.as<int32_t>();
+        W.tb_b.reset(s);
         launch(k_items<body_nb_insert, 9>, s, 9 * nmax, B);
         launch(k_items<body_nb_resolve, 9>, s, 9 * nmax, B);
         launch(k_dyn<body_climate_col, 16>, s, nmax * 16 * 2, B, cnt_b);
@@ -568,23 +588,23 @@ struct Generator {
     }
 
     // every kernel of one batch; with timed set, events split the stages
-    void enqueue_batch(const Batch& B, cudaStream_t s, long nmax, uint16_t* aquifer_dev, bool timed) {
+    void enqueue_batch(const Work& W, const Batch& B, cudaStream_t s, long nmax, uint16_t* aquifer_dev, bool timed) {
         auto mark = [&](int i) {
             if (timed) ck(cudaEventRecord(ev[i], s), "event");
         };
-        const int32_t* cnt_c = tb_c.count.as<int32_t>();
-        const int32_t* cnt_s = tb_s.count.as<int32_t>();
+        const int32_t* cnt_c = W.tb_c.count.as<int32_t>();
+        const int32_t* cnt_s = W.tb_s.count.as<int32_t>();
         mark(0);
-        enqueue_biomes(B, s, nmax);
+        enqueue_biomes(W, B, s, nmax);
         mark(1);
-        tb_c.reset(s);
+        W.tb_c.reset(s);
         launch(k_items<body_cc_insert, 25>, s, 25 * nmax, B);
         launch(k_items<body_cc_resolve, 25>, s, 25 * nmax, B);
         launch(k_dyn<body_corner_col, 1>, s, 16 * nmax, B, cnt_c);
         launch(k_dyn<body_corner, kRows, TB_MINB_CORNER>, s, 16 * nmax * kRows, B, cnt_c);
         launch(k_items<body_zoom_table, kZoomVerts>, s, kZoomVerts * nmax, B);
         mark(2);
-        tb_s.reset(s);
+        W.tb_s.reset(s);
         launch(k_items<body_sg_insert, kGrid>, s, kGrid * nmax, B);
         launch(k_items<body_sg_resolve, kGrid>, s, kGrid * nmax, B);
         launch(k_dyn<body_surface_level, 1>, s, 2 * nmax * 100, B, cnt_s);
@@ -630,18 +650,19 @@ struct Generator {
 
     // Runs one batch whose staged coordinates sit in o.coords into output slot o.
     void run_batch(OutSlot& o, int n, tg_timing* t, bool want_aquifer) {
-        cudaStream_t s = stream;
+        Work& W = work[o.lane];
+        cudaStream_t s = o.lane ? lane_stream : stream;
         if (o.busy) ck(cudaStreamWaitEvent(s, o.drained, 0), "wait");   // the slot's previous outputs are copied out
         const int32_t* h = o.coords.as<int32_t>();
-        ck(cudaMemcpyAsync(d_cx.p, h, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(d_cz.p, h + max_batch, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(d_cs.p, h + 2 * max_batch, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_cx.p, h, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_cz.p, h + max_batch, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_cs.p, h + 2 * max_batch, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
         if (want_aquifer && !o.aquifer.p) o.aquifer.alloc(sizeof(uint16_t) * static_cast<size_t>(max_batch) * kBlocksPerChunk);
-        const Batch B = batch_view(&o);
+        const Batch B = batch_view(W, &o);
         uint16_t* aq = want_aquifer ? o.aquifer.as<uint16_t>() : nullptr;
         if (t) {
-            enqueue_batch(B, s, max_batch, aq, true);
+            enqueue_batch(W, B, s, max_batch, aq, true);
             add_stage_times(t);
         } else if (use_graphs) {
             if (!o.graph || o.graph_aquifer != want_aquifer || o.graph_stream != s) {
@@ -650,7 +671,7 @@ struct Generator {
                 cudaGraph_t g;
                 ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
                 const int before = g_launches;
-                enqueue_batch(B, s, max_batch, aq, false);
+                enqueue_batch(W, B, s, max_batch, aq, false);
                 ck(cudaStreamEndCapture(s, &g), "capture");
                 ck(cudaGraphInstantiate(&o.graph, g, 0), "graph instantiate");
                 cudaGraphDestroy(g);
@@ -662,7 +683,7 @@ struct Generator {
             ck(cudaGraphLaunch(o.graph, s), "graph launch");
             g_launches += graph_launches;
         } else {
-            enqueue_batch(B, s, max_batch, aq, false);
+            enqueue_batch(W, B, s, max_batch, aq, false);
         }
         ck(cudaGetLastError(), "kernel launch");
         ck(cudaEventRecord(o.computed, s), "event");
@@ -717,10 +738,19 @@ struct Generator {
                 o.busy = false;
             }
         ck(cudaStreamSynchronize(stream), "sync");
+        ck(cudaStreamSynchronize(lane_stream), "sync");
+    }
+
+    // lane 1's stream starts after the work already queued on `stream` (the caller's)
+    void order_lanes() {
+        if (lanes < 2) return;
+        ck(cudaEventRecord(ev_entry, stream), "event");
+        ck(cudaStreamWaitEvent(lane_stream, ev_entry, 0), "wait");
     }
 
     void generate(const tg_chunk_xz* chunks, int count, uint16_t* blocks, uint8_t* biomes, uint16_t* aquifer, tg_timing* t) {
         if (current_slot < 0) throw Error(TG_ERR_NO_SEED, "tg_set_seed has not been called");
+        order_lanes();
         check_chunks(chunks, count);
         std::vector<int32_t> cx(max_batch), cz(max_batch), cs(max_batch, current_slot);
         for (int off = 0; off < count;) {
@@ -748,11 +778,12 @@ struct Generator {
         if (count > max_batch) throw Error(TG_ERR_INVALID_ARGUMENT, "count exceeds max_batch_chunks");
         finish();
         OutSlot& o = out[0];
+        Work& W = work[0];
         cudaStream_t s = stream;
-        launch(k_split_chunks, s, count, chunks_dev, count, static_cast<int32_t>(current_slot), d_cx.as<int32_t>(), d_cz.as<int32_t>(), d_cs.as<int32_t>(),
-               d_n.as<int32_t>());
-        const Batch B = batch_view(&o);
-        enqueue_batch(B, s, max_batch, nullptr, t != nullptr);
+        launch(k_split_chunks, s, count, chunks_dev, count, static_cast<int32_t>(current_slot), W.d_cx.as<int32_t>(), W.d_cz.as<int32_t>(),
+               W.d_cs.as<int32_t>(), W.d_n.as<int32_t>());
+        const Batch B = batch_view(W, &o);
+        enqueue_batch(W, B, s, max_batch, nullptr, t != nullptr);
         if (t) add_stage_times(t);
         ck(cudaMemcpyAsync(blocks_dev, o.blocks.p, sizeof(uint16_t) * count * kBlocksPerChunk, cudaMemcpyDeviceToDevice, s), "d2d");
         if (biomes_dev) ck(cudaMemcpyAsync(biomes_dev, o.biomes.p, static_cast<size_t>(count) * kQuartsPerChunk, cudaMemcpyDeviceToDevice, s), "d2d");
@@ -778,16 +809,17 @@ struct Generator {
                 if (std::find(used.begin(), used.end(), cs[i]) == used.end()) used.push_back(cs[i]);
             }
             OutSlot& o = out[0];
+            Work& W = work[0];
             stage(o, m, cx.data(), cz.data(), cs.data());
             const int32_t* h = o.coords.as<int32_t>();
             cudaStream_t s = stream;
-            ck(cudaMemcpyAsync(d_cx.p, h, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
-            ck(cudaMemcpyAsync(d_cz.p, h + max_batch, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
-            ck(cudaMemcpyAsync(d_cs.p, h + 2 * max_batch, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
-            ck(cudaMemcpyAsync(d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
+            ck(cudaMemcpyAsync(W.d_cx.p, h, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
+            ck(cudaMemcpyAsync(W.d_cz.p, h + max_batch, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
+            ck(cudaMemcpyAsync(W.d_cs.p, h + 2 * max_batch, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
+            ck(cudaMemcpyAsync(W.d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
             ck(cudaMemcpyAsync(d_xyz.p, xyz + 3 * off, sizeof(int32_t) * 3 * m, cudaMemcpyHostToDevice, s), "h2d");
-            const Batch B = batch_view(nullptr);
-            enqueue_biomes(B, s, m);
+            const Batch B = batch_view(W, nullptr);
+            enqueue_biomes(W, B, s, m);
             launch(k_biome_lookup, s, m, B, d_xyz.as<int32_t>(), d_res.as<uint8_t>());
             ck(cudaMemcpyAsync(res + off, d_res.p, m, cudaMemcpyDeviceToHost, s), "d2h");
             ck(cudaStreamSynchronize(s), "sync");
@@ -818,14 +850,15 @@ struct Generator {
         }
         h[3 * max_batch] = n;
         cudaStream_t s = stream;
+        Work& W = work[0];
         ck(cudaMemsetAsync(scratch, 0, sizeof(unsigned int), s), "memset");   // the finished count starts at zero
-        ck(cudaMemcpyAsync(d_cx.p, h, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(d_cz.p, h + max_batch, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(d_cs.p, h + 2 * max_batch, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_cx.p, h, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_cz.p, h + max_batch, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_cs.p, h + 2 * max_batch, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
         ck(cudaMemcpyAsync(scratch + kNoAllocXyzOff, xyz, sizeof(int32_t) * 3 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
-        const Batch B = batch_view(nullptr);
-        enqueue_biomes(B, s, n);
+        const Batch B = batch_view(W, nullptr);
+        enqueue_biomes(W, B, s, n);
         launch(k_biome_lookup_scratch, s, n, B, scratch);
         ck(cudaGetLastError(), "kernel launch");
         unsigned int finished = 0;
@@ -838,6 +871,7 @@ struct Generator {
 
     // Multi-seed batch: requests are cut into device batches; a batch mixes seeds.
     void generate_batch(const tg_request* req, int n, tg_timing* t) {
+        order_lanes();
         for (int r = 0; r < n; ++r) {
             if (req[r].count < 0 || (req[r].count > 0 && (!req[r].chunks || !req[r].blocks_out))) throw Error(TG_ERR_INVALID_ARGUMENT, "bad request");
             check_chunks(req[r].chunks, req[r].count);
@@ -1190,7 +1224,7 @@ tg_status tg_create(const char* ir_json_path, const char* terrain_json_path, con
         if (config && (config->pipeline_slots < 0 || config->pipeline_slots > 2)) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "pipeline_slots must be 0, 1 or 2");
         const int dev = config ? config->device : 0;
         auto h = std::make_unique<tg_generator>();
-        h->g = std::make_unique<tb::Generator>(dev, batch);
+        h->g = std::make_unique<tb::Generator>(dev, batch, config ? config->pipeline_slots : 0);
         *out = h.release();
     });
 }
