@@ -1072,11 +1072,29 @@ struct Server {
             ck(cudaSetDevice(g->device), "cudaSetDevice");
             std::deque<InFlight> flight;
             std::vector<int32_t> cx(g->max_batch), cz(g->max_batch), cs(g->max_batch);
+            auto unissued = [&] {
+                for (Req* r : active)
+                    if (r->issued < static_cast<int>(r->chunks.size())) return true;
+                return false;
+            };
             for (;;) {
+                // retire the batches whose copies have landed, without blocking
+                while (!flight.empty()) {
+                    const cudaError_t q = cudaEventQuery(g->out[flight.front().out].drained);
+                    if (q == cudaErrorNotReady) break;
+                    ck(q, "event query");
+                    complete_batch(flight.front());
+                    flight.pop_front();
+                }
                 std::vector<Req*> admitted;
                 {
                     std::unique_lock<std::mutex> l(mu);
-                    cv_work.wait(l, [&] { return stop || !queue.empty() || !flight.empty() || !active.empty(); });
+                    // idle until a request arrives; with batches in flight, wake every 100 us to
+                    // retire them (a new request wakes the worker at once)
+                    if (!stop && queue.empty() && !unissued()) {
+                        if (flight.empty()) cv_work.wait(l, [&] { return stop || !queue.empty(); });
+                        else cv_work.wait_for(l, std::chrono::microseconds(100), [&] { return stop || !queue.empty(); });
+                    }
                     if (stop && flight.empty()) break;
                     // admission: chunks still to issue across the active set stay within the limit
                     long pending = 0;
@@ -1141,11 +1159,6 @@ struct Server {
                     g->drain(o, pieces);
                     f.out = oi;
                     flight.push_back(std::move(f));
-                    continue;
-                }
-                if (!flight.empty()) {
-                    complete_batch(flight.front());
-                    flight.pop_front();
                 }
             }
         } catch (const Error& e) {
