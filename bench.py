@@ -107,7 +107,8 @@ class ClockSampler:
 
 
 def cpu_baseline(threads=None, sample_side=8):
-    """The reference C++ port on this host: an 8x8-chunk square of each region."""
+    """The reference C++ port on this host: an 8x8-chunk square of each region on all threads,
+    and a 2x2 square of each region on one thread."""
     import ref_oracle
     if not ref_oracle.available():
         return None
@@ -119,9 +120,15 @@ def cpu_baseline(threads=None, sample_side=8):
     t0 = time.perf_counter()
     s.generate(chunks, threads=threads)
     dt = time.perf_counter() - t0
+    one = np.concatenate([region_chunks(x0, z0, 2) for _, x0, z0 in REGIONS])
+    t0 = time.perf_counter()
+    s.generate(one, threads=1)
+    dt1 = time.perf_counter() - t0
     return {'value': round(len(chunks) / dt, 2), 'unit': 'chunks/s', 'cores': threads, 'kind': 'reference',
+            'value_1_thread': round(len(one) / dt1, 2),
             'sample': '%d chunks: an %dx%d square at the corner of each of the three regions, region form (biomes of the '
-                      'square plus a 1-chunk border, then fill + surface per chunk), %d threads' % (len(chunks), sample_side, sample_side, threads)}
+                      'square plus a 1-chunk border, then fill + surface per chunk), %d threads; 1-thread figure from a 2x2 square '
+                      'per region (%d chunks)' % (len(chunks), sample_side, sample_side, threads, len(one))}
 
 
 def run_reference(args, rank):
@@ -159,6 +166,22 @@ def run_reference(args, rank):
                              'sample': '%d chunks per step, 4x8 per region' % per_step},
             'e2e': {'value': round(v, 2), 'unit': 'chunks/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line))
+
+
+def pcie_d2h_gbs(nbytes=1 << 30, reps=5):
+    """Device-to-pinned-host copy bandwidth of this box (GB/s), one 1 GiB copy at a time."""
+    import torch
+    d = torch.empty(nbytes, dtype=torch.uint8, device='cuda')
+    h = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    h.copy_(d, non_blocking=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        h.copy_(d, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    return round(reps * nbytes / (e0.elapsed_time(e1) / 1000.0) / 1e9, 2)
 
 
 def max_over_ranks(value, world, device=None):
@@ -269,6 +292,82 @@ def served_bench(g, n_unique=96, repeats=4, batch_sizes=(512, 768, 1024), loads=
     return out
 
 
+def batched_bench(g, n_seeds=256, seed=3):
+    """Many seeds and uneven chunk lists in one tg_generate_batch call: 256 seeds, list sizes
+    log-uniform in [1, 1024]; each list a contiguous square, scattered chunks within +/-117,187,
+    or chunks straddling the noise-lattice wrap at chunk 6128 / -6129. Outputs to pinned host
+    memory (requests share one pool; only the time is used)."""
+    import ctypes
+    import torch
+    import terrain_b200
+    rng = np.random.default_rng(seed)
+    seeds = [int(v) for v in rng.integers(-(1 << 62), 1 << 62, n_seeds)]
+    lists = []
+    for k in range(n_seeds):
+        n = int(min(1024, max(1, round(np.exp(rng.uniform(0, np.log(1024)))))))
+        kind = k % 3
+        if kind == 0:
+            side = int(np.ceil(np.sqrt(n)))
+            x0, z0 = (int(v) for v in rng.integers(-117187, 117187 - side, 2))
+            c = [(x0 + i % side, z0 + i // side) for i in range(n)]
+        elif kind == 1:
+            c = [(int(a), int(b)) for a, b in rng.integers(-117187, 117188, (n, 2))]
+        else:
+            xs = rng.choice(np.array([6127, 6128, 6129, -6128, -6129, -6130]), n)
+            c = [(int(a), int(b)) for a, b in zip(xs, rng.integers(-117187, 117188, n))]
+        lists.append(np.array(c, np.int32))
+    total = sum(len(c) for c in lists)
+    biggest = max(len(c) for c in lists)
+    pool_b = torch.empty(biggest * 98304, dtype=torch.int16, pin_memory=True).numpy().view(np.uint16)
+    pool_q = torch.empty(biggest * 1536, dtype=torch.uint8, pin_memory=True).numpy()
+    reqs = (terrain_b200.TgRequest * n_seeds)()
+    for i, c in enumerate(lists):
+        reqs[i].seed = seeds[i]
+        reqs[i].chunks = c.ctypes.data_as(ctypes.POINTER(terrain_b200.TgChunk))
+        reqs[i].count = len(c)
+        reqs[i].blocks_out = pool_b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))
+        reqs[i].biomes_out = pool_q.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+    for sd in seeds:
+        g.set_seed(sd)
+    t = terrain_b200.TgTiming()
+    g._check(g.L.tg_generate_batch(g.h, reqs, n_seeds, ctypes.byref(t)))          # warm-up (graphs)
+    best = None
+    for _ in range(3):
+        t0 = time.perf_counter()
+        g._check(g.L.tg_generate_batch(g.h, reqs, n_seeds, None))
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return {'seeds': n_seeds, 'chunks': total, 'chunks_per_s': round(total / best, 1), 'ms': round(best * 1000, 2),
+            'form': 'tg_generate_batch, device batches of up to 4,096 chunks mixing seeds, outputs copied to pinned host memory',
+            'lists': 'log-uniform sizes 1..1024; squares, scattered within +/-117,187, and wrap-straddling chunks 6127..6129 / -6128..-6130'}
+
+
+def biome_stream_bench(g, n_seeds=1024, per_seed=16384, seed=5):
+    """Biome-only lookups: n_seeds seeds x per_seed positions (x, z uniform in +/-1,874,999,
+    y uniform in [-64, 319]) through tg_biome_lookup; the per-seed tables are built inside the
+    call as seeds arrive (more seeds than stay resident), so their setup is part of the time."""
+    rng = np.random.default_rng(seed)
+    seeds = np.repeat(np.array([int(v) for v in rng.integers(-(1 << 62), 1 << 62, n_seeds)], np.int64), per_seed)
+    n = n_seeds * per_seed
+    xyz = np.empty((n, 3), np.int32)
+    xyz[:, 0] = rng.integers(-1874999, 1875000, n)
+    xyz[:, 1] = rng.integers(-64, 320, n)
+    xyz[:, 2] = rng.integers(-1874999, 1875000, n)
+    g.biome_lookup(seeds[:per_seed], xyz[:per_seed])                                      # warm-up
+    t0 = time.perf_counter()
+    g.biome_lookup(seeds, xyz)
+    dt = time.perf_counter() - t0
+    # resident tables: the last seeds of the stream again (their tables are still loaded)
+    k = min(n_seeds, 256) * per_seed
+    t0 = time.perf_counter()
+    g.biome_lookup(seeds[-k:], xyz[-k:])
+    dt_res = time.perf_counter() - t0
+    return {'lookups': n, 'seeds': n_seeds, 'lookups_per_s': round(n / dt, 1), 'ms': round(dt * 1000, 1),
+            'resident_lookups_per_s': round(k / dt_res, 1),
+            'form': 'tg_biome_lookup: one thread per position, zoom corner then that quart\'s climate, R-tree minimum and tie test, '
+                    'replaying the chunk chain only from the nearest earlier quart whose result is fixed'}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import terrain_b200
@@ -337,6 +436,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ms_e2e = max_over_ranks(e2.elapsed_time(e3), world, 'cuda')
     e2e_value = chunks_total / (ms_e2e / 1000.0)
+    pcie = pcie_d2h_gbs()
 
     if rank != 0:
         return
@@ -364,13 +464,18 @@ def run_ours(args, rank, world, local_rank):
                              'profiles/walk_rules_traffic.md). The kernel is issue- and latency-bound (integer and FP64 rule '
                              'arithmetic), so its HBM fraction is small'},
         'e2e': {'value': round(e2e_value, 1), 'unit': 'chunks/s', 'h2d_bytes_per_step': int(n * nreg * 8),
-                'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK)},
+                'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK), 'd2h_gbs': round(e2e_value * BYTES_PER_CHUNK / 1e9, 2),
+                'pcie_d2h_gbs_measured': pcie, 'pcie_frac': round(e2e_value * BYTES_PER_CHUNK / 1e9 / pcie, 3) if pcie else None},
         'gpu_launches': int(launches),
         'clocks': clk.summary(),
     }
     if not args.no_serve:
         g.set_stream(0)
         line['served'] = served_bench(g)
+    if not args.no_extra:
+        g.set_stream(0)
+        line['batched'] = batched_bench(g)
+        line['biome_stream'] = biome_stream_bench(g)
     if not args.no_cpu_baseline:
         line['cpu_baseline'] = cpu_baseline()
     print(json.dumps(line))
@@ -384,6 +489,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-serve', action='store_true', help='skip the served-versus-plain request-stream measurement')
+    ap.add_argument('--no-extra', action='store_true', help='skip the batched-seeds and biome-stream measurements')
     ap.add_argument('--profile-small', action='store_true',
                     help='one untimed step over a 32x32-chunk corner of each region, 1,024-chunk batches (a small case for ncu captures)')
     args = ap.parse_args()

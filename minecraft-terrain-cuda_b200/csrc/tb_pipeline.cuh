@@ -388,6 +388,84 @@ TB_HD inline int tree_first_min32_levels(const DevModel& M, const int32_t* t, in
 #define TB_SEARCH_LEVELS 1
 #endif
 
+// Whether a leaf other than `leaf` reaches distance m (the minimum) from target t: then the
+// chain's previous result may be kept over the first minimal leaf. Boxes farther than m
+// are pruned.
+template <int L>
+TB_HD TB_FI bool other_min_level32(const DevModel& M, const int32_t* t, int node, int leaf, long long m) {
+    const int info = M.boxes[node].info;
+    const int first = info >> 5, cnt = info & 31;
+    for (int k = 0; k < cnt; ++k) {
+        const RBox ch = M.boxes[first + k];
+        const long long d = box_dist32(ch, t);
+        if (d > m) continue;
+        if (ch.info < 0) {
+            if (~ch.info != leaf) return true;
+        } else if constexpr (L > 1) {
+            if (other_min_level32<L - 1>(M, t, first + k, leaf, m)) return true;
+        }
+    }
+    return false;
+}
+TB_HD inline bool tree_other_min(const DevModel& M, const long long* t, int leaf, long long m) {
+    int stack_node[kSearchStack], stack_next[kSearchStack];
+    int sp = 1;
+    stack_node[0] = M.root;
+    stack_next[0] = 0;
+    while (sp > 0) {
+        const RNode& nd = M.tree[stack_node[sp - 1]];
+        const int k = stack_next[sp - 1];
+        if (k >= nd.child_count) {
+            --sp;
+            continue;
+        }
+        stack_next[sp - 1] = k + 1;
+        const int ci = M.children[nd.first_child + k];
+        const RNode& ch = M.tree[ci];
+        if (param_dist(ch, t) > m) continue;
+        if (ch.leaf >= 0) {
+            if (ch.leaf != leaf) return true;
+        } else if (sp < kSearchStack) {
+            stack_node[sp] = ci;
+            stack_next[sp] = 0;
+            ++sp;
+        }
+    }
+    return false;
+}
+
+// One quart on its own (biome lookups): climate, quantized target, the first minimal leaf,
+// the minimum distance, and whether another leaf reaches it. (X, Z) are absolute quart
+// coordinates, qy the quart row 0..height/4-1.
+struct QuartLeaf {
+    int leaf;
+    bool tie;
+    long long m;
+    long long t[6];
+};
+TB_HD TB_NOINLINE inline QuartLeaf quart_leaf(const DevModel& M, const DevSeed& S, int X, int qy, int Z) {
+    const int x = 4 * X, y = tbm::kMinY + 4 * qy, z = 4 * Z;
+    float col[tbm::kClimateCols], cl[6];
+    tbgen::gen_climate_col(S.nt, x, z, col);
+    tbgen::gen_climate(S.nt, x, y, z, col, cl);
+    QuartLeaf q;
+    bool small = M.boxes != nullptr && M.depth <= kRecDepth;
+    int32_t t32[6];
+    for (int k = 0; k < 6; ++k) {
+        q.t[k] = f2l(cl[k] * 10000.0f);
+        small = small && q.t[k] >= -kBox32Limit && q.t[k] <= kBox32Limit;
+        t32[k] = static_cast<int32_t>(q.t[k]);
+    }
+    if (small) {
+        q.leaf = tree_first_min32_levels(M, t32, 0, q.m);
+        q.tie = other_min_level32<kRecDepth - 1>(M, t32, 0, q.leaf, q.m);
+    } else {
+        q.leaf = tree_first_min(M, q.t, 0, q.m);
+        q.tie = tree_other_min(M, q.t, q.leaf, q.m);
+    }
+    return q;
+}
+
 // One quart column run: climate per quart, quantized targets, first minimal leaf.
 // item = run * (biome chunks * 16) + biome chunk * 16 + column; a run is kRun
 // consecutive quarts in y. A warp holds 32 neighbouring columns at the same heights,
@@ -785,8 +863,9 @@ TB_HD TB_FI int zoom_stored(const Batch& B, int c, int best, int px, int py, int
     const int b = B.nb9[static_cast<size_t>(c) * 9 + (dcz + 1) * 3 + dcx + 1];
     return B.qbiome[static_cast<size_t>(b) * kQuartsPerChunk + (cqy * 4 + (qz & 3)) * 4 + (qx & 3)];
 }
+// The index (x 4 + y 2 + z 1 steps) of the fiddled corner nearest to block (x, y, z).
 template <class Fiddles>
-TB_HD TB_FI int zoom_pick(const Batch& B, int c, int x, int y, int z, Fiddles fid) {
+TB_HD TB_FI int zoom_best(int x, int y, int z, Fiddles fid) {
     const int ax = x - 2, ay = y - 2, az = z - 2;
     const int px = ax >> 2, py = ay >> 2, pz = az >> 2;
     const double fx = static_cast<double>(ax & 3) / 4.0, fy = static_cast<double>(ay & 3) / 4.0, fz = static_cast<double>(az & 3) / 4.0;
@@ -806,7 +885,12 @@ TB_HD TB_FI int zoom_pick(const Batch& B, int c, int x, int y, int z, Fiddles fi
             best_d = d;
         }
     }
-    return zoom_stored(B, c, best, px, py, pz);
+    return best;
+}
+template <class Fiddles>
+TB_HD TB_FI int zoom_pick(const Batch& B, int c, int x, int y, int z, Fiddles fid) {
+    const int best = zoom_best(x, y, z, fid);
+    return zoom_stored(B, c, best, (x - 2) >> 2, (y - 2) >> 2, (z - 2) >> 2);
 }
 
 // any position (biome lookups): the LCG chains computed in place
@@ -819,6 +903,37 @@ TB_HD TB_NOINLINE inline int zoom_biome_tab(const Batch& B, int c, int x, int y,
     const uint32_t* tab = B.zoom_tab + static_cast<size_t>(c) * kZoomVerts;
     const int qx0 = B.cx[c] * 4 - 1, qz0 = B.cz[c] * 4 - 1;
     return zoom_pick(B, c, x, y, z, [&](int qx, int qy, int qz) { return tab[((qy - kZoomQyMin) * 6 + (qz - qz0)) * 6 + (qx - qx0)]; });
+}
+
+// BiomeManager.getBiome at one block with the chunk chain's exact result, from the quart
+// alone where its minimum is unique (the chain's previous result cannot be kept there) and
+// otherwise from the nearest earlier quart of the chunk's chain order whose result is
+// fixed (unique minimum, or the chunk's first quart), replaying the chain from it.
+TB_HD inline int biome_point(const DevModel& M, const DevSeed& S, int x, int y, int z) {
+    const int best = zoom_best(x, y, z, [&](int qx, int qy, int qz) { return zoom_fiddles(S.zoom_seed, qx, qy, qz); });
+    const int px = (x - 2) >> 2, py = (y - 2) >> 2, pz = (z - 2) >> 2;
+    const int qx = (best & 4) == 0 ? px : px + 1;
+    const int qy = (best & 2) == 0 ? py : py + 1;
+    const int qz = (best & 1) == 0 ? pz : pz + 1;
+    constexpr int qmin = tbm::kMinY >> 2, qh = tbm::kHeight / 4;
+    const int cqy = (qy < qmin ? qmin : (qy > qmin + qh - 1 ? qmin + qh - 1 : qy)) - qmin;
+    const int X0 = (qx >> 2) * 4, Z0 = (qz >> 2) * 4;   // the chunk's first quart column
+    const int p = chain_pos(qx & 3, cqy, qz & 3);
+    QuartLeaf q = quart_leaf(M, S, qx, cqy, qz);
+    if (!q.tie || p == 0) return M.leaf_biome[q.leaf];
+    int j = p - 1, a, b, c;
+    for (;; --j) {
+        chain_quart(j, a, b, c);
+        q = quart_leaf(M, S, X0 + a, b, Z0 + c);
+        if (!q.tie || j == 0) break;
+    }
+    int r = q.leaf;
+    for (int k = j + 1; k <= p; ++k) {
+        chain_quart(k, a, b, c);
+        const QuartLeaf u = quart_leaf(M, S, X0 + a, b, Z0 + c);
+        r = (r != u.leaf && param_dist(M.tree[M.leaf_node[r]], u.t) == u.m) ? r : u.leaf;
+    }
+    return M.leaf_biome[r];
 }
 
 // item = chunk * kZoomVerts + vertex

@@ -166,12 +166,13 @@ __global__ void __launch_bounds__(256) k_chain_warp(const __grid_constant__ Batc
     for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) chain_warp(B, w, lane);
 }
 
-// one lookup position per item: the zoomed biome from its chunk's neighbourhood
-__global__ void k_biome_lookup(const __grid_constant__ Batch B, const int32_t* xyz, uint8_t* out) {
-    const int n = *B.n_dev;
+// one lookup position per item, on its own: the zoomed quart and its chain result (biome_point)
+__global__ void k_biome_point(const __grid_constant__ DevModel M, const DevSeed* seeds, const int32_t* slot, const int32_t* xyz, int n,
+                              uint8_t* out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        out[i] = static_cast<uint8_t>(zoom_biome(B, i, B.seeds[B.cseed[i]].zoom_seed, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+        out[i] = static_cast<uint8_t>(biome_point(M, seeds[slot[i]], xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
 }
+
 
 // ---- scratch of the no-allocation biome lookup ---------------------------------------------------
 // tg_biome_lookup_noalloc stages its positions and results in this fixed device array
@@ -191,7 +192,8 @@ constexpr size_t kNoAllocOutOff = kNoAllocXyzOff + sizeof(int32_t) * 3 * kNoAllo
 constexpr size_t kNoAllocBytes = kNoAllocOutOff + kNoAllocMaxLookups;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// k_biome_lookup with its positions and results in the no-allocation scratch; counts the
+// Zoomed biomes of the positions staged in the no-allocation scratch, each from its chunk's
+// neighbourhood computed by the biome stage; writes them to the scratch and counts the
 // positions it finished into the scratch header.
 __global__ void k_biome_lookup_scratch(const __grid_constant__ Batch B, unsigned char* scratch) {
     const int n = *B.n_dev;
@@ -791,38 +793,47 @@ struct Generator {
         ck(cudaStreamSynchronize(s), "sync");
     }
 
+    // Biome lookups at independent positions: one thread per position computes the zoomed
+    // quart and its exact chain result on its own (biome_point), so scattered positions cost
+    // one quart each instead of the 3x3 chunk neighbourhood. Positions go in sub-batches of
+    // up to 2^20 whose distinct seeds fit the resident seed slots.
     void biome_lookup(const int64_t* seeds, const int32_t* xyz, int n, uint8_t* res) {
-        std::vector<int32_t> cx(max_batch), cz(max_batch), cs(max_batch);
-        DevBuf d_xyz, d_res;
-        d_xyz.alloc(sizeof(int32_t) * 3 * max_batch);
-        d_res.alloc(max_batch);
+        const int cap = std::min(n, 1 << 20);
+        if (cap <= 0) return;
         finish();
-        for (int off = 0; off < n; off += max_batch) {
-            const int m = std::min(max_batch, n - off);
+        DevBuf d_xyz, d_slot, d_res;
+        d_xyz.alloc(sizeof(int32_t) * 3 * static_cast<size_t>(cap));
+        d_slot.alloc(sizeof(int32_t) * static_cast<size_t>(cap));
+        d_res.alloc(static_cast<size_t>(cap));
+        std::vector<int32_t> slot_of(cap);
+        cudaStream_t s = stream;
+        for (int off = 0; off < n;) {
             std::vector<int> used;
-            for (int i = 0; i < m; ++i) {
-                const int32_t* p = xyz + 3 * (off + i);
-                cx[i] = p[0] >> 4;
-                cz[i] = p[2] >> 4;
-                if (cx[i] <= -(1 << 23) || cx[i] >= (1 << 23) || cz[i] <= -(1 << 23) || cz[i] >= (1 << 23)) throw Error(TG_ERR_RANGE, "position out of range");
-                cs[i] = seed_slot(seeds[off + i], used);
-                if (std::find(used.begin(), used.end(), cs[i]) == used.end()) used.push_back(cs[i]);
+            std::unordered_map<int64_t, int> seen;
+            int m = 0;
+            for (; m < cap && off + m < n; ++m) {
+                const int32_t* p = xyz + 3 * static_cast<size_t>(off + m);
+                const int32_t cx = p[0] >> 4, cz = p[2] >> 4;
+                if (cx <= -(1 << 23) || cx >= (1 << 23) || cz <= -(1 << 23) || cz >= (1 << 23)) throw Error(TG_ERR_RANGE, "position out of range");
+                const int64_t sd = seeds[off + m];
+                auto it = seen.find(sd);
+                if (it != seen.end()) {
+                    slot_of[m] = it->second;
+                    continue;
+                }
+                if (static_cast<int>(used.size()) == kMaxSlots) break;
+                const int sl = seed_slot(sd, used);
+                used.push_back(sl);
+                seen.emplace(sd, sl);
+                slot_of[m] = sl;
             }
-            OutSlot& o = out[0];
-            Work& W = work[0];
-            stage(o, m, cx.data(), cz.data(), cs.data());
-            const int32_t* h = o.coords.as<int32_t>();
-            cudaStream_t s = stream;
-            ck(cudaMemcpyAsync(W.d_cx.p, h, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
-            ck(cudaMemcpyAsync(W.d_cz.p, h + max_batch, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
-            ck(cudaMemcpyAsync(W.d_cs.p, h + 2 * max_batch, 4 * m, cudaMemcpyHostToDevice, s), "h2d");
-            ck(cudaMemcpyAsync(W.d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
-            ck(cudaMemcpyAsync(d_xyz.p, xyz + 3 * off, sizeof(int32_t) * 3 * m, cudaMemcpyHostToDevice, s), "h2d");
-            const Batch B = batch_view(W, nullptr);
-            enqueue_biomes(W, B, s, m);
-            launch(k_biome_lookup, s, m, B, d_xyz.as<int32_t>(), d_res.as<uint8_t>());
-            ck(cudaMemcpyAsync(res + off, d_res.p, m, cudaMemcpyDeviceToHost, s), "d2h");
+            ck(cudaMemcpyAsync(d_xyz.p, xyz + 3 * static_cast<size_t>(off), sizeof(int32_t) * 3 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s), "h2d");
+            ck(cudaMemcpyAsync(d_slot.p, slot_of.data(), sizeof(int32_t) * static_cast<size_t>(m), cudaMemcpyHostToDevice, s), "h2d");
+            launch(k_biome_point, s, m, model, d_seeds.as<DevSeed>(), d_slot.as<int32_t>(), d_xyz.as<int32_t>(), m, d_res.as<uint8_t>());
+            ck(cudaGetLastError(), "kernel launch");
+            ck(cudaMemcpyAsync(res + off, d_res.p, static_cast<size_t>(m), cudaMemcpyDeviceToHost, s), "d2h");
             ck(cudaStreamSynchronize(s), "sync");
+            off += m;
         }
     }
 

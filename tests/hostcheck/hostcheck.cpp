@@ -302,6 +302,15 @@ int hc_tree_visits(const long long* t, int32_t n, int32_t* visits, int32_t* leav
 }
 
 extern "C" {
+// Biome lookups of one seed through the single-block path (biome_point): n xyz triples.
+int hc_biome_point(int64_t seed, const int32_t* xyz, int32_t n, uint8_t* out) {
+    HostRun R(seed);
+    for (int i = 0; i < n; ++i) out[i] = static_cast<uint8_t>(biome_point(R.M, R.D, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+    return 0;
+}
+}
+
+extern "C" {
 // Climate tree shape: depth (root = 1), node count, whether the 32-bit search applies.
 int hc_tree_info(int32_t* out3) {
     ModelHost m;

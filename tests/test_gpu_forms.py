@@ -86,6 +86,21 @@ def test_biome_lookup_matches_reference(gpu_gen, ref_model):
         assert (got[sel] == want).all(), 'seed %d' % s
 
 
+def test_biome_lookup_dense_and_many_seeds(gpu_gen, ref_model):
+    """Lookups packed into a few chunks (so chain ties are replayed from earlier quarts), y
+    outside the world (clamped quart rows), and 40 seeds interleaved position by position."""
+    rng = np.random.default_rng(17)
+    n = 4000
+    xyz = np.stack([rng.integers(-48, 48, n), rng.integers(-90, 345, n), rng.integers(-48, 48, n)], 1).astype(np.int32)
+    pool = np.array([int(v) for v in rng.integers(-(1 << 62), 1 << 62, 40)], np.int64)
+    seeds = pool[rng.integers(0, 40, n)]
+    got = gpu_gen.biome_lookup(seeds, xyz)
+    for s in np.unique(seeds):
+        sel = seeds == s
+        want = ref_model.seed(int(s)).biome_lookup(xyz[sel])
+        assert (got[sel] == want).all(), 'seed %d' % s
+
+
 def test_errors_are_status_codes(gpu_gen):
     with pytest.raises(terrain_b200.TerrainError) as e:
         gpu_gen.generate([(1 << 23, 0)])
