@@ -909,17 +909,28 @@ TB_HD TB_NOINLINE inline int zoom_biome_tab(const Batch& B, int c, int x, int y,
 // alone where its minimum is unique (the chain's previous result cannot be kept there) and
 // otherwise from the nearest earlier quart of the chunk's chain order whose result is
 // fixed (unique minimum, or the chunk's first quart), replaying the chain from it.
-TB_HD inline int biome_point(const DevModel& M, const DevSeed& S, int x, int y, int z) {
-    const int best = zoom_best(x, y, z, [&](int qx, int qy, int qz) { return zoom_fiddles(S.zoom_seed, qx, qy, qz); });
+// The quart BiomeManager.getBiome reads for block (x, y, z): absolute quart x / z, the quart
+// row clamped to the world, and its index in the chunk's chain order.
+struct LookupQuart {
+    int qx, cqy, qz, p;
+};
+TB_HD TB_FI LookupQuart lookup_quart(int64_t zoom_seed, int x, int y, int z) {
+    const int best = zoom_best(x, y, z, [&](int qx, int qy, int qz) { return zoom_fiddles(zoom_seed, qx, qy, qz); });
     const int px = (x - 2) >> 2, py = (y - 2) >> 2, pz = (z - 2) >> 2;
-    const int qx = (best & 4) == 0 ? px : px + 1;
+    LookupQuart L;
+    L.qx = (best & 4) == 0 ? px : px + 1;
     const int qy = (best & 2) == 0 ? py : py + 1;
-    const int qz = (best & 1) == 0 ? pz : pz + 1;
+    L.qz = (best & 1) == 0 ? pz : pz + 1;
     constexpr int qmin = tbm::kMinY >> 2, qh = tbm::kHeight / 4;
-    const int cqy = (qy < qmin ? qmin : (qy > qmin + qh - 1 ? qmin + qh - 1 : qy)) - qmin;
-    const int X0 = (qx >> 2) * 4, Z0 = (qz >> 2) * 4;   // the chunk's first quart column
-    const int p = chain_pos(qx & 3, cqy, qz & 3);
-    QuartLeaf q = quart_leaf(M, S, qx, cqy, qz);
+    L.cqy = (qy < qmin ? qmin : (qy > qmin + qh - 1 ? qmin + qh - 1 : qy)) - qmin;
+    L.p = chain_pos(L.qx & 3, L.cqy, L.qz & 3);
+    return L;
+}
+TB_HD inline int biome_point(const DevModel& M, const DevSeed& S, int x, int y, int z) {
+    const LookupQuart L = lookup_quart(S.zoom_seed, x, y, z);
+    const int X0 = (L.qx >> 2) * 4, Z0 = (L.qz >> 2) * 4;   // the chunk's first quart column
+    const int p = L.p;
+    QuartLeaf q = quart_leaf(M, S, L.qx, L.cqy, L.qz);
     if (!q.tie || p == 0) return M.leaf_biome[q.leaf];
     int j = p - 1, a, b, c;
     for (;; --j) {

@@ -166,11 +166,110 @@ __global__ void __launch_bounds__(256) k_chain_warp(const __grid_constant__ Batc
     for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) chain_warp(B, w, lane);
 }
 
-// one lookup position per item, on its own: the zoomed quart and its chain result (biome_point)
-__global__ void k_biome_point(const __grid_constant__ DevModel M, const DevSeed* seeds, const int32_t* slot, const int32_t* xyz, int n,
-                              uint8_t* out) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        out[i] = static_cast<uint8_t>(biome_point(M, seeds[slot[i]], xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+// Biome lookups in two passes. Pass 1, one thread per position: the zoomed quart, its
+// climate, first minimal leaf and tie test; a quart whose minimum is unique (or the chunk's
+// first in chain order) has its result fixed, and the rest go to a list. Pass 2, one warp
+// per listed position: the chain is replayed from the nearest earlier quart whose result is
+// fixed, 32 quarts of the walk evaluated at a time (biome_point's result, without one thread
+// walking hundreds of quarts while the rest of its warp waits).
+struct TiedLookup {
+    int32_t i, qx, cqy, qz;
+};
+__global__ void k_biome_point1(const __grid_constant__ DevModel M, const DevSeed* seeds, const int32_t* slot, const int32_t* xyz, int n, uint8_t* out,
+                               TiedLookup* tied, int32_t* n_tied) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const DevSeed& S = seeds[slot[i]];
+        const LookupQuart L = lookup_quart(S.zoom_seed, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        const QuartLeaf q = quart_leaf(M, S, L.qx, L.cqy, L.qz);
+        if (!q.tie || L.p == 0) {
+            out[i] = static_cast<uint8_t>(M.leaf_biome[q.leaf]);
+        } else {
+            tied[atomicAdd(n_tied, 1)] = TiedLookup{i, L.qx, L.cqy, L.qz};
+        }
+    }
+}
+
+__device__ int tied_chain(const DevModel& M, const DevSeed& S, const TiedLookup& T, int lane) {
+    const unsigned full = 0xFFFFFFFFu;
+    const int X0 = (T.qx >> 2) * 4, Z0 = (T.qz >> 2) * 4;
+    const int p = chain_pos(T.qx & 3, T.cqy, T.qz & 3);
+    int a, b, c;
+    // walk back: the nearest j < p whose result is fixed (unique minimum, or j = 0)
+    int anchor = -1, r = -1;
+    for (int base = p - 1; anchor < 0; base -= 32) {
+        const int j = base - lane;
+        bool fixed = false;
+        int leaf = -1;
+        if (j >= 0) {
+            chain_quart(j, a, b, c);
+            const QuartLeaf q = quart_leaf(M, S, X0 + a, b, Z0 + c);
+            fixed = !q.tie || j == 0;
+            leaf = q.leaf;
+        }
+        const unsigned m = __ballot_sync(full, fixed);
+        if (m) {
+            const int k = __ffs(m) - 1;
+            anchor = base - k;
+            r = __shfl_sync(full, leaf, k);
+        }
+    }
+    // replay the chain from the anchor to p, 32 quarts at a time (chain_warp's resolution)
+    for (int k0 = anchor + 1; k0 <= p; k0 += 32) {
+        const int nvalid = min(32, p - k0 + 1);
+        const int k = k0 + lane;
+        QuartLeaf u;
+        u.leaf = -1;
+        u.m = 0;
+        if (lane < nvalid) {
+            chain_quart(k, a, b, c);
+            u = quart_leaf(M, S, X0 + a, b, Z0 + c);
+        }
+        const int ls = u.leaf;
+        int prev = __shfl_up_sync(full, ls, 1);
+        if (lane == 0) prev = r;
+        const bool keep = lane < nvalid && prev >= 0 && prev != ls && param_dist(M.tree[M.leaf_node[prev]], u.t) == u.m;
+        const unsigned keeps = __ballot_sync(full, keep);
+        int res = ls, v = r, pos = 0;
+        while (pos < nvalid) {
+            const int spec = pos == 0 ? r : __shfl_sync(full, ls, pos - 1);
+            if (v == spec) {
+                const unsigned mk = keeps & (full << pos);
+                if (!mk) {
+                    pos = nvalid;
+                    break;
+                }
+                const int jj = __ffs(mk) - 1;
+                if (jj >= nvalid) {
+                    pos = nvalid;
+                    break;
+                }
+                if (lane == jj) res = prev;
+                v = __shfl_sync(full, prev, jj);
+                pos = jj + 1;
+            } else {
+                const bool carry = lane >= pos && lane < nvalid && v != ls && param_dist(M.tree[M.leaf_node[v]], u.t) == u.m;
+                const unsigned run = __ballot_sync(full, carry) | ~(full << pos);
+                int jj = (~run) ? __ffs(~run) - 1 : 32;
+                if (jj > nvalid) jj = nvalid;
+                if (lane >= pos && lane < jj) res = v;
+                if (jj < nvalid) v = __shfl_sync(full, ls, jj);
+                pos = jj + 1;
+            }
+        }
+        r = __shfl_sync(full, res, nvalid - 1);
+    }
+    return r;
+}
+
+__global__ void k_biome_tied(const __grid_constant__ DevModel M, const DevSeed* seeds, const int32_t* slot, const TiedLookup* tied, const int32_t* n_tied,
+                             uint8_t* out) {
+    const int n = *n_tied, lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
+        const TiedLookup T = tied[w];
+        const int r = tied_chain(M, seeds[slot[T.i]], T, lane);
+        if (lane == 0) out[T.i] = static_cast<uint8_t>(M.leaf_biome[r]);
+    }
 }
 
 
@@ -801,7 +900,9 @@ struct Generator {
         const int cap = std::min(n, 1 << 20);
         if (cap <= 0) return;
         finish();
-        DevBuf d_xyz, d_slot, d_res;
+        DevBuf d_xyz, d_slot, d_res, d_tied, d_ntied;
+        d_tied.alloc(sizeof(TiedLookup) * static_cast<size_t>(cap));
+        d_ntied.alloc(sizeof(int32_t));
         d_xyz.alloc(sizeof(int32_t) * 3 * static_cast<size_t>(cap));
         d_slot.alloc(sizeof(int32_t) * static_cast<size_t>(cap));
         d_res.alloc(static_cast<size_t>(cap));
@@ -829,7 +930,11 @@ struct Generator {
             }
             ck(cudaMemcpyAsync(d_xyz.p, xyz + 3 * static_cast<size_t>(off), sizeof(int32_t) * 3 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s), "h2d");
             ck(cudaMemcpyAsync(d_slot.p, slot_of.data(), sizeof(int32_t) * static_cast<size_t>(m), cudaMemcpyHostToDevice, s), "h2d");
-            launch(k_biome_point, s, m, model, d_seeds.as<DevSeed>(), d_slot.as<int32_t>(), d_xyz.as<int32_t>(), m, d_res.as<uint8_t>());
+            ck(cudaMemsetAsync(d_ntied.p, 0, sizeof(int32_t), s), "memset");
+            launch(k_biome_point1, s, m, model, d_seeds.as<DevSeed>(), d_slot.as<int32_t>(), d_xyz.as<int32_t>(), m, d_res.as<uint8_t>(),
+                   d_tied.as<TiedLookup>(), d_ntied.as<int32_t>());
+            launch(k_biome_tied, s, 32L * m, model, d_seeds.as<DevSeed>(), d_slot.as<int32_t>(), d_tied.as<TiedLookup>(), d_ntied.as<int32_t>(),
+                   d_res.as<uint8_t>());
             ck(cudaGetLastError(), "kernel launch");
             ck(cudaMemcpyAsync(res + off, d_res.p, static_cast<size_t>(m), cudaMemcpyDeviceToHost, s), "d2h");
             ck(cudaStreamSynchronize(s), "sync");
