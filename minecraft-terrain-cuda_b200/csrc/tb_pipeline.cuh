@@ -119,6 +119,7 @@ struct Batch {
     uint32_t* zoom_tab;               // n * kZoomVerts packed fiddle draws per quart vertex
     uint32_t* walk;                   // n * kBlocksPerChunk packed column-walk state per block
     uint8_t* bbiome;                  // n * kBlocksPerChunk zoomed biome per block up to the column height
+    uint8_t* oremask;                 // n * kBlocksPerChunk ore-vein density tests passed, bit per vein
     struct ColumnRec* colrec;         // n * 256 per-column surface context
 };
 
@@ -129,6 +130,12 @@ struct ColumnRec {
     int32_t surface_biome, start_h;
 };
 constexpr uint32_t kNoWalk = 0xFFFFFFFFu;
+// Per block, bit k: whether ore vein k's density test passes (its density is not <= 0),
+// decided by the fill from the channel values it already holds, so that the rule tree
+// interpolates channels only inside veins.
+#ifndef TB_ORE_MASK
+#define TB_ORE_MASK (tbm::kNumOres <= 8)
+#endif
 #ifndef TB_FUSED_WALK
 #define TB_FUSED_WALK 1     // rule tree inside the column walk (1) or a per-block pass after it (0)
 #endif
@@ -824,7 +831,14 @@ TB_HD inline void body_fill(const Batch& B, int it) {
         const float d = tbgen::gen_final_density(S.nt, bx, y, bz, ch);
         int s = aq_substance(S.nt, A, skip, bx, y, bz, static_cast<double>(d));
         if (s < 0) s = tbm::kDefaultBlock;
-        out[((y - tbm::kMinY) * 16 + lz) * 16 + lx] = static_cast<uint16_t>(s);
+        const size_t bi = ((y - tbm::kMinY) * 16 + lz) * 16 + lx;
+        out[bi] = static_cast<uint16_t>(s);
+        if (TB_ORE_MASK) {
+            uint32_t om = 0;
+            for (int k = 0; k < tbm::kNumOres; ++k)
+                if (!(tbgen::gen_ore_density(k, S.nt, bx, y, bz, ch) <= 0.0f)) om |= 1u << k;
+            B.oremask[static_cast<size_t>(c) * kBlocksPerChunk + bi] = static_cast<uint8_t>(om);
+        }
         if (!(B.M.block_flags[s] & 1)) top = y;
         for (int q = 0; q < tbm::kNumChannels; ++q) ch[q] += ci.step[q];
     }
@@ -1252,6 +1266,7 @@ struct RuleCtx {
     // OreVeinRule: the density inline (its guards usually end it after a y test), the rest
     // out of line
     TB_HD TB_FI int ore_vein(int k, int ore, int raw, int filler, float chance) const {
+        if (TB_ORE_MASK && !((B->oremask[static_cast<size_t>(c) * kBlocksPerChunk + col->idx(y)] >> k) & 1)) return -1;
         const LazyChannels ch{B, c, col->lx, col->lz, y, false, {}};
         const float density = tbgen::gen_ore_density(k, col->S->nt, col->bx, y, col->bz, ch);
         if (density <= 0.0f) return -1;
