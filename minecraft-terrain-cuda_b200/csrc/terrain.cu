@@ -471,7 +471,14 @@ struct Work {
 
 // ---- the generator ----------------------------------------------------------------------------------
 struct Generator {
-    static constexpr int kTailMin = 512;   // smallest batch the tail split of generate() makes
+#ifndef TB_TAIL_MIN
+#define TB_TAIL_MIN 512
+#endif
+    static constexpr int kTailMin = TB_TAIL_MIN;   // smallest batch the tail split of generate() makes (0: no split)
+#ifndef TB_ORDERED_BATCH
+#define TB_ORDERED_BATCH 2048
+#endif
+    static constexpr int kOrderedBatch = TB_ORDERED_BATCH;   // batches this large run one after another
     int device = 0;
     int max_batch = 2048;
     cudaStream_t stream = nullptr;      // compute stream (the caller's, when set)
@@ -756,6 +763,10 @@ struct Generator {
         Work& W = work[o.lane];
         cudaStream_t s = o.lane ? lane_stream : stream;
         if (o.busy) ck(cudaStreamWaitEvent(s, o.drained, 0), "wait");   // the slot's previous outputs are copied out
+        // A batch that fills the GPU alone runs after the previous one rather than beside it,
+        // so each finishes (and its copy starts) as early as possible; smaller ones overlap.
+        OutSlot& other = out[&o == &out[0] ? 1 : 0];
+        if (lanes > 1 && n >= kOrderedBatch && other.lane != o.lane && other.busy) ck(cudaStreamWaitEvent(s, other.computed, 0), "wait");
         const int32_t* h = o.coords.as<int32_t>();
         ck(cudaMemcpyAsync(W.d_cx.p, h, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
         ck(cudaMemcpyAsync(W.d_cz.p, h + max_batch, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
@@ -860,7 +871,8 @@ struct Generator {
             // The copy of the last batch is the one no compute hides: within the last two
             // batches' worth, halve the batches (down to kTailMin chunks) so that it is short.
             const int rem = count - off;
-            const int n = rem > 2 * max_batch ? max_batch : std::min(max_batch, std::max((rem + 1) / 2, std::min(rem, kTailMin)));
+            const int n = (kTailMin == 0 || rem > 2 * max_batch) ? std::min(max_batch, rem)
+                                                                   : std::min(max_batch, std::max((rem + 1) / 2, std::min(rem, kTailMin)));
             for (int i = 0; i < n; ++i) {
                 cx[i] = chunks[off + i].x;
                 cz[i] = chunks[off + i].z;

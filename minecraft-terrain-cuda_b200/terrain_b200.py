@@ -161,17 +161,21 @@ class TerrainGenerator:
         blocks = blocks_out if blocks_out is not None else np.empty((n, self.height, 16, 16), np.uint16)
         biomes = biomes_out if biomes_out is not None else np.empty((n, self.qper), np.uint8)
         aq = np.empty((n, self.height, 16, 16), np.uint16) if aquifer else None
-        t = TgTiming()
-        self._check(self.L.tg_generate(self.h, a.ctypes.data_as(ctypes.POINTER(TgChunk)), n, _ptr(blocks), _ptr(biomes), _ptr(aq), ctypes.byref(t)))
+        # stage timing records events between the kernels and waits for each batch, so it is
+        # requested only when asked for; without it batches run as CUDA graphs and overlap
+        t = TgTiming() if timing else None
+        self._check(self.L.tg_generate(self.h, a.ctypes.data_as(ctypes.POINTER(TgChunk)), n, _ptr(blocks), _ptr(biomes), _ptr(aq),
+                                       ctypes.byref(t) if timing else None))
         out = (blocks, biomes) + ((aq,) if aquifer else ())
         return out + (t.as_dict(),) if timing else out
 
-    def generate_device(self, chunks_ptr, count, blocks_ptr, biomes_ptr=None):
-        """Device pointers (ints); returns the stage timing dict."""
-        t = TgTiming()
+    def generate_device(self, chunks_ptr, count, blocks_ptr, biomes_ptr=None, timing=True):
+        """Device pointers (ints); returns the stage timing dict (None with timing=False, which
+        leaves out the stage events)."""
+        t = TgTiming() if timing else None
         self._check(self.L.tg_generate_device(self.h, ctypes.c_void_p(chunks_ptr), count, ctypes.c_void_p(blocks_ptr),
-                                              ctypes.c_void_p(biomes_ptr) if biomes_ptr else None, ctypes.byref(t)))
-        return t.as_dict()
+                                              ctypes.c_void_p(biomes_ptr) if biomes_ptr else None, ctypes.byref(t) if timing else None))
+        return t.as_dict() if timing else None
 
     def generate_batch(self, requests, timing=False):
         """requests: list of (seed, chunks). Returns list of (blocks, biomes)."""
@@ -188,8 +192,8 @@ class TerrainGenerator:
             reqs[i].count = n
             reqs[i].blocks_out = b.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))
             reqs[i].biomes_out = bi.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
-        t = TgTiming()
-        self._check(self.L.tg_generate_batch(self.h, reqs, len(requests), ctypes.byref(t)))
+        t = TgTiming() if timing else None
+        self._check(self.L.tg_generate_batch(self.h, reqs, len(requests), ctypes.byref(t) if timing else None))
         return (outs, t.as_dict()) if timing else outs
 
     def biome_lookup(self, seeds, xyz):

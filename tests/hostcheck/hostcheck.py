@@ -29,6 +29,7 @@ def lib():
         L.hc_corners.argtypes = [ctypes.c_int64, vp, ctypes.c_int32, vp]
         L.hc_seed_scalars.argtypes = [ctypes.c_int64, vp, vp]
         L.hc_noise_layers.argtypes = [ctypes.c_int64, ctypes.c_int32, vp, vp, vp, vp]
+        L.hc_biome_point.argtypes = [ctypes.c_int64, vp, ctypes.c_int32, vp]
         _L = L
     return _L
 
@@ -46,6 +47,14 @@ def generate(seed, chunks, aquifer=False):
     aq = np.empty((n, 384, 16, 16), np.uint16) if aquifer else None
     lib().hc_generate(int(seed), _p(cx), _p(cz), n, _p(b), _p(q), _p(aq) if aquifer else None)
     return (b, q, aq) if aquifer else (b, q)
+
+
+def biome_point(seed, xyz):
+    """Biome lookups through the single-position path (zoom corner, quart leaf, tie replay)."""
+    xyz = np.ascontiguousarray(np.asarray(xyz, np.int32).reshape(-1, 3))
+    out = np.empty(xyz.shape[0], np.uint8)
+    assert lib().hc_biome_point(int(seed), _p(xyz), xyz.shape[0], _p(out)) == 0
+    return out
 
 
 def point(seed, root, xyz):

@@ -76,3 +76,16 @@ def test_whole_chunks(ref_model, seed):
         assert (q[i] == rq[i]).all(), c
         assert (aq[i] == raq[i]).all(), c
         assert (b[i] == rb[i]).all(), c
+
+
+@pytest.mark.parametrize('seed', [123456789, -4172144997902289642])
+def test_biome_point_lookups(ref_model, seed):
+    """The single-position lookup path (zoom corner, the quart's minimum and tie test, the
+    chunk chain replayed from the nearest earlier fixed quart) against the reference's
+    zoomed_biome over whole-chunk quart biomes: scattered positions up to the world border,
+    dense ones (tied quarts replay the chain), and y outside the world (clamped rows)."""
+    rng = np.random.default_rng(seed & 0xFFFF)
+    far = np.stack([rng.integers(-1874999, 1875000, 300), rng.integers(-64, 320, 300), rng.integers(-1874999, 1875000, 300)], 1)
+    near = np.stack([rng.integers(-40, 40, 300), rng.integers(-90, 345, 300), rng.integers(-40, 40, 300)], 1)
+    xyz = np.ascontiguousarray(np.concatenate([far, near]).astype(np.int32))
+    assert (hostcheck.biome_point(seed, xyz) == ref_model.seed(seed).biome_lookup(xyz)).all()
