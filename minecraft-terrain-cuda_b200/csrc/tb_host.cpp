@@ -227,6 +227,7 @@ void make_octave(Xoro& r, double smear, SeedHost& s) {
     }
     s.off.push_back(o);
     s.perm.insert(s.perm.end(), p, p + 256);
+    for (int i = 0; i < 256; ++i) s.perm2.push_back(static_cast<uint16_t>(p[i] | (p[(i + 1) & 255] << 8)));
 }
 
 // NormalNoise(parameters).create(random): octave list, normalisation, two positional forks.

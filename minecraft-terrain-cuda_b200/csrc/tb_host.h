@@ -64,6 +64,7 @@ struct SeedHost {
     int64_t seed = 0;
     std::vector<OctaveOff> off;
     std::vector<uint8_t> perm;
+    std::vector<uint16_t> perm2;   // perm[i] | perm[(i + 1) & 255] << 8, per octave
     std::vector<Layer> layers;
     Positional random{}, aquifer{}, ore{};
     std::vector<Positional> gradient;

@@ -410,7 +410,7 @@ struct SeedSlot {
     int64_t seed = 0;
     bool valid = false;
     uint64_t last_use = 0;
-    DevBuf off, perm, layers;
+    DevBuf off, perm, layers, perm2;
 };
 
 // one output buffer set (the pipeline's outputs are double-buffered)
@@ -625,9 +625,10 @@ struct Generator {
         SeedSlot& sl = slots[s];
         upload(sl.off, h.off);
         upload(sl.perm, h.perm);
+        upload(sl.perm2, h.perm2);
         upload(sl.layers, h.layers);
         DevSeed d{};
-        d.nt = NoiseTables{sl.off.as<OctaveOff>(), sl.perm.as<uint8_t>(), sl.layers.as<Layer>()};
+        d.nt = NoiseTables{sl.off.as<OctaveOff>(), sl.perm.as<uint8_t>(), sl.layers.as<Layer>(), sl.perm2.as<uint16_t>()};
         d.random = h.random;
         d.aquifer = h.aquifer;
         d.ore = h.ore;

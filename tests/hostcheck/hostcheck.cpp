@@ -50,7 +50,7 @@ struct HostRun {
         M.info = m.info;
         M.f2 = m.f2;
         M.g2 = m.g2;
-        D.nt = NoiseTables{s.off.data(), s.perm.data(), s.layers.data()};
+        D.nt = NoiseTables{s.off.data(), s.perm.data(), s.layers.data(), s.perm2.data()};
         D.random = s.random;
         D.aquifer = s.aquifer;
         D.ore = s.ore;
