@@ -67,12 +67,25 @@ TB_HD TB_FI int32_t d2i(double v) {
 
 // Mth.floor(double): (int) Math.floor(v). The device form is one cvt.rmi.s32.f64,
 // which saturates like the Java cast; NaN is decided on the bits.
+#ifndef TB_FLOOR_FINITE
+#define TB_FLOOR_FINITE 1
+#endif
 TB_HD TB_FI int32_t jfloor(double v) {
 #if defined(__CUDA_ARCH__)
     if ((dbits(v) << 1) > 0xFFE0000000000000ull) return 0;
     return __double2int_rd(v);
 #else
     return d2i(std::floor(v));
+#endif
+}
+
+// Mth.floor for a value known to be finite (an integer block coordinate times a finite
+// scale plus a finite offset): the NaN test of jfloor is not needed.
+TB_HD TB_FI int32_t jfloor_finite(double v) {
+#if defined(__CUDA_ARCH__) && TB_FLOOR_FINITE
+    return __double2int_rd(v);
+#else
+    return jfloor(v);
 #endif
 }
 

@@ -171,7 +171,7 @@ struct AxisSetup {
 };
 TB_HD TB_FI AxisSetup axis_setup(int32_t b, double scale, double off) {
     const double v = nwrap(static_cast<double>(b) * scale) + off;
-    const int32_t f = jfloor(v);
+    const int32_t f = jfloor_finite(v);
     const float r = static_cast<float>(v - static_cast<double>(f));
     return {f, r, smoothf(r)};
 }
@@ -199,7 +199,7 @@ TB_HD TB_FI float octave_volume_smeared(const NoiseTables& T, int32_t oct, int32
     const AxisSetup X = axis_setup(bx, xs, o.ox);
     const double oy = static_cast<double>(by) * ys;
     const double y = nwrap(oy) + o.oy;
-    const int32_t fy = jfloor(y);
+    const int32_t fy = jfloor_finite(y);
     const double rel = y - static_cast<double>(fy);
     const float ay = smoothf(static_cast<float>(rel));
     const CellHash c = octave_hash(T, oct, X.f, fy, Z.f);
