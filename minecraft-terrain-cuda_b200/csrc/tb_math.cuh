@@ -110,6 +110,7 @@ TB_HD TB_FI float fabs_j(float v) { return bitsf(fbits(v) & 0x7FFFFFFFu); }
 
 // wrapping int32 arithmetic (Java int overflow semantics)
 TB_HD TB_FI int32_t iadd(int32_t a, int32_t b) { return static_cast<int32_t>(static_cast<uint32_t>(a) + static_cast<uint32_t>(b)); }
+TB_HD TB_FI int32_t isub(int32_t a, int32_t b) { return static_cast<int32_t>(static_cast<uint32_t>(a) - static_cast<uint32_t>(b)); }
 TB_HD TB_FI int32_t imul(int32_t a, int32_t b) { return static_cast<int32_t>(static_cast<uint32_t>(a) * static_cast<uint32_t>(b)); }
 
 // Math.floorDiv / floorMod (int)
@@ -118,6 +119,8 @@ TB_HD TB_FI int32_t fdiv(int32_t a, int32_t b) {
     return (q * b != a && ((a ^ b) < 0)) ? q - 1 : q;
 }
 TB_HD TB_FI int32_t fmod_i(int32_t a, int32_t b) { return a - fdiv(a, b) * b; }
+TB_HD TB_FI int32_t imin(int32_t a, int32_t b) { return a < b ? a : b; }
+TB_HD TB_FI int32_t imax(int32_t a, int32_t b) { return a < b ? b : a; }
 
 // Math.min / Math.max (float and double): NaN propagates from either side, and
 // -0.0 orders below +0.0.

@@ -28,6 +28,9 @@ constexpr int kMaxY = tbm::kMinY + tbm::kHeight - 1;
 constexpr int kGridX = 27, kGridZ = 19, kGrid = kGridX * kGridZ;   // surface-level quarts per chunk
 constexpr int kAqX = 3, kAqY = 35, kAqZ = 3, kAqCells = kAqX * kAqY * kAqZ;
 constexpr int kAqMinGridY = -7;
+// Nearest-cell queries per chunk: the lowest of the three candidate layers (33 for the world
+// height) x the two x and two z candidate columns a block of the chunk can start from.
+constexpr int kAqQueryLayers = kAqY - 2, kAqQueries = kAqQueryLayers * 4;
 constexpr int kWayBelowMinY = -2032 * 16;   // DimensionType.WAY_BELOW_MIN_Y
 constexpr int kMaxGradientRandoms = 8;
 constexpr int kSearchStack = 16;
@@ -78,6 +81,21 @@ struct HashTab {
 };
 constexpr unsigned long long kEmpty = ~0ull;
 
+// One aquifer grid cell (NoiseBasedAquifer's aquiferLocationCache and aquiferCache entries
+// together): its jittered location and its fluid status packed as level * 4 + fluid block,
+// 16 bytes so that the nearest-cell scan reads a cell with one vector load.
+struct alignas(16) AqCell {
+    int32_t x, y, z, st;
+};
+
+// What the 12 candidate cells of one nearest-cell query decide without their distances:
+// the status all of them share (kAqMixed when they differ) and the height from which every
+// block is air (the highest level + 5).
+struct alignas(8) AqQuery {
+    int32_t uni, air_from;
+};
+constexpr int32_t kAqMixed = INT32_MIN;   // no status packs to it (fluid blocks are 2 or 3)
+
 struct Batch {
     DevModel M;
     const DevSeed* seeds;
@@ -106,8 +124,8 @@ struct Batch {
     int32_t* g513;                    // n * kGrid indices
     float* sfts;                      // sg_cap: find_top_surface value per unique quart
     // aquifer
-    int32_t* aq_loc;                  // n * kAqCells * 3 (x, y, z)
-    int32_t* aq_status;               // n * kAqCells * 2 (level, fluid state)
+    AqCell* aq_cell;                  // n * kAqCells, (iy * kAqZ + iz) * kAqX + ix
+    AqQuery* aq_query;                // n * kAqQueries, (layer * 2 + z column) * 2 + x column
     int32_t* aq_skip;                 // n
     // outputs and heights
     uint16_t* blocks;                 // n * kBlocksPerChunk
@@ -567,6 +585,11 @@ struct Fluid {
     int32_t level, type;
     TB_HD TB_FI int at(int y) const { return y < level ? type : tbm::kAir; }
 };
+// Aquifer status packing: the fluid block is water or lava (below 4), the level at least
+// kWayBelowMinY, so level * 4 + type fits and the arithmetic shift gives the level back.
+static_assert(tbm::kWater >= 0 && tbm::kWater < 4 && tbm::kLava >= 0 && tbm::kLava < 4 && tbm::kDefaultFluid < 4, "fluid packing");
+TB_HD TB_FI int32_t fluid_pack(Fluid f) { return f.level * 4 + f.type; }
+TB_HD TB_FI Fluid fluid_unpack(int32_t st) { return Fluid{st >> 2, st & 3}; }
 TB_HD TB_FI Fluid global_fluid(int y) {
     constexpr int lava_level = tbm::kTmSeaLevel < -54 ? tbm::kTmSeaLevel : -54;
     return y < lava_level ? Fluid{-54, tbm::kLava} : Fluid{tbm::kTmSeaLevel, tbm::kDefaultFluid};
@@ -582,10 +605,16 @@ TB_HD TB_FI void blockpos_wrap(int32_t& x, int32_t& y, int32_t& z) {
     z = static_cast<int32_t>(static_cast<int64_t>(v << 26) >> 38);
 }
 
-// surface level at block (sx, sz) as seen by chunk c
-TB_HD TB_FI int surface_at(const Batch& B, int c, int sx, int sz) {
+// Surface level at block (sx, sz) as seen by chunk c (NoiseBasedAquifer's surface-level
+// cache, cpu/src/terrain.cpp:324-331): the chunk's grid of surface quarts, which holds every
+// unwrapped position the aquifer cells ask for. Cell locations that the BlockPos packing
+// wrapped (chunks from |c| = 2^21 - 1 on) lie 2^26 blocks away, outside the cached window,
+// so the point path evaluates them.
+TB_HD TB_FI int surface_at(const Batch& B, const NoiseTables& T, int c, int sx, int sz) {
     const int gx = (sx >> 2) - (B.cx[c] * 4 - 16), gz = (sz >> 2) - (B.cz[c] * 4 - 8);
-    return jfloor(static_cast<double>(B.sfts[B.g513[static_cast<size_t>(c) * kGrid + gz * kGridX + gx]]));
+    if (gx >= 0 && gx < kGridX && gz >= 0 && gz < kGridZ)
+        return jfloor(static_cast<double>(B.sfts[B.g513[static_cast<size_t>(c) * kGrid + gz * kGridX + gx]]));
+    return jfloor(static_cast<double>(tbgen::gen_fts_pt(T, (sx >> 2) * 4, (sz >> 2) * 4)));
 }
 
 TB_HD inline void body_aquifer_cell(const Batch& B, int it) {
@@ -598,10 +627,6 @@ TB_HD inline void body_aquifer_cell(const Batch& B, int it) {
     int32_t y = gy * 12 + r.next_int(9);
     int32_t z = gz * 16 + r.next_int(10);
     blockpos_wrap(x, y, z);
-    int32_t* loc = B.aq_loc + static_cast<size_t>(it) * 3;
-    loc[0] = x;
-    loc[1] = y;
-    loc[2] = z;
     // NoiseBasedAquifer.computeFluid
     const Fluid glob = global_fluid(y);
     Fluid res{0, 0};
@@ -612,7 +637,7 @@ TB_HD inline void body_aquifer_cell(const Batch& B, int it) {
     const signed char off[13][2] = {{0, 0}, {-2, -1}, {-1, -1}, {0, -1}, {1, -1}, {-3, 0}, {-2, 0}, {-1, 0}, {1, 0}, {-2, 1}, {-1, 1}, {0, 1}, {1, 1}};
     for (int k = 0; k < 13 && !done; ++k) {
         const int sx = x + (off[k][0] << 4), sz = z + (off[k][1] << 4);
-        const int level = surface_at(B, c, sx, sz);
+        const int level = surface_at(B, S.nt, c, sx, sz);
         const int adjusted = level + 8;
         const bool start = k == 0;
         if (start && bottom > adjusted) {
@@ -672,9 +697,38 @@ TB_HD inline void body_aquifer_cell(const Batch& B, int it) {
         }
         res = Fluid{level, type};
     }
-    int32_t* st = B.aq_status + static_cast<size_t>(it) * 2;
-    st[0] = res.level;
-    st[1] = res.type;
+    B.aq_cell[it] = AqCell{x, y, z, fluid_pack(res)};
+}
+
+// The 12 cells of one query: x columns xa..xa+1 (outer), layers (middle), z columns (inner).
+TB_HD TB_FI int aq_query_cell(int base, int j) {
+    const int ox = j >= 6 ? 1 : 0, r = j - 6 * ox;
+    return base + ((r >> 1) * kAqZ + (r & 1)) * kAqX + ox;
+}
+
+// Shortcuts of NoiseBasedAquifer.computeSubstance (cpu/src/terrain.cpp:215-275) that hold for
+// every block of a query, whatever its distances to the cells:
+//  - all 12 statuses equal: each pressure is 0 (equal levels), so no barrier test can make
+//    the block solid and the result is that status's fluid at y;
+//  - y >= every level + 5: for any two cells, above = y + 0.5 - average exceeds diff / 2 + 5,
+//    so the gradient is at most -5.5 / 2.5 < -2, the barrier noise is not sampled, every
+//    pressure is negative and no test makes the block solid; the nearest cell's fluid at y
+//    is air.
+TB_HD inline void body_aquifer_query(const Batch& B, int it) {
+    const int c = it / kAqQueries, q = it % kAqQueries;
+    const int layer = q >> 2, zc = (q >> 1) & 1, xc = q & 1;
+    const AqCell* cell = B.aq_cell + static_cast<size_t>(c) * kAqCells;
+    const int base = (layer * kAqZ + zc) * kAqX + xc;
+    const int32_t st0 = cell[base].st;
+    bool uni = true;
+    int top = INT_MIN;
+    for (int j = 0; j < 12; ++j) {
+        const int32_t st = cell[aq_query_cell(base, j)].st;
+        uni = uni && st == st0;
+        const int level = fluid_unpack(st).level;
+        top = level > top ? level : top;
+    }
+    B.aq_query[it] = AqQuery{uni ? st0 : kAqMixed, top + 5};
 }
 
 // per-chunk skip height from the volume-semantics window maximum
@@ -691,13 +745,19 @@ TB_HD inline void body_aquifer_skip(const Batch& B, int c) {
 }
 
 // ---- fill: channels, final density, aquifer substance --------------------------------------------
-TB_HD TB_FI double aq_similarity(int a, int b) { return 1.0 - static_cast<double>(b - a) / 25.0; }
+// b - a wraps like the reference's int subtraction (distances of wrapped locations overflow)
+TB_HD TB_FI double aq_similarity(int a, int b) { return 1.0 - static_cast<double>(isub(b, a)) / 25.0; }
 
 struct AqBlock {
-    const int32_t* loc;
-    const int32_t* st;
+    const AqCell* cell;
+    const AqQuery* query;
     int cx, cz;
+    bool keyed;   // aq_keyed(cx, cz)
 };
+// Chunks this far from the BlockPos wrap have unwrapped cell locations and squared
+// distances below 2^13, so distance * 16 + scan position fits an int.
+constexpr int kAqKeyedMax = (1 << 21) - 4;
+TB_HD TB_FI bool aq_keyed(int cx, int cz) { return cx >= -kAqKeyedMax && cx <= kAqKeyedMax && cz >= -kAqKeyedMax && cz <= kAqKeyedMax; }
 
 TB_HD inline double aq_pressure(const NoiseTables& T, int x, int y, int z, double& barrier, bool& barrier_set, Fluid a, Fluid b) {
     const int t1 = a.at(y), t2 = b.at(y);
@@ -736,51 +796,73 @@ TB_HD inline int aq_substance(const NoiseTables& T, const AqBlock& A, int skip, 
     if (y > skip) return glob.at(y);
     if (glob.at(y) == tbm::kLava) return tbm::kLava;
     const int xa = (x - 5) >> 4, ya = fdiv(y + 1, 12), za = (z - 5) >> 4;
-    int d1 = INT_MAX, d2 = INT_MAX, d3 = INT_MAX, d4 = INT_MAX;
-    int i1 = 0, i2 = 0, i3 = 0, i4 = 0;
-    for (int ox = 0; ox <= 1; ++ox)
-        for (int oy = -1; oy <= 1; ++oy)
-            for (int oz = 0; oz <= 1; ++oz) {
-                const int ix = xa + ox - (A.cx - 1), iy = ya + oy - kAqMinGridY, iz = za + oz - (A.cz - 1);
-                const int idx = (iy * kAqZ + iz) * kAqX + ix;
-                const int32_t* l = A.loc + idx * 3;
-                const int dx = l[0] - x, dy = l[1] - y, dz = l[2] - z;
-                const int nd = dx * dx + dy * dy + dz * dz;
-                if (d1 >= nd) {
-                    i4 = i3; i3 = i2; i2 = i1; i1 = idx;
-                    d4 = d3; d3 = d2; d2 = d1; d1 = nd;
-                } else if (d2 >= nd) {
-                    i4 = i3; i3 = i2; i2 = idx;
-                    d4 = d3; d3 = d2; d2 = nd;
-                } else if (d3 >= nd) {
-                    i4 = i3; i3 = idx;
-                    d4 = d3; d3 = nd;
-                } else if (d4 >= nd) {
-                    i4 = idx;
-                    d4 = nd;
+    const int layer = ya - 1 - kAqMinGridY, zc = za - (A.cz - 1), xc = xa - (A.cx - 1);
+    const AqQuery Q = A.query[(layer * 2 + zc) * 2 + xc];
+    if (Q.uni != kAqMixed) return fluid_unpack(Q.uni).at(y);
+    if (y >= Q.air_from) return tbm::kAir;
+    // the three nearest of the 12 candidate cells, later ones first on equal distance
+    int d1 = INT_MAX, d2 = INT_MAX, d3 = INT_MAX, i1 = 0, i2 = 0, i3 = 0;
+    const int base = (layer * kAqZ + zc) * kAqX + xc;
+    if (A.keyed) {
+        // Each candidate as one key, distance * 16 + (15 - scan position): ascending keys are
+        // ascending distances with later cells first, so the insertion chain's order is the
+        // order of the three smallest keys, kept by a min/max network.
+        int k1 = INT_MAX, k2 = INT_MAX, k3 = INT_MAX;
+        int j = 15;
+        for (int ox = 0; ox <= 1; ++ox)
+            for (int oy = 0; oy <= 2; ++oy)
+                for (int oz = 0; oz <= 1; ++oz, --j) {
+                    const AqCell l = A.cell[base + (oy * kAqZ + oz) * kAqX + ox];
+                    const int dx = l.x - x, dy = l.y - y, dz = l.z - z;
+                    const int key = (dx * dx + dy * dy + dz * dz) * 16 + j;
+                    k3 = imin(k3, imax(k2, key));
+                    k2 = imin(k2, imax(k1, key));
+                    k1 = imin(k1, key);
                 }
-            }
-    (void)i4;
-    auto status = [&](int idx) { return Fluid{A.st[idx * 2], A.st[idx * 2 + 1]}; };
-    const Fluid s1 = status(i1);
-    const double sim12 = aq_similarity(d1, d2);
+        auto cell_of = [&](int k) { return aq_query_cell(base, 15 - (k & 15)); };
+        d1 = k1 >> 4; d2 = k2 >> 4; d3 = k3 >> 4;
+        i1 = cell_of(k1); i2 = cell_of(k2); i3 = cell_of(k3);
+    } else {
+        for (int ox = 0; ox <= 1; ++ox)
+            for (int oy = 0; oy <= 2; ++oy)
+                for (int oz = 0; oz <= 1; ++oz) {
+                    const int idx = base + (oy * kAqZ + oz) * kAqX + ox;
+                    const AqCell l = A.cell[idx];
+                    const int dx = l.x - x, dy = l.y - y, dz = l.z - z;
+                    const int nd = iadd(iadd(imul(dx, dx), imul(dy, dy)), imul(dz, dz));
+                    if (d1 >= nd) {
+                        i3 = i2; i2 = i1; i1 = idx;
+                        d3 = d2; d2 = d1; d1 = nd;
+                    } else if (d2 >= nd) {
+                        i3 = i2; i2 = idx;
+                        d3 = d2; d2 = nd;
+                    } else if (d3 >= nd) {
+                        i3 = idx;
+                        d3 = nd;
+                    }
+                }
+    }
+    const int32_t t1 = A.cell[i1].st;
+    const Fluid s1 = fluid_unpack(t1);
     const int fluid = s1.at(y);
-    if (sim12 <= 0.0) return fluid;
+    // similarity(a, b) = 1 - (b - a) / 25: the quotient of an integer below 25 by 25 rounds
+    // below 1 (and a wrapped negative difference gives a similarity above 1), so the
+    // similarity is <= 0 exactly when the wrapped b - a is >= 25
+    if (isub(d2, d1) >= 25) return fluid;
     if (fluid == tbm::kWater && global_fluid(y - 1).at(y - 1) == tbm::kLava) return fluid;
+    const double sim12 = aq_similarity(d1, d2);
     double barrier = 0.0;
     bool barrier_set = false;
-    const Fluid s2 = status(i2);
+    const Fluid s2 = fluid_unpack(A.cell[i2].st);
     const double b12 = sim12 * aq_pressure(T, x, y, z, barrier, barrier_set, s1, s2);
     if (density + b12 > 0.0) return -1;
-    const Fluid s3 = status(i3);
-    const double sim13 = aq_similarity(d1, d3);
-    if (sim13 > 0.0) {
-        const double b13 = sim12 * sim13 * aq_pressure(T, x, y, z, barrier, barrier_set, s1, s3);
+    const Fluid s3 = fluid_unpack(A.cell[i3].st);
+    if (isub(d3, d1) < 25) {
+        const double b13 = sim12 * aq_similarity(d1, d3) * aq_pressure(T, x, y, z, barrier, barrier_set, s1, s3);
         if (density + b13 > 0.0) return -1;
     }
-    const double sim23 = aq_similarity(d2, d3);
-    if (sim23 > 0.0) {
-        const double b23 = sim12 * sim23 * aq_pressure(T, x, y, z, barrier, barrier_set, s2, s3);
+    if (isub(d3, d2) < 25) {
+        const double b23 = sim12 * aq_similarity(d2, d3) * aq_pressure(T, x, y, z, barrier, barrier_set, s2, s3);
         if (density + b23 > 0.0) return -1;
     }
     return fluid;
@@ -822,7 +904,8 @@ TB_HD inline void body_fill(const Batch& B, int it) {
     cell_interp(B, c, lx, lz, cell_y, ci);
     float ch[tbm::kNumChannels];
     for (int k = 0; k < tbm::kNumChannels; ++k) ch[k] = ci.a0[k];
-    const AqBlock A{B.aq_loc + static_cast<size_t>(c) * kAqCells * 3, B.aq_status + static_cast<size_t>(c) * kAqCells * 2, B.cx[c], B.cz[c]};
+    const AqBlock A{B.aq_cell + static_cast<size_t>(c) * kAqCells, B.aq_query + static_cast<size_t>(c) * kAqQueries, B.cx[c], B.cz[c],
+                    aq_keyed(B.cx[c], B.cz[c])};
     const int skip = B.aq_skip[c];
     uint16_t* out = B.blocks + static_cast<size_t>(c) * kBlocksPerChunk;
     int top = INT_MIN;

@@ -429,8 +429,8 @@ struct OutSlot {
 // per-block biomes). A generator holds one set per lane; two lanes let the batches of the
 // two output slots run concurrently on two streams.
 struct Work {
-    DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_loc, d_aq_status,
-        d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_walk, d_bbiome, d_oremask, d_colrec;
+    DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_cell,
+        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_walk, d_bbiome, d_oremask, d_colrec;
     TableBufs tb_b, tb_c, tb_s;
     void alloc(int n) {
         const size_t N = static_cast<size_t>(n);
@@ -453,8 +453,8 @@ struct Work {
         d_corners.alloc(sizeof(float) * cc * kRows * tbm::kNumChannels);
         d_g513.alloc(4 * sg);
         d_sfts.alloc(sizeof(float) * sg);
-        d_aq_loc.alloc(sizeof(int32_t) * N * kAqCells * 3);
-        d_aq_status.alloc(sizeof(int32_t) * N * kAqCells * 2);
+        d_aq_cell.alloc(sizeof(AqCell) * N * kAqCells);
+        d_aq_query.alloc(sizeof(AqQuery) * N * kAqQueries);
         d_aq_skip.alloc(4 * N);
         d_h0.alloc(4 * 256 * N);
         d_h1.alloc(4 * 256 * N);
@@ -667,8 +667,8 @@ struct Generator {
         B.sg_cap = kGrid * max_batch;
         B.g513 = W.d_g513.as<int32_t>();
         B.sfts = W.d_sfts.as<float>();
-        B.aq_loc = W.d_aq_loc.as<int32_t>();
-        B.aq_status = W.d_aq_status.as<int32_t>();
+        B.aq_cell = W.d_aq_cell.as<AqCell>();
+        B.aq_query = W.d_aq_query.as<AqQuery>();
         B.aq_skip = W.d_aq_skip.as<int32_t>();
         B.blocks = o ? o->blocks.as<uint16_t>() : nullptr;
         B.h0 = W.d_h0.as<int32_t>();
@@ -720,6 +720,7 @@ struct Generator {
         launch(k_items<body_sg_resolve, kGrid>, s, kGrid * nmax, B);
         launch(k_dyn<body_surface_level, 1>, s, 2 * nmax * 100, B, cnt_s);
         launch(k_items<body_aquifer_cell, kAqCells>, s, kAqCells * nmax, B);
+        launch(k_items<body_aquifer_query, kAqQueries>, s, kAqQueries * nmax, B);
         launch(k_items<body_aquifer_skip, 1>, s, nmax, B);
         mark(3);
         launch(k_init_heights, s, 256 * nmax, B);

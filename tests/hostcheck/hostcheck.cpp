@@ -95,7 +95,9 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     hc.init(25 * static_cast<size_t>(n));
     hs.init(static_cast<size_t>(kGrid) * n);
     const size_t N = n, nb = 9 * N, cc = 25 * N, sg = kGrid * N;
-    std::vector<int32_t> nb9(9 * N), c25(25 * N), g513(sg), aq_loc(N * kAqCells * 3), aq_status(N * kAqCells * 2), aq_skip(N);
+    std::vector<int32_t> nb9(9 * N), c25(25 * N), g513(sg), aq_skip(N);
+    std::vector<AqCell> aq_cell(N * kAqCells);
+    std::vector<AqQuery> aq_query(N * kAqQueries);
     std::vector<float> bcol(nb * 16 * tbm::kClimateCols), ccol(cc * tbm::kCornerCols), corners(cc * kRows * tbm::kNumChannels), sfts(sg);
     std::vector<long long> tgt(nb * kQuartsPerChunk * 6), mdist(nb * kQuartsPerChunk);
     std::vector<int32_t> lstar(nb * kQuartsPerChunk), h0(256 * N, tbm::kMinY), h1(256 * N), h2(256 * N);
@@ -128,8 +130,8 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     B.sg_cap = static_cast<int32_t>(sg);
     B.g513 = g513.data();
     B.sfts = sfts.data();
-    B.aq_loc = aq_loc.data();
-    B.aq_status = aq_status.data();
+    B.aq_cell = aq_cell.data();
+    B.aq_query = aq_query.data();
     B.aq_skip = aq_skip.data();
     B.blocks = bl.data();
     B.h0 = h0.data();
@@ -155,6 +157,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     each(kGrid * n, [&](int i) { body_sg_resolve(B, i); });
     each(hs.count, [&](int i) { body_surface_level(B, i); });
     each(kAqCells * n, [&](int i) { body_aquifer_cell(B, i); });
+    each(kAqQueries * n, [&](int i) { body_aquifer_query(B, i); });
     each(n, [&](int i) { body_aquifer_skip(B, i); });
     each(256 * kCellsY * n, [&](int i) { body_fill(B, i); });
     if (aquifer) std::memcpy(aquifer, bl.data(), sizeof(uint16_t) * bl.size());

@@ -13,9 +13,12 @@ SEEDS = [0, 1, -1, 12345, -9223372036854775808, 9223372036854775807, 2147483648,
 
 # chunk sets: origin block, near / far / world border (reference corpus positions),
 # the 32-bit noise-lattice wrap chunks, the literal +/-117,187 border reading, and
-# chunks whose surface biomes trigger the eroded-badlands and frozen-ocean extensions
+# chunks whose surface biomes trigger the eroded-badlands and frozen-ocean extensions, and
+# chunks past the BlockPos wrap of the aquifer cell locations (|c| from 2^21 - 1 to the
+# accepted 2^23 - 1)
 CHUNKS = [(0, 0), (1, 0), (0, 1), (-1, -1), (6250, -6250), (-625000, 625000), (1874999, -1874999), (-1874999, 1874999), (6128, -6129),
-          (-6129, 6128), (117187, -117187), (-4000, -3360), (-4000, -1440), (-4000, 1600)]
+          (-6129, 6128), (117187, -117187), (-4000, -3360), (-4000, -1440), (-4000, 1600), (2097148, -2097149), (3000000, -5000000),
+          (-8388607, 8388607)]
 
 
 def compare(got_blocks, got_biomes, ref_blocks, ref_biomes, chunks):

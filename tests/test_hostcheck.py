@@ -65,7 +65,8 @@ def test_point_path_roots(ref_model, ir):
         assert (hostcheck.point(77, k, xyz).view(np.uint32) == want.view(np.uint32)).all(), name
 
 
-CHUNKS = [(0, 0), (-1, -1), (6128, -6129), (1874999, -1874999), (117187, -117187), (-4000, -3360), (-4000, -1440), (-4000, 1600)]
+CHUNKS = [(0, 0), (-1, -1), (6128, -6129), (1874999, -1874999), (117187, -117187), (-4000, -3360), (-4000, -1440), (-4000, 1600),
+          (2097148, -2097149), (3000000, -5000000), (-2097152, 4194303), (8388607, -8388607)]
 
 
 @pytest.mark.parametrize('seed', [12345, -1])
@@ -76,6 +77,17 @@ def test_whole_chunks(ref_model, seed):
         assert (q[i] == rq[i]).all(), c
         assert (aq[i] == raq[i]).all(), c
         assert (b[i] == rb[i]).all(), c
+
+
+def test_random_chunks(ref_model):
+    """Scattered chunks of random seeds: every aquifer decision (the nearest-cell scan and
+    the per-query shortcuts) on terrain of all kinds, blocks after the fill and final."""
+    rng = np.random.default_rng(5)
+    for seed in [int(v) for v in rng.integers(-(1 << 62), 1 << 62, 3)]:
+        chunks = [(int(a), int(b)) for a, b in zip(rng.integers(-200000, 200000, 24), rng.integers(-200000, 200000, 24))]
+        b, q, aq = hostcheck.generate(seed, chunks, aquifer=True)
+        rb, rq, raq = ref_model.seed(seed).generate(chunks, aquifer=True)
+        assert (aq == raq).all() and (b == rb).all() and (q == rq).all(), seed
 
 
 @pytest.mark.parametrize('seed', [123456789, -4172144997902289642])
