@@ -120,6 +120,14 @@ TB_HD TB_FI int32_t fdiv(int32_t a, int32_t b) {
 }
 TB_HD TB_FI int32_t fmod_i(int32_t a, int32_t b) { return a - fdiv(a, b) * b; }
 TB_HD TB_FI int32_t imin(int32_t a, int32_t b) { return a < b ? a : b; }
+// index of the highest set bit of m != 0
+TB_HD TB_FI int hibit(uint32_t m) {
+#if defined(__CUDA_ARCH__)
+    return 31 - __clz(m);
+#else
+    return 31 - __builtin_clz(m);
+#endif
+}
 TB_HD TB_FI int32_t imax(int32_t a, int32_t b) { return a < b ? b : a; }
 
 // Math.min / Math.max (float and double): NaN propagates from either side, and

@@ -25,6 +25,9 @@ constexpr int kBlocksPerChunk = 256 * tbm::kHeight;
 constexpr int kRows = tbm::kHeight / 8 + 1;              // 4x8 cell corner rows
 constexpr int kCellsY = tbm::kHeight / 8;
 constexpr int kMaxY = tbm::kMinY + tbm::kHeight - 1;
+// Column masks: 32 heights per word, air words then fluid words.
+constexpr int kMaskWords = tbm::kHeight / 32;
+static_assert(tbm::kHeight % 32 == 0, "column mask words");
 constexpr int kGridX = 27, kGridZ = 19, kGrid = kGridX * kGridZ;   // surface-level quarts per chunk
 constexpr int kAqX = 3, kAqY = 35, kAqZ = 3, kAqCells = kAqX * kAqY * kAqZ;
 constexpr int kAqMinGridY = -7;
@@ -138,6 +141,9 @@ struct Batch {
     uint32_t* walk;                   // n * kBlocksPerChunk packed column-walk state per block
     uint8_t* bbiome;                  // n * kBlocksPerChunk zoomed biome per block up to the column height
     uint8_t* oremask;                 // n * kBlocksPerChunk ore-vein density tests passed, bit per vein
+    uint32_t* colmask;                // n * 2 * kMaskWords * 256: word w of column lz * 16 + lx at
+                                      // (c * 2 * kMaskWords + w) * 256 + column; words below
+                                      // kMaskWords hold air, the rest fluid; bit k = y kMinY + 32 w + k
     struct ColumnRec* colrec;         // n * 256 per-column surface context
 };
 
@@ -175,6 +181,15 @@ TB_HD TB_FI int32_t add32(int32_t* p, int32_t v) {
     const int32_t old = *p;
     *p += v;
     return old;
+#endif
+}
+// The largest v over the warp's lanes that run together here (device) or v itself (host
+// build, where items run one at a time). Either way the result is at least v.
+TB_HD TB_FI int warp_max(int v) {
+#if defined(__CUDA_ARCH__)
+    return __reduce_max_sync(__activemask(), v);
+#else
+    return v;
 #endif
 }
 TB_HD TB_FI void max32(int32_t* p, int32_t v) {
@@ -909,6 +924,7 @@ TB_HD inline void body_fill(const Batch& B, int it) {
     const int skip = B.aq_skip[c];
     uint16_t* out = B.blocks + static_cast<size_t>(c) * kBlocksPerChunk;
     int top = INT_MIN;
+    uint32_t air = 0, fluid = 0;
     for (int k = 0; k < 8; ++k) {
         const int y = tbm::kMinY + cell_y * 8 + k;
         const float d = tbgen::gen_final_density(S.nt, bx, y, bz, ch);
@@ -922,9 +938,16 @@ TB_HD inline void body_fill(const Batch& B, int it) {
                 if (!(tbgen::gen_ore_density(k, S.nt, bx, y, bz, ch) <= 0.0f)) om |= 1u << k;
             B.oremask[static_cast<size_t>(c) * kBlocksPerChunk + bi] = static_cast<uint8_t>(om);
         }
-        if (!(B.M.block_flags[s] & 1)) top = y;
+        const uint8_t f = B.M.block_flags[s];
+        if (!(f & 1)) top = y;
+        air |= static_cast<uint32_t>(f & 1) << k;
+        fluid |= static_cast<uint32_t>((f >> 3) & 1) << k;
         for (int q = 0; q < tbm::kNumChannels; ++q) ch[q] += ci.step[q];
     }
+    // the cell's 8 heights are byte cell_y & 3 of mask word cell_y >> 2 (little-endian words)
+    uint8_t* cm = reinterpret_cast<uint8_t*>(B.colmask + (static_cast<size_t>(c) * 2 * kMaskWords + (cell_y >> 2)) * 256 + col) + (cell_y & 3);
+    cm[0] = static_cast<uint8_t>(air);
+    cm[static_cast<size_t>(kMaskWords) * 256 * 4] = static_cast<uint8_t>(fluid);
     if (top != INT_MIN) max32(B.h0 + static_cast<size_t>(c) * 256 + lx * 16 + lz, top + 1);
 }
 
@@ -1359,6 +1382,22 @@ struct RuleCtx {
 
 // pass 1 (item = chunk * 256 + z * 16 + x): eroded badlands (writes), heights after it
 // and after a dry run of the frozen-ocean extension
+// Air and fluid words of one column rebuilt from its blocks, after a pass that turned air
+// into other blocks.
+TB_HD inline void column_mask_rebuild(const Batch& B, const Column& C) {
+    uint32_t* cm = B.colmask + static_cast<size_t>(C.c) * 2 * kMaskWords * 256 + C.lz * 16 + C.lx;
+    for (int w = 0; w < kMaskWords; ++w) {
+        uint32_t air = 0, fluid = 0;
+        for (int k = 0; k < 32; ++k) {
+            const uint8_t f = C.flags(C.get(tbm::kMinY + 32 * w + k));
+            air |= static_cast<uint32_t>(f & 1) << k;
+            fluid |= static_cast<uint32_t>((f >> 3) & 1) << k;
+        }
+        cm[w * 256] = air;
+        cm[(kMaskWords + w) * 256] = fluid;
+    }
+}
+
 TB_HD inline void body_surface1(const Batch& B, int it) {
     const int c = it >> 8, lz = (it >> 4) & 15, lx = it & 15;
     const int ci = (c << 8) | (lx << 4) | lz;   // x * 16 + z column index
@@ -1366,7 +1405,10 @@ TB_HD inline void body_surface1(const Batch& B, int it) {
              B.h0[ci]};
     const int start_h = C.hm;
     const int surface_biome = zoom_biome_tab(B, c, C.bx, start_h, C.bz);
-    if (surface_biome == tbm::kBiomeErodedBadlands) eroded_badlands(C, start_h);
+    if (surface_biome == tbm::kBiomeErodedBadlands) {
+        eroded_badlands(C, start_h);
+        column_mask_rebuild(B, C);
+    }
     B.h1[ci] = C.hm;
     if (surface_biome == tbm::kBiomeFrozenOcean || surface_biome == tbm::kBiomeDeepFrozenOcean) {
         const double n = C.noise<tbm::kNoise_surface>(C.bx, 0.0, C.bz);
@@ -1503,24 +1545,47 @@ TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
     R.min_surf = r.min_surface;
     R.sec_set = true;
     R.secondary = r.secondary;
+    // The walk reads the column's air and fluid bits, which stay true while it runs (the rules
+    // never make air or fluid). All lanes of a warp walk the same height: above its own
+    // height a column holds air, which leaves the walk state as it starts.
+    const uint32_t* cm = B.colmask + static_cast<size_t>(c) * 2 * kMaskWords * 256 + (it & 255);
     const int height = C.hm;
+#if defined(__CUDA_ARCH__)
+    const int start = warp_max(height > kMaxY ? kMaxY : height);
+#else
+    // the host build takes the maximum over the same 32 items a device warp holds
+    int start = INT_MIN;
+    for (int j = it & ~31; j < (it & ~31) + 32; ++j) {
+        const int h = B.h1[(static_cast<size_t>(c) << 8) | ((j & 15) << 4) | ((j >> 4) & 15)];
+        start = imax(start, h > kMaxY ? kMaxY : h);
+    }
+#endif
     int stone_above = 0, water_height = INT_MIN, next_ceiling = INT_MAX;
-    for (int y = height > kMaxY ? kMaxY : height; y >= tbm::kMinY; --y) {
-        const uint8_t f = C.flags(C.get(y));
-        if (f & 1) {
+    int wi = -1;
+    uint32_t aw = 0, fw = 0;
+    for (int y = start; y >= tbm::kMinY; --y) {
+        const int r = y - tbm::kMinY;
+        if ((r >> 5) != wi) {
+            wi = r >> 5;
+            aw = cm[wi * 256];
+            fw = cm[(kMaskWords + wi) * 256];
+        }
+        const uint32_t bit = 1u << (r & 31);
+        if (aw & bit) {
             stone_above = 0;
             water_height = INT_MIN;
-        } else if (f & 8) {
+        } else if (fw & bit) {
             if (water_height == INT_MIN) water_height = y + 1;
         } else {
             if (next_ceiling >= y) {
-                next_ceiling = kWayBelowMinY;
-                for (int la = y - 1; la >= tbm::kMinY - 1; --la) {
-                    if (C.flags(C.get(la)) & 9) {
-                        next_ceiling = la + 1;
-                        break;
-                    }
+                // one above the highest air or fluid block below y; below the world is air
+                uint32_t m = (aw | fw) & (bit - 1u);
+                int w = wi;
+                while (m == 0 && w > 0) {
+                    --w;
+                    m = cm[w * 256] | cm[(kMaskWords + w) * 256];
                 }
+                next_ceiling = m != 0 ? tbm::kMinY + 32 * w + hibit(m) + 1 : tbm::kMinY;
             }
             ++stone_above;
             R.y = y;

@@ -430,7 +430,7 @@ struct OutSlot {
 // two output slots run concurrently on two streams.
 struct Work {
     DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_cell,
-        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_walk, d_bbiome, d_oremask, d_colrec;
+        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_walk, d_bbiome, d_oremask, d_colmask, d_colrec;
     TableBufs tb_b, tb_c, tb_s;
     void alloc(int n) {
         const size_t N = static_cast<size_t>(n);
@@ -463,6 +463,7 @@ struct Work {
         if (!TB_FUSED_WALK) d_walk.alloc(sizeof(uint32_t) * N * kBlocksPerChunk);   // per-block walk states of the split pass
         d_bbiome.alloc(N * kBlocksPerChunk);
         if (TB_ORE_MASK) d_oremask.alloc(N * kBlocksPerChunk);
+        d_colmask.alloc(sizeof(uint32_t) * N * 2 * kMaskWords * 256);
         d_colrec.alloc(sizeof(ColumnRec) * N * 256);
     }
 };
@@ -679,6 +680,7 @@ struct Generator {
         B.walk = W.d_walk.as<uint32_t>();
         B.bbiome = W.d_bbiome.as<uint8_t>();
         B.oremask = W.d_oremask.as<uint8_t>();
+        B.colmask = W.d_colmask.as<uint32_t>();
         B.colrec = W.d_colrec.as<ColumnRec>();
         return B;
     }

@@ -105,6 +105,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     std::vector<uint16_t> bl(N * kBlocksPerChunk);
     std::vector<uint32_t> ztab(N * kZoomVerts), walk(N * kBlocksPerChunk);
     std::vector<uint8_t> bbiome(N * kBlocksPerChunk), oremask(N * kBlocksPerChunk);
+    std::vector<uint32_t> colmask(N * 2 * kMaskWords * 256);
     std::vector<ColumnRec> colrec(N * 256);
     Batch B{};
     B.M = R.M;
@@ -142,6 +143,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     B.walk = walk.data();
     B.bbiome = bbiome.data();
     B.oremask = oremask.data();
+    B.colmask = colmask.data();
     B.colrec = colrec.data();
     each(9 * n, [&](int i) { body_nb_insert(B, i); });
     each(9 * n, [&](int i) { body_nb_resolve(B, i); });
