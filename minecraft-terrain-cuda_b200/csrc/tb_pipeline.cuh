@@ -138,6 +138,7 @@ struct Batch {
     int32_t* h2;                      // after the frozen-ocean extension (dry run)
     uint8_t* biomes_out;              // n * kQuartsPerChunk
     uint32_t* zoom_tab;               // n * kZoomVerts packed fiddle draws per quart vertex
+    uint8_t* zoom_uni;                // n * kZoomCells: the biome all 8 corners of a zoom cell store, or kZoomMixed
     uint32_t* walk;                   // n * kBlocksPerChunk packed column-walk state per block
     uint8_t* bbiome;                  // n * kBlocksPerChunk zoomed biome per block up to the column height
     uint8_t* oremask;                 // n * kBlocksPerChunk ore-vein density tests passed, bit per vein
@@ -1081,6 +1082,24 @@ TB_HD inline void body_zoom_table(const Batch& B, int it) {
 constexpr int kZoomPyMin = (tbm::kMinY - 2) >> 2;
 constexpr int kZoomGroups = ((kMaxY - 2) >> 2) - kZoomPyMin + 1;
 
+// Zoom cells of a chunk: the corner quart (px, py, pz) of the 8 candidates of its blocks,
+// px and pz over the 5 values ((cx * 16 - 2) >> 2 .. (cx * 16 + 13) >> 2), py over the groups.
+constexpr int kZoomCells = kZoomGroups * 25;
+constexpr uint8_t kZoomMixed = 0xFF;
+static_assert(tbm::kNumBiomes < kZoomMixed, "biome ids below the mixed marker");
+
+// item = chunk * kZoomCells + (group * 5 + pz - (cz * 4 - 1)) * 5 + px - (cx * 4 - 1). When
+// the 8 candidate quarts of a cell store one biome, every block of the cell zooms to it,
+// whichever corner is nearest.
+TB_HD inline void body_zoom_uniform(const Batch& B, int it) {
+    const int c = it / kZoomCells, r = it % kZoomCells;
+    const int px = B.cx[c] * 4 - 1 + r % 5, pz = B.cz[c] * 4 - 1 + (r / 5) % 5, py = kZoomPyMin + r / 25;
+    const int b0 = zoom_stored(B, c, 0, px, py, pz);
+    bool uni = true;
+    for (int i = 1; i < 8; ++i) uni = uni && zoom_stored(B, c, i, px, py, pz) == b0;
+    B.zoom_uni[it] = uni ? static_cast<uint8_t>(b0) : kZoomMixed;
+}
+
 // item = (chunk * kZoomGroups + group) * 256 + z * 16 + x; blocks up to the column height
 TB_HD inline void body_block_biome(const Batch& B, int it) {
     const int col = it & 255, g = (it >> 8) % kZoomGroups, c = (it >> 8) / kZoomGroups;
@@ -1093,9 +1112,15 @@ TB_HD inline void body_block_biome(const Batch& B, int it) {
     if (ylo > yhi) return;
     const int x = B.cx[c] * 16 + lx, z = B.cz[c] * 16 + lz;
     const int ax = x - 2, az = z - 2, px = ax >> 2, pz = az >> 2;
+    const int qx0 = B.cx[c] * 4 - 1, qz0 = B.cz[c] * 4 - 1;
+    uint8_t* out = B.bbiome + static_cast<size_t>(c) * kBlocksPerChunk;
+    const uint8_t uni = B.zoom_uni[static_cast<size_t>(c) * kZoomCells + (g * 5 + pz - qz0) * 5 + px - qx0];
+    if (uni != kZoomMixed) {
+        for (int y = ylo; y <= yhi; ++y) out[((y - tbm::kMinY) * 16 + lz) * 16 + lx] = uni;
+        return;
+    }
     const double fx = static_cast<double>(ax & 3) / 4.0, fz = static_cast<double>(az & 3) / 4.0;
     const uint32_t* tab = B.zoom_tab + static_cast<size_t>(c) * kZoomVerts;
-    const int qx0 = B.cx[c] * 4 - 1, qz0 = B.cz[c] * 4 - 1;
     double sx[8], sz[8], oy[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
@@ -1109,7 +1134,6 @@ TB_HD inline void body_block_biome(const Batch& B, int it) {
         sz[i] = (dz + oz) * (dz + oz);
         sx[i] = (dx + ox) * (dx + ox);
     }
-    uint8_t* out = B.bbiome + static_cast<size_t>(c) * kBlocksPerChunk;
     for (int y = ylo; y <= yhi; ++y) {
         const double fy = static_cast<double>((y - 2) & 3) / 4.0;
         int best = 0;

@@ -430,7 +430,7 @@ struct OutSlot {
 // two output slots run concurrently on two streams.
 struct Work {
     DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_cell,
-        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_walk, d_bbiome, d_oremask, d_colmask, d_colrec;
+        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_zoom_uni, d_walk, d_bbiome, d_oremask, d_colmask, d_colrec;
     TableBufs tb_b, tb_c, tb_s;
     void alloc(int n) {
         const size_t N = static_cast<size_t>(n);
@@ -460,6 +460,7 @@ struct Work {
         d_h1.alloc(4 * 256 * N);
         d_h2.alloc(4 * 256 * N);
         d_zoom.alloc(sizeof(uint32_t) * N * kZoomVerts);
+        d_zoom_uni.alloc(N * kZoomCells);
         if (!TB_FUSED_WALK) d_walk.alloc(sizeof(uint32_t) * N * kBlocksPerChunk);   // per-block walk states of the split pass
         d_bbiome.alloc(N * kBlocksPerChunk);
         if (TB_ORE_MASK) d_oremask.alloc(N * kBlocksPerChunk);
@@ -677,6 +678,7 @@ struct Generator {
         B.h2 = W.d_h2.as<int32_t>();
         B.biomes_out = o ? o->biomes.as<uint8_t>() : nullptr;
         B.zoom_tab = W.d_zoom.as<uint32_t>();
+        B.zoom_uni = W.d_zoom_uni.as<uint8_t>();
         B.walk = W.d_walk.as<uint32_t>();
         B.bbiome = W.d_bbiome.as<uint8_t>();
         B.oremask = W.d_oremask.as<uint8_t>();
@@ -716,6 +718,7 @@ struct Generator {
         launch(k_dyn<body_corner_col, 1>, s, 16 * nmax, B, cnt_c);
         launch(k_dyn<body_corner, kRows, TB_MINB_CORNER>, s, 16 * nmax * kRows, B, cnt_c);
         launch(k_items<body_zoom_table, kZoomVerts>, s, kZoomVerts * nmax, B);
+        launch(k_items<body_zoom_uniform, kZoomCells>, s, kZoomCells * nmax, B);
         mark(2);
         W.tb_s.reset(s);
         launch(k_items<body_sg_insert, kGrid>, s, kGrid * nmax, B);

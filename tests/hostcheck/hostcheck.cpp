@@ -106,6 +106,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     std::vector<uint32_t> ztab(N * kZoomVerts), walk(N * kBlocksPerChunk);
     std::vector<uint8_t> bbiome(N * kBlocksPerChunk), oremask(N * kBlocksPerChunk);
     std::vector<uint32_t> colmask(N * 2 * kMaskWords * 256);
+    std::vector<uint8_t> zuni(N * kZoomCells);
     std::vector<ColumnRec> colrec(N * 256);
     Batch B{};
     B.M = R.M;
@@ -140,6 +141,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     B.h2 = h2.data();
     B.biomes_out = bout.data();
     B.zoom_tab = ztab.data();
+    B.zoom_uni = zuni.data();
     B.walk = walk.data();
     B.bbiome = bbiome.data();
     B.oremask = oremask.data();
@@ -155,6 +157,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     each(hc.count, [&](int i) { body_corner_col(B, i); });
     each(hc.count * kRows, [&](int i) { body_corner(B, i); });
     each(kZoomVerts * n, [&](int i) { body_zoom_table(B, i); });
+    each(kZoomCells * n, [&](int i) { body_zoom_uniform(B, i); });
     each(kGrid * n, [&](int i) { body_sg_insert(B, i); });
     each(kGrid * n, [&](int i) { body_sg_resolve(B, i); });
     each(hs.count, [&](int i) { body_surface_level(B, i); });
