@@ -28,6 +28,15 @@ constexpr int kMaxY = tbm::kMinY + tbm::kHeight - 1;
 // Column masks: 32 heights per word, air words then fluid words.
 constexpr int kMaskWords = tbm::kHeight / 32;
 static_assert(tbm::kHeight % 32 == 0, "column mask words");
+// Per-block bytes the column walk reads (zoomed biome, ore-vein bits) in column order: 4
+// heights per 32-bit word, word (y - kMinY) >> 2 of column lz * 16 + lx at
+// (c * kColWords + word) * 256 + column, byte (y - kMinY) & 3 of it (little-endian), so that
+// a warp's 32 columns read 128 contiguous bytes per 4 heights.
+constexpr int kColWords = tbm::kHeight / 4;
+TB_HD TB_FI size_t colbyte(int c, int col, int y) {
+    const int r = y - tbm::kMinY;
+    return ((static_cast<size_t>(c) * kColWords + (r >> 2)) * 256 + col) * 4 + (r & 3);
+}
 constexpr int kGridX = 27, kGridZ = 19, kGrid = kGridX * kGridZ;   // surface-level quarts per chunk
 constexpr int kAqX = 3, kAqY = 35, kAqZ = 3, kAqCells = kAqX * kAqY * kAqZ;
 constexpr int kAqMinGridY = -7;
@@ -139,9 +148,8 @@ struct Batch {
     uint8_t* biomes_out;              // n * kQuartsPerChunk
     uint32_t* zoom_tab;               // n * kZoomVerts packed fiddle draws per quart vertex
     uint8_t* zoom_uni;                // n * kZoomCells: the biome all 8 corners of a zoom cell store, or kZoomMixed
-    uint32_t* walk;                   // n * kBlocksPerChunk packed column-walk state per block
-    uint8_t* bbiome;                  // n * kBlocksPerChunk zoomed biome per block up to the column height
-    uint8_t* oremask;                 // n * kBlocksPerChunk ore-vein density tests passed, bit per vein
+    uint8_t* bbiome;                  // n * kBlocksPerChunk zoomed biome per block up to the column height, colbyte order
+    uint8_t* oremask;                 // n * kBlocksPerChunk ore-vein density tests passed, bit per vein, colbyte order
     uint32_t* colmask;                // n * 2 * kMaskWords * 256: word w of column lz * 16 + lx at
                                       // (c * 2 * kMaskWords + w) * 256 + column; words below
                                       // kMaskWords hold air, the rest fluid; bit k = y kMinY + 32 w + k
@@ -154,15 +162,11 @@ struct ColumnRec {
     int32_t surface_depth, min_surface, grad_x, grad_z;
     int32_t surface_biome, start_h;
 };
-constexpr uint32_t kNoWalk = 0xFFFFFFFFu;
 // Per block, bit k: whether ore vein k's density test passes (its density is not <= 0),
 // decided by the fill from the channel values it already holds, so that the rule tree
 // interpolates channels only inside veins.
 #ifndef TB_ORE_MASK
 #define TB_ORE_MASK (tbm::kNumOres <= 8)
-#endif
-#ifndef TB_FUSED_WALK
-#define TB_FUSED_WALK 1     // rule tree inside the column walk (1) or a per-block pass after it (0)
 #endif
 
 // ---- atomics (device) / plain operations (host test build) --------------------------------------
@@ -925,7 +929,7 @@ TB_HD inline void body_fill(const Batch& B, int it) {
     const int skip = B.aq_skip[c];
     uint16_t* out = B.blocks + static_cast<size_t>(c) * kBlocksPerChunk;
     int top = INT_MIN;
-    uint32_t air = 0, fluid = 0;
+    uint32_t air = 0, fluid = 0, ore_lo = 0, ore_hi = 0;
     for (int k = 0; k < 8; ++k) {
         const int y = tbm::kMinY + cell_y * 8 + k;
         const float d = tbgen::gen_final_density(S.nt, bx, y, bz, ch);
@@ -935,9 +939,10 @@ TB_HD inline void body_fill(const Batch& B, int it) {
         out[bi] = static_cast<uint16_t>(s);
         if (TB_ORE_MASK) {
             uint32_t om = 0;
-            for (int k = 0; k < tbm::kNumOres; ++k)
-                if (!(tbgen::gen_ore_density(k, S.nt, bx, y, bz, ch) <= 0.0f)) om |= 1u << k;
-            B.oremask[static_cast<size_t>(c) * kBlocksPerChunk + bi] = static_cast<uint8_t>(om);
+            for (int v = 0; v < tbm::kNumOres; ++v)
+                if (!(tbgen::gen_ore_density(v, S.nt, bx, y, bz, ch) <= 0.0f)) om |= 1u << v;
+            if (k < 4) ore_lo |= om << (8 * k);
+            else ore_hi |= om << (8 * (k - 4));
         }
         const uint8_t f = B.M.block_flags[s];
         if (!(f & 1)) top = y;
@@ -949,6 +954,12 @@ TB_HD inline void body_fill(const Batch& B, int it) {
     uint8_t* cm = reinterpret_cast<uint8_t*>(B.colmask + (static_cast<size_t>(c) * 2 * kMaskWords + (cell_y >> 2)) * 256 + col) + (cell_y & 3);
     cm[0] = static_cast<uint8_t>(air);
     cm[static_cast<size_t>(kMaskWords) * 256 * 4] = static_cast<uint8_t>(fluid);
+    if (TB_ORE_MASK) {
+        // the cell's 8 heights are words 2 cell_y and 2 cell_y + 1 of the column
+        uint32_t* ow = reinterpret_cast<uint32_t*>(B.oremask) + (static_cast<size_t>(c) * kColWords + 2 * cell_y) * 256 + col;
+        ow[0] = ore_lo;
+        ow[256] = ore_hi;
+    }
     if (top != INT_MIN) max32(B.h0 + static_cast<size_t>(c) * 256 + lx * 16 + lz, top + 1);
 }
 
@@ -1113,10 +1124,9 @@ TB_HD inline void body_block_biome(const Batch& B, int it) {
     const int x = B.cx[c] * 16 + lx, z = B.cz[c] * 16 + lz;
     const int ax = x - 2, az = z - 2, px = ax >> 2, pz = az >> 2;
     const int qx0 = B.cx[c] * 4 - 1, qz0 = B.cz[c] * 4 - 1;
-    uint8_t* out = B.bbiome + static_cast<size_t>(c) * kBlocksPerChunk;
     const uint8_t uni = B.zoom_uni[static_cast<size_t>(c) * kZoomCells + (g * 5 + pz - qz0) * 5 + px - qx0];
     if (uni != kZoomMixed) {
-        for (int y = ylo; y <= yhi; ++y) out[((y - tbm::kMinY) * 16 + lz) * 16 + lx] = uni;
+        for (int y = ylo; y <= yhi; ++y) B.bbiome[colbyte(c, col, y)] = uni;
         return;
     }
     const double fx = static_cast<double>(ax & 3) / 4.0, fz = static_cast<double>(az & 3) / 4.0;
@@ -1148,7 +1158,7 @@ TB_HD inline void body_block_biome(const Batch& B, int it) {
                 best_d = d;
             }
         }
-        out[((y - tbm::kMinY) * 16 + lz) * 16 + lx] = static_cast<uint8_t>(zoom_stored(B, c, best, px, py, pz));
+        B.bbiome[colbyte(c, col, y)] = static_cast<uint8_t>(zoom_stored(B, c, best, px, py, pz));
     }
 }
 
@@ -1349,16 +1359,10 @@ struct RuleCtx {
     float prelim;
     // block
     int y, stone_above, stone_below, water_height;
-    bool biome_set;
-    int biome_v;
+    int biome_v;        // zoomed biome of the block
+    uint32_t ore_bits;  // its ore-vein density tests
 
-    TB_HD TB_FI int biome() {
-        if (!biome_set) {
-            biome_v = B->bbiome[static_cast<size_t>(c) * kBlocksPerChunk + col->idx(y)];
-            biome_set = true;
-        }
-        return biome_v;
-    }
+    TB_HD TB_FI int biome() const { return biome_v; }
     TB_HD TB_FI double noise2d(int k, int first, int count) const {
         return static_cast<double>(stack_point_rt(col->S->nt, first, count, col->bx, 0.0, col->bz));
     }
@@ -1396,7 +1400,7 @@ struct RuleCtx {
     // OreVeinRule: the density inline (its guards usually end it after a y test), the rest
     // out of line
     TB_HD TB_FI int ore_vein(int k, int ore, int raw, int filler, float chance) const {
-        if (TB_ORE_MASK && !((B->oremask[static_cast<size_t>(c) * kBlocksPerChunk + col->idx(y)] >> k) & 1)) return -1;
+        if (TB_ORE_MASK && !((ore_bits >> k) & 1)) return -1;
         const LazyChannels ch{B, c, col->lx, col->lz, y, false, {}};
         const float density = tbgen::gen_ore_density(k, col->S->nt, col->bx, y, col->bz, ch);
         if (density <= 0.0f) return -1;
@@ -1442,94 +1446,6 @@ TB_HD inline void body_surface1(const Batch& B, int it) {
         frozen_ocean(C, min_surface, surface_biome, start_h, false);
     }
     B.h2[ci] = C.hm;
-}
-
-// pass 2a (item = chunk * 256 + z * 16 + x): the column context and the top-down walk
-// state of every solid block (stone above, stone below, water height), packed per block.
-// The rule tree reads no block other than its own and never turns a block into air or a
-// fluid, so these states are those the sequential walk sees.
-TB_HD inline void body_surface_walk(const Batch& B, int it) {
-    const int c = it >> 8, lz = (it >> 4) & 15, lx = it & 15;
-    const int ci = (c << 8) | (lx << 4) | lz;   // x * 16 + z column index
-    const size_t hb = static_cast<size_t>(c) * 256;
-    Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
-             B.h1[ci]};
-    // heights of the neighbours as vanilla's x-major, z-minor column order sees them
-    auto H = [&](int x, int z) -> int {
-        if (x == lx && z == lz) return B.h1[hb + x * 16 + z] - 1;
-        const bool done = x < lx || (x == lx && z < lz);
-        return (done ? B.h2[hb + x * 16 + z] : B.h0[hb + x * 16 + z]) - 1;
-    };
-    ColumnRec r;
-    r.start_h = B.h0[ci];
-    r.surface_biome = zoom_biome_tab(B, c, C.bx, r.start_h, C.bz);
-    r.grad_x = H(lx + 1 < 15 ? lx + 1 : 15, lz) - H(lx - 1 > 0 ? lx - 1 : 0, lz);
-    r.grad_z = H(lx, lz + 1 < 15 ? lz + 1 : 15) - H(lx, lz - 1 > 0 ? lz - 1 : 0);
-    const double n = C.noise<tbm::kNoise_surface>(C.bx, 0.0, C.bz);
-    const double rr = C.S->random.at(C.bx, 0, C.bz).next_double();
-    r.surface_depth = d2i(n * 2.75 + 3.0 + rr * 0.25);
-    r.min_surface = jfloor(static_cast<double>(prelim_surface(B, c, lx, lz))) + r.surface_depth - 8;
-    r.secondary = C.noise<tbm::kNoise_surface_secondary>(C.bx, 0.0, C.bz);
-    B.colrec[ci] = r;
-    uint32_t* walk = B.walk + static_cast<size_t>(c) * kBlocksPerChunk;
-    const int height = C.hm;
-    for (int y = kMaxY; y > height && y >= tbm::kMinY; --y) walk[C.idx(y)] = kNoWalk;
-    int stone_above = 0, water_height = INT_MIN, next_ceiling = INT_MAX;
-    for (int y = height > kMaxY ? kMaxY : height; y >= tbm::kMinY; --y) {
-        const uint8_t f = C.flags(C.get(y));
-        uint32_t w = kNoWalk;
-        if (f & 1) {
-            stone_above = 0;
-            water_height = INT_MIN;
-        } else if (f & 8) {
-            if (water_height == INT_MIN) water_height = y + 1;
-        } else {
-            if (next_ceiling >= y) {
-                next_ceiling = kWayBelowMinY;
-                for (int la = y - 1; la >= tbm::kMinY - 1; --la) {
-                    if (C.flags(C.get(la)) & 9) {
-                        next_ceiling = la + 1;
-                        break;
-                    }
-                }
-            }
-            ++stone_above;
-            const uint32_t below = static_cast<uint32_t>(y - next_ceiling + 1);
-            const uint32_t wh = water_height == INT_MIN ? 1023u : static_cast<uint32_t>(water_height - tbm::kMinY);
-            w = static_cast<uint32_t>(stone_above) | (below << 10) | (wh << 20);
-        }
-        walk[C.idx(y)] = w;
-    }
-}
-
-// pass 2b (item = chunk * kBlocksPerChunk + block index): the rule tree for one solid block
-TB_HD inline void body_surface_rules(const Batch& B, int it) {
-    const int c = it / kBlocksPerChunk, b = it % kBlocksPerChunk;
-    const uint32_t w = B.walk[it];
-    if (w == kNoWalk) return;
-    const int lx = b & 15, lz = (b >> 4) & 15, y = tbm::kMinY + (b >> 8);
-    const int col = lx * 16 + lz;
-    const ColumnRec& r = B.colrec[static_cast<size_t>(c) * 256 + col];
-    Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz, 0};
-    RuleCtx R{};
-    R.col = &C;
-    R.B = &B;
-    R.c = c;
-    R.surface_depth = r.surface_depth;
-    R.grad_x = r.grad_x;
-    R.grad_z = r.grad_z;
-    R.min_set = true;
-    R.min_surf = r.min_surface;
-    R.sec_set = true;
-    R.secondary = r.secondary;
-    R.y = y;
-    R.stone_above = static_cast<int>(w & 1023u);
-    R.stone_below = static_cast<int>((w >> 10) & 1023u);
-    const uint32_t wh = w >> 20;
-    R.water_height = wh == 1023u ? INT_MIN : static_cast<int>(wh) + tbm::kMinY;
-    R.biome_set = false;
-    const int state = tbgen::apply_rules(R);
-    if (state >= 0) C.blocks[b] = static_cast<uint16_t>(state);
 }
 
 // pass 2 fused (item = chunk * 256 + z * 16 + x): the column context and the top-down walk,
@@ -1584,6 +1500,17 @@ TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
         start = imax(start, h > kMaxY ? kMaxY : h);
     }
 #endif
+    // Zoomed biomes and ore bits, 4 heights per word: the walk descends one height at a time,
+    // so the word below is loaded while the current one is in use.
+    const uint32_t* bwords = reinterpret_cast<const uint32_t*>(B.bbiome) + static_cast<size_t>(c) * kColWords * 256 + (it & 255);
+    const uint32_t* owords = reinterpret_cast<const uint32_t*>(B.oremask) + static_cast<size_t>(c) * kColWords * 256 + (it & 255);
+    int wq = (start - tbm::kMinY) >> 2;
+    uint32_t bq = bwords[wq * 256], oq = TB_ORE_MASK ? owords[wq * 256] : 0u;
+    uint32_t bq_next = 0, oq_next = 0;
+    if (wq > 0) {
+        bq_next = bwords[(wq - 1) * 256];
+        if (TB_ORE_MASK) oq_next = owords[(wq - 1) * 256];
+    }
     int stone_above = 0, water_height = INT_MIN, next_ceiling = INT_MAX;
     int wi = -1;
     uint32_t aw = 0, fw = 0;
@@ -1593,6 +1520,15 @@ TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
             wi = r >> 5;
             aw = cm[wi * 256];
             fw = cm[(kMaskWords + wi) * 256];
+        }
+        if ((r >> 2) != wq) {
+            wq = r >> 2;
+            bq = bq_next;
+            oq = oq_next;
+            if (wq > 0) {
+                bq_next = bwords[(wq - 1) * 256];
+                if (TB_ORE_MASK) oq_next = owords[(wq - 1) * 256];
+            }
         }
         const uint32_t bit = 1u << (r & 31);
         if (aw & bit) {
@@ -1616,7 +1552,8 @@ TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
             R.stone_above = stone_above;
             R.stone_below = y - next_ceiling + 1;
             R.water_height = water_height;
-            R.biome_set = false;
+            R.biome_v = static_cast<int>((bq >> (8 * (r & 3))) & 255u);
+            R.ore_bits = (oq >> (8 * (r & 3))) & 255u;
             const int state = tbgen::apply_rules(R);
             if (state >= 0) C.blocks[C.idx(y)] = static_cast<uint16_t>(state);
         }

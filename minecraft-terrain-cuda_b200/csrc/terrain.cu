@@ -68,9 +68,6 @@ double now_ms() { return std::chrono::duration<double, std::milli>(std::chrono::
 #ifndef TB_CHAIN_WARP
 #define TB_CHAIN_WARP 1     // last-result chain with one warp per biome chunk
 #endif
-#ifndef TB_MINB_SURFACE2
-#define TB_MINB_SURFACE2 4
-#endif
 #ifndef TB_MINB_FILL
 #define TB_MINB_FILL 1
 #endif
@@ -430,7 +427,7 @@ struct OutSlot {
 // two output slots run concurrently on two streams.
 struct Work {
     DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_cell,
-        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_zoom_uni, d_walk, d_bbiome, d_oremask, d_colmask, d_colrec;
+        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_zoom_uni, d_bbiome, d_oremask, d_colmask, d_colrec;
     TableBufs tb_b, tb_c, tb_s;
     void alloc(int n) {
         const size_t N = static_cast<size_t>(n);
@@ -461,7 +458,6 @@ struct Work {
         d_h2.alloc(4 * 256 * N);
         d_zoom.alloc(sizeof(uint32_t) * N * kZoomVerts);
         d_zoom_uni.alloc(N * kZoomCells);
-        if (!TB_FUSED_WALK) d_walk.alloc(sizeof(uint32_t) * N * kBlocksPerChunk);   // per-block walk states of the split pass
         d_bbiome.alloc(N * kBlocksPerChunk);
         if (TB_ORE_MASK) d_oremask.alloc(N * kBlocksPerChunk);
         d_colmask.alloc(sizeof(uint32_t) * N * 2 * kMaskWords * 256);
@@ -679,7 +675,6 @@ struct Generator {
         B.biomes_out = o ? o->biomes.as<uint8_t>() : nullptr;
         B.zoom_tab = W.d_zoom.as<uint32_t>();
         B.zoom_uni = W.d_zoom_uni.as<uint8_t>();
-        B.walk = W.d_walk.as<uint32_t>();
         B.bbiome = W.d_bbiome.as<uint8_t>();
         B.oremask = W.d_oremask.as<uint8_t>();
         B.colmask = W.d_colmask.as<uint32_t>();
@@ -737,12 +732,7 @@ struct Generator {
         launch(k_items<body_surface1, 256>, s, 256 * nmax, B);
         launch(k_items<body_block_biome, 256 * kZoomGroups>, s, 256L * kZoomGroups * nmax, B);
         mark(6);
-#if TB_FUSED_WALK
         launch(k_items<body_surface_walk_rules, 256, TB_MINB_WALK>, s, 256 * nmax, B);
-#else
-        launch(k_items<body_surface_walk, 256>, s, 256 * nmax, B);
-        launch(k_items<body_surface_rules, kBlocksPerChunk, TB_MINB_SURFACE2>, s, static_cast<long>(kBlocksPerChunk) * nmax, B);
-#endif
         mark(7);
         launch(k_items<body_surface_frozen, 256>, s, 256 * nmax, B);
         launch(k_items<body_gather, kQuartsPerChunk>, s, static_cast<long>(kQuartsPerChunk) * nmax, B);

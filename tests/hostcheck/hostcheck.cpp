@@ -103,7 +103,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     std::vector<int32_t> lstar(nb * kQuartsPerChunk), h0(256 * N, tbm::kMinY), h1(256 * N), h2(256 * N);
     std::vector<uint8_t> qbiome(nb * kQuartsPerChunk), bout(N * kQuartsPerChunk);
     std::vector<uint16_t> bl(N * kBlocksPerChunk);
-    std::vector<uint32_t> ztab(N * kZoomVerts), walk(N * kBlocksPerChunk);
+    std::vector<uint32_t> ztab(N * kZoomVerts);
     std::vector<uint8_t> bbiome(N * kBlocksPerChunk), oremask(N * kBlocksPerChunk);
     std::vector<uint32_t> colmask(N * 2 * kMaskWords * 256);
     std::vector<uint8_t> zuni(N * kZoomCells);
@@ -142,7 +142,6 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     B.biomes_out = bout.data();
     B.zoom_tab = ztab.data();
     B.zoom_uni = zuni.data();
-    B.walk = walk.data();
     B.bbiome = bbiome.data();
     B.oremask = oremask.data();
     B.colmask = colmask.data();
@@ -168,12 +167,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     if (aquifer) std::memcpy(aquifer, bl.data(), sizeof(uint16_t) * bl.size());
     each(256 * n, [&](int i) { body_surface1(B, i); });
     each(256 * kZoomGroups * n, [&](int i) { body_block_biome(B, i); });
-#if TB_FUSED_WALK
     each(256 * n, [&](int i) { body_surface_walk_rules(B, i); });
-#else
-    each(256 * n, [&](int i) { body_surface_walk(B, i); });
-    each(kBlocksPerChunk * n, [&](int i) { body_surface_rules(B, i); });
-#endif
     each(256 * n, [&](int i) { body_surface_frozen(B, i); });
     each(kQuartsPerChunk * n, [&](int i) { body_gather(B, i); });
     std::memcpy(blocks, bl.data(), sizeof(uint16_t) * bl.size());
