@@ -36,10 +36,12 @@ SEED = 0x5445525241494E31   # "TERRAIN1"
 REGIONS = [('origin', 0, 0), ('negative', -62500, -62500), ('border', 117124, 117124)]
 SIDE = 64
 BYTES_PER_CHUNK = 98304 * 2 + 1536
-WALK_BYTES_PER_CHUNK = 98304 * 2 + 98304
+# data the walk-rules kernel touches once per chunk: the u8 biome and u8 ore-vein bits of each
+# block read, its u16 state written, and the column air / fluid masks (2 x 12 words x 256 columns)
+WALK_BYTES_PER_CHUNK = 98304 * (1 + 1 + 2) + 2 * 12 * 4 * 256
 # dram__bytes_read.sum + dram__bytes_write.sum of one 4,096-chunk launch of the walk-rules
-# kernel in this workload (596.56 MB + 238.69 MB), from profiles/walk_rules_traffic.md
-WALK_TRAFFIC_PER_LAUNCH = 835250000
+# kernel in this workload (508.71 MB + 256.17 MB), from profiles/walk_rules_traffic.md
+WALK_TRAFFIC_PER_LAUNCH = 764880000
 METRIC = 'bit-exact TERRAIN chunks/s on 1 B200, served vs plain; p50/p99 request latency'
 
 
@@ -462,8 +464,8 @@ def run_ours(args, rank, world, local_rank):
         'roofline': {'bound': 'hbm', 'kernel': 'surface_walk_rules', 'achieved': round(achieved, 2), 'peak': peak, 'unit': 'GB/s',
                      'frac': round(achieved / peak, 5), 'traffic': WALK_TRAFFIC_PER_LAUNCH, 'peak_source': peak_kind,
                      'launch_ms': round(per_launch_ms, 3), 'share_of_step': round(per_launch_ms * calls / stage['kernel_ms'], 3),
-                     'note': 'algorithmic bytes = 294,912 B per chunk (the u16 block column read once, the u8 per-block biome read once) x '
-                             '4,096 chunks per launch; traffic = dram read + write bytes of one 4,096-chunk launch (ncu, '
+                     'note': 'algorithmic bytes = 417,792 B per chunk (per block the u8 biome and u8 ore bits read and the u16 state '
+                             'written, plus the column air / fluid masks) x 4,096 chunks per launch; traffic = dram read + write bytes of one 4,096-chunk launch (ncu, '
                              'profiles/walk_rules_traffic.md). The kernel is issue- and latency-bound (integer and FP64 rule '
                              'arithmetic), so its HBM fraction is small'},
         'e2e': {'value': round(e2e_value, 1), 'unit': 'chunks/s', 'h2d_bytes_per_step': int(n * nreg * 8),
