@@ -433,6 +433,80 @@ TB_HD inline int tree_first_min32_levels(const DevModel& M, const int32_t* t, in
 #define TB_SEARCH_LEVELS 1
 #endif
 
+// The first minimal leaf for G targets that agree in every coordinate but depth (index 4),
+// in one descent of the tree: a box's terms of the other coordinates are summed once, each
+// target adds its own depth term and keeps its own best (distance, rank, leaf), and a box is
+// entered when any target could find a better leaf in it. Each result is the one
+// tree_first_min32 gives for that target alone: both are the least (distance, rank) over
+// all leaves, and a box is skipped only when it cannot hold a better pair for any target.
+template <int G>
+struct MultiBest {
+    long long d[G];
+    int rank[G], leaf[G];
+};
+TB_HD TB_FI long long box_dist32_no_depth(const RBox& n, const int32_t* t) {
+    long long d = 0;
+#pragma unroll
+    for (int i = 0; i < 7; ++i) {
+        if (i == 4) continue;
+        const int32_t tv = i < 6 ? t[i] : 0;
+        int32_t p = tv - n.mx[i];
+        const int32_t q = n.mn[i] - tv;
+        p = p > q ? p : q;
+        p = p > 0 ? p : 0;
+        d += static_cast<long long>(static_cast<unsigned long long>(static_cast<uint32_t>(p)) * static_cast<uint32_t>(p));
+    }
+    return d;
+}
+TB_HD TB_FI long long depth_term32(const RBox& n, int32_t depth) {
+    int32_t p = depth - n.mx[4];
+    const int32_t q = n.mn[4] - depth;
+    p = p > q ? p : q;
+    p = p > 0 ? p : 0;
+    return static_cast<long long>(static_cast<unsigned long long>(static_cast<uint32_t>(p)) * static_cast<uint32_t>(p));
+}
+template <int L, int G>
+TB_HD TB_FI void search_multi32(const DevModel& M, const int32_t* t, const int32_t* depth, int node, MultiBest<G>& b) {
+    const int info = M.boxes[node].info;
+    const int first = info >> 5, cnt = info & 31;
+    for (int k = 0; k < cnt; ++k) {
+        const RBox ch = M.boxes[first + k];
+        const long long a = box_dist32_no_depth(ch, t);
+        bool enter = false;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const long long d = a + depth_term32(ch, depth[g]);
+            const bool better = d < b.d[g] || (d == b.d[g] && ch.rank < b.rank[g]);
+            if (ch.info < 0) {
+                if (better) {
+                    b.d[g] = d;
+                    b.rank[g] = ch.rank;
+                    b.leaf[g] = ~ch.info;
+                }
+            } else {
+                enter = enter || better;
+            }
+        }
+        if constexpr (L > 1) {
+            if (ch.info >= 0 && enter) search_multi32<L - 1, G>(M, t, depth, first + k, b);
+        }
+    }
+}
+// Starts every target from start_leaf (the previous result), as tree_first_min32 does.
+template <int G>
+TB_HD inline void tree_first_min32_multi(const DevModel& M, const int32_t* t, const int32_t* depth, int start_leaf, MultiBest<G>& b) {
+    const RBox& s0 = M.boxes[M.box_leaf[start_leaf]];
+    const long long a = box_dist32_no_depth(s0, t);
+    const int r0 = M.leaf_rank[start_leaf];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+        b.d[g] = a + depth_term32(s0, depth[g]);
+        b.rank[g] = r0;
+        b.leaf[g] = start_leaf;
+    }
+    search_multi32<kRecDepth - 1, G>(M, t, depth, 0, b);
+}
+
 // Whether a leaf other than `leaf` reaches distance m (the minimum) from target t: then the
 // chain's previous result may be kept over the first minimal leaf. Boxes farther than m
 // are pruned.
@@ -519,6 +593,12 @@ TB_HD TB_NOINLINE inline QuartLeaf quart_leaf(const DevModel& M, const DevSeed& 
 #define TB_QUART_RUN 16
 #endif
 constexpr int kRun = TB_QUART_RUN;
+// quarts of a run searched together (one descent of the tree for the group)
+#ifndef TB_QUART_GROUP
+#define TB_QUART_GROUP 4
+#endif
+constexpr int kQuartGroup = TB_QUART_GROUP;
+static_assert(kRun % kQuartGroup == 0, "quart group must divide the run");
 constexpr int kRuns = (tbm::kHeight / 4) / kRun;
 static_assert((tbm::kHeight / 4) % kRun == 0, "quart run must divide the quart height");
 TB_HD inline void body_climate_quart(const Batch& B, int it) {
@@ -532,27 +612,53 @@ TB_HD inline void body_climate_quart(const Batch& B, int it) {
     const int x = bx * 16 + 4 * qx, z = bz * 16 + 4 * qz;
     const float* colv = B.bcol + static_cast<size_t>(cidx) * tbm::kClimateCols;
     int prev = 0;
-    for (int r = 0; r < kRun; ++r) {
-        const int qy = run * kRun + r;
-        float cl[6];
-        tbgen::gen_climate(S.nt, x, tbm::kMinY + 4 * qy, z, colv, cl);
-        long long t[6];
-        for (int k = 0; k < 6; ++k) t[k] = f2l(cl[k] * 10000.0f);
-        long long md;
-        bool small = B.M.boxes != nullptr;
-        int32_t t32[6];
-        for (int k = 0; k < 6; ++k) {
-            small = small && t[k] >= -kBox32Limit && t[k] <= kBox32Limit;
-            t32[k] = static_cast<int32_t>(t[k]);
+    for (int r0 = 0; r0 < kRun; r0 += kQuartGroup) {
+        // The group's targets go out as they are computed; the shared search needs 32-bit
+        // targets that agree outside depth.
+        bool shared = B.M.boxes != nullptr && TB_SEARCH_LEVELS && B.M.depth <= kRecDepth;
+        int32_t t32[6], depth[kQuartGroup];
+        for (int g = 0; g < kQuartGroup; ++g) {
+            float cl[6];
+            tbgen::gen_climate(S.nt, x, tbm::kMinY + 4 * (run * kRun + r0 + g), z, colv, cl);
+            long long* tg = B.tgt + (static_cast<size_t>(b) * kQuartsPerChunk + chain_pos(qx, run * kRun + r0 + g, qz)) * 6;
+            for (int k = 0; k < 6; ++k) {
+                const long long v = f2l(cl[k] * 10000.0f);
+                tg[k] = v;
+                shared = shared && v >= -kBox32Limit && v <= kBox32Limit;
+                if (g == 0) t32[k] = static_cast<int32_t>(v);
+                else if (k != 4) shared = shared && static_cast<int32_t>(v) == t32[k];
+                if (k == 4) depth[g] = static_cast<int32_t>(v);
+            }
         }
-        const int leaf = !small                                     ? tree_first_min(B.M, t, prev, md)
-                         : (TB_SEARCH_LEVELS && B.M.depth <= kRecDepth) ? tree_first_min32_levels(B.M, t32, prev, md)
-                                                                        : tree_first_min32(B.M, t32, prev, md);
-        prev = leaf;
-        const size_t p = static_cast<size_t>(b) * kQuartsPerChunk + chain_pos(qx, qy, qz);
-        for (int k = 0; k < 6; ++k) B.tgt[p * 6 + k] = t[k];
-        B.lstar[p] = leaf;
-        B.mdist[p] = md;
+        if (shared) {
+            MultiBest<kQuartGroup> mb;
+            tree_first_min32_multi<kQuartGroup>(B.M, t32, depth, prev, mb);
+            // each quart's least (distance, rank) is the same whichever leaf its search starts from
+            for (int g = 0; g < kQuartGroup; ++g) {
+                const size_t p = static_cast<size_t>(b) * kQuartsPerChunk + chain_pos(qx, run * kRun + r0 + g, qz);
+                B.lstar[p] = mb.leaf[g];
+                B.mdist[p] = mb.d[g];
+            }
+            prev = mb.leaf[kQuartGroup - 1];
+        } else {
+            for (int g = 0; g < kQuartGroup; ++g) {
+                const size_t p = static_cast<size_t>(b) * kQuartsPerChunk + chain_pos(qx, run * kRun + r0 + g, qz);
+                const long long* t = B.tgt + p * 6;
+                bool small = B.M.boxes != nullptr;
+                int32_t u32[6];
+                for (int k = 0; k < 6; ++k) {
+                    small = small && t[k] >= -kBox32Limit && t[k] <= kBox32Limit;
+                    u32[k] = static_cast<int32_t>(t[k]);
+                }
+                long long md;
+                const int leaf = !small                                     ? tree_first_min(B.M, t, prev, md)
+                                 : (TB_SEARCH_LEVELS && B.M.depth <= kRecDepth) ? tree_first_min32_levels(B.M, u32, prev, md)
+                                                                                : tree_first_min32(B.M, u32, prev, md);
+                B.lstar[p] = leaf;
+                B.mdist[p] = md;
+                prev = leaf;
+            }
+        }
     }
 }
 
