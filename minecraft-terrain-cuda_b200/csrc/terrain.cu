@@ -473,6 +473,13 @@ struct Generator {
 #define TB_TAIL_MIN 512
 #endif
     static constexpr int kTailMin = TB_TAIL_MIN;   // smallest batch the tail split of generate() makes (0: no split)
+#ifndef TB_HOST_BATCH
+#define TB_HOST_BATCH 2048
+#endif
+    // Batches of generate() (outputs to host memory) hold at most this many chunks: once the
+    // kernels outrun the device-to-host link, smaller batches start the copies sooner while
+    // still keeping the GPU busy.
+    static constexpr int kHostBatch = TB_HOST_BATCH;
 #ifndef TB_ORDERED_BATCH
 #define TB_ORDERED_BATCH 2048
 #endif
@@ -864,12 +871,12 @@ struct Generator {
         order_lanes();
         check_chunks(chunks, count);
         std::vector<int32_t> cx(max_batch), cz(max_batch), cs(max_batch, current_slot);
+        const int hb = kHostBatch > 0 ? std::min(max_batch, kHostBatch) : max_batch;
         for (int off = 0; off < count;) {
             // The copy of the last batch is the one no compute hides: within the last two
             // batches' worth, halve the batches (down to kTailMin chunks) so that it is short.
             const int rem = count - off;
-            const int n = (kTailMin == 0 || rem > 2 * max_batch) ? std::min(max_batch, rem)
-                                                                   : std::min(max_batch, std::max((rem + 1) / 2, std::min(rem, kTailMin)));
+            const int n = (kTailMin == 0 || rem > 2 * hb) ? std::min(hb, rem) : std::min(hb, std::max((rem + 1) / 2, std::min(rem, kTailMin)));
             for (int i = 0; i < n; ++i) {
                 cx[i] = chunks[off + i].x;
                 cz[i] = chunks[off + i].z;
