@@ -1404,37 +1404,44 @@ TB_HD TB_FI float prelim_surface(const Batch& B, int c, int lx, int lz) {
     return a0 + step * 0.0f;
 }
 
-// The 8 channel values of one block: the cell's a0 plus the step added once per block
-// above the cell floor, as in the fill. Out of line, returned in registers.
-struct ChannelValues {
-    float v[tbm::kNumChannels];
-};
-TB_HD TB_NOINLINE inline ChannelValues block_channels(const Batch& B, int c, int lx, int lz, int y) {
-    CellInterp ci;
+// Channel k of one block: cell_interp's arithmetic for that channel, then the step added
+// once per block above the cell floor, as in the fill. Out of line.
+TB_HD TB_NOINLINE inline float block_channel(const Batch& B, int c, int lx, int lz, int y, int k) {
     const int cell_y = (y - tbm::kMinY) >> 3, yi = (y - tbm::kMinY) & 7;
-    cell_interp(B, c, lx, lz, cell_y, ci);
-    ChannelValues out;
-    for (int j = 0; j < tbm::kNumChannels; ++j) {
-        float v = ci.a0[j];
-        for (int q = 0; q < yi; ++q) v += ci.step[j];
-        out.v[j] = v;
-    }
-    return out;
+    const int ci = lx >> 2, xi = lx & 3, ck = lz >> 2, zi = lz & 3;
+    const int32_t* cc = B.c25 + static_cast<size_t>(c) * 25;
+    const size_t u00 = cc[ck * 5 + ci], u10 = cc[ck * 5 + ci + 1], u01 = cc[(ck + 1) * 5 + ci], u11 = cc[(ck + 1) * 5 + ci + 1];
+    const int C = tbm::kNumChannels;
+    const float* p00 = B.corners + (u00 * kRows + cell_y) * C;
+    const float* p10 = B.corners + (u10 * kRows + cell_y) * C;
+    const float* p01 = B.corners + (u01 * kRows + cell_y) * C;
+    const float* p11 = B.corners + (u11 * kRows + cell_y) * C;
+    const float az = static_cast<float>(zi) * 0.25f, ax = static_cast<float>(xi) * 0.25f;
+    const float v000 = p00[k], v100 = p10[k], v001 = p01[k], v101 = p11[k];
+    const float v010 = p00[C + k], v110 = p10[C + k], v011 = p01[C + k], v111 = p11[C + k];
+    const float v00 = lerpf(az, v000, v001), v01 = lerpf(az, v010, v011);
+    const float v10 = lerpf(az, v100, v101), v11 = lerpf(az, v110, v111);
+    const float a0 = lerpf(ax, v00, v10), a1 = lerpf(ax, v01, v11);
+    const float step = (a1 - a0) * 0.125f;
+    float v = a0 + step * 0.0f;
+    for (int q = 0; q < yi; ++q) v += step;
+    return v;
 }
 
-// Channel values of one block on first use: the generated ore functions read a channel
-// only under the guards that need it (a vein's y range, for one).
+// Channel values of one block, each interpolated on its first use: the generated ore
+// functions read a channel only under the guards that need it (a vein's y range, for one),
+// and a vein reads few of them (its density one, its richness two more).
 struct LazyChannels {
     const Batch* B;
     int c, lx, lz, y;
-    mutable bool set;
-    mutable ChannelValues cv;
+    mutable uint32_t set;
+    mutable float v[tbm::kNumChannels];
     TB_HD TB_FI float operator[](int k) const {
-        if (!set) {
-            cv = block_channels(*B, c, lx, lz, y);
-            set = true;
+        if (!((set >> k) & 1u)) {
+            v[k] = block_channel(*B, c, lx, lz, y, k);
+            set |= 1u << k;
         }
-        return cv.v[k];
+        return v[k];
     }
 };
 
@@ -1446,7 +1453,7 @@ TB_HD TB_NOINLINE inline int ore_vein_hit(const Batch& B, int c, int lx, int lz,
     const NoiseTables& T = S.nt;
     Xoro r = S.ore.at(bx, y, bz);
     if (r.next_float() > density) return -1;
-    const LazyChannels ch{&B, c, lx, lz, y, false, {}};
+    const LazyChannels ch{&B, c, lx, lz, y, 0u, {}};
     const float richness = tbgen::gen_ore_richness(k, T, bx, y, bz, ch);
     if (r.next_float() < richness && tbgen::gen_ore_gap(k, T, bx, y, bz) < 0.0f) return r.next_float() < chance ? raw : ore;
     return filler;
@@ -1507,7 +1514,7 @@ struct RuleCtx {
     // out of line
     TB_HD TB_FI int ore_vein(int k, int ore, int raw, int filler, float chance) const {
         if (TB_ORE_MASK && !((ore_bits >> k) & 1)) return -1;
-        const LazyChannels ch{B, c, col->lx, col->lz, y, false, {}};
+        const LazyChannels ch{B, c, col->lx, col->lz, y, 0u, {}};
         const float density = tbgen::gen_ore_density(k, col->S->nt, col->bx, y, col->bz, ch);
         if (density <= 0.0f) return -1;
         return ore_vein_hit(*B, c, col->lx, col->lz, col->bx, y, col->bz, *col->S, k, ore, raw, filler, chance, density);
