@@ -1217,54 +1217,69 @@ TB_HD inline void body_zoom_uniform(const Batch& B, int it) {
     B.zoom_uni[it] = uni ? static_cast<uint8_t>(b0) : kZoomMixed;
 }
 
-// item = (chunk * kZoomGroups + group) * 256 + z * 16 + x; blocks up to the column height
+// item = chunk * 256 + z * 16 + x: the zoomed biome of every block of the column up to its
+// height, written 4 heights to a word (column order). Blocks of a uniform zoom cell take its
+// biome; the others pick the nearest fiddled corner in FP64, the 8 candidates' x and z terms
+// once per group of 4 heights.
 TB_HD inline void body_block_biome(const Batch& B, int it) {
-    const int col = it & 255, g = (it >> 8) % kZoomGroups, c = (it >> 8) / kZoomGroups;
-    const int lx = col & 15, lz = col >> 4;
-    const int py = kZoomPyMin + g;
-    const int top = B.h1[(static_cast<size_t>(c) << 8) | (lx << 4) | lz];
-    const int ylo = 4 * py + 2 < tbm::kMinY ? tbm::kMinY : 4 * py + 2;
-    int yhi = 4 * py + 5 > kMaxY ? kMaxY : 4 * py + 5;
-    if (yhi > top) yhi = top;
-    if (ylo > yhi) return;
+    const int c = it >> 8, col = it & 255, lx = col & 15, lz = col >> 4;
+    const int h = B.h1[(static_cast<size_t>(c) << 8) | (lx << 4) | lz];
+    const int top = h > kMaxY ? kMaxY : h;
+    if (top < tbm::kMinY) return;
     const int x = B.cx[c] * 16 + lx, z = B.cz[c] * 16 + lz;
     const int ax = x - 2, az = z - 2, px = ax >> 2, pz = az >> 2;
     const int qx0 = B.cx[c] * 4 - 1, qz0 = B.cz[c] * 4 - 1;
-    const uint8_t uni = B.zoom_uni[static_cast<size_t>(c) * kZoomCells + (g * 5 + pz - qz0) * 5 + px - qx0];
-    if (uni != kZoomMixed) {
-        for (int y = ylo; y <= yhi; ++y) B.bbiome[colbyte(c, col, y)] = uni;
-        return;
-    }
-    const double fx = static_cast<double>(ax & 3) / 4.0, fz = static_cast<double>(az & 3) / 4.0;
+    const uint8_t* uni_of = B.zoom_uni + static_cast<size_t>(c) * kZoomCells + (pz - qz0) * 5 + px - qx0;
     const uint32_t* tab = B.zoom_tab + static_cast<size_t>(c) * kZoomVerts;
+    uint32_t* words = reinterpret_cast<uint32_t*>(B.bbiome) + static_cast<size_t>(c) * kColWords * 256 + col;
     double sx[8], sz[8], oy[8];
+    int g_cur = -1;
+    uint8_t uni = 0;
+    uint32_t word = 0;
+    for (int y = tbm::kMinY; y <= top; ++y) {
+        const int py = (y - 2) >> 2, g = py - kZoomPyMin;
+        if (g != g_cur) {
+            g_cur = g;
+            uni = uni_of[g * 25];
+            if (uni == kZoomMixed) {
+                const double fx = static_cast<double>(ax & 3) / 4.0, fz = static_cast<double>(az & 3) / 4.0;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const bool xe = (i & 4) == 0, ye = (i & 2) == 0, ze = (i & 1) == 0;
-        const int qx = xe ? px : px + 1, qy = ye ? py : py + 1, qz = ze ? pz : pz + 1;
-        const uint32_t m = tab[((qy - kZoomQyMin) * 6 + (qz - qz0)) * 6 + (qx - qx0)];
-        const double ox = zoom_fiddle(static_cast<int32_t>(m & 1023u));
-        oy[i] = zoom_fiddle(static_cast<int32_t>((m >> 10) & 1023u));
-        const double oz = zoom_fiddle(static_cast<int32_t>(m >> 20));
-        const double dx = xe ? fx : fx - 1.0, dz = ze ? fz : fz - 1.0;
-        sz[i] = (dz + oz) * (dz + oz);
-        sx[i] = (dx + ox) * (dx + ox);
-    }
-    for (int y = ylo; y <= yhi; ++y) {
-        const double fy = static_cast<double>((y - 2) & 3) / 4.0;
-        int best = 0;
-        double best_d = 0.0;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const double dy = (i & 2) == 0 ? fy : fy - 1.0;
-            const double sy = (dy + oy[i]) * (dy + oy[i]);
-            const double d = sz[i] + sy + sx[i];
-            if (i == 0 || best_d > d) {
-                best = i;
-                best_d = d;
+                for (int i = 0; i < 8; ++i) {
+                    const bool xe = (i & 4) == 0, ye = (i & 2) == 0, ze = (i & 1) == 0;
+                    const int qx = xe ? px : px + 1, qy = ye ? py : py + 1, qz = ze ? pz : pz + 1;
+                    const uint32_t m = tab[((qy - kZoomQyMin) * 6 + (qz - qz0)) * 6 + (qx - qx0)];
+                    const double ox = zoom_fiddle(static_cast<int32_t>(m & 1023u));
+                    oy[i] = zoom_fiddle(static_cast<int32_t>((m >> 10) & 1023u));
+                    const double oz = zoom_fiddle(static_cast<int32_t>(m >> 20));
+                    const double dx = xe ? fx : fx - 1.0, dz = ze ? fz : fz - 1.0;
+                    sz[i] = (dz + oz) * (dz + oz);
+                    sx[i] = (dx + ox) * (dx + ox);
+                }
             }
         }
-        B.bbiome[colbyte(c, col, y)] = static_cast<uint8_t>(zoom_stored(B, c, best, px, py, pz));
+        uint32_t biome = uni;
+        if (uni == kZoomMixed) {
+            const double fy = static_cast<double>((y - 2) & 3) / 4.0;
+            int best = 0;
+            double best_d = 0.0;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const double dy = (i & 2) == 0 ? fy : fy - 1.0;
+                const double sy = (dy + oy[i]) * (dy + oy[i]);
+                const double d = sz[i] + sy + sx[i];
+                if (i == 0 || best_d > d) {
+                    best = i;
+                    best_d = d;
+                }
+            }
+            biome = static_cast<uint32_t>(zoom_stored(B, c, best, px, py, pz));
+        }
+        const int r = y - tbm::kMinY;
+        word |= biome << (8 * (r & 3));
+        if ((r & 3) == 3 || y == top) {
+            words[(r >> 2) * 256] = word;
+            word = 0;
+        }
     }
 }
 

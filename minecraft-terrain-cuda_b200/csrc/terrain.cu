@@ -737,7 +737,7 @@ struct Generator {
                "d2d");
         mark(4);
         launch(k_items<body_surface1, 256>, s, 256 * nmax, B);
-        launch(k_items<body_block_biome, 256 * kZoomGroups>, s, 256L * kZoomGroups * nmax, B);
+        launch(k_items<body_block_biome, 256>, s, 256L * nmax, B);
         mark(6);
         launch(k_items<body_surface_walk_rules, 256, TB_MINB_WALK>, s, 256 * nmax, B);
         mark(7);

@@ -166,7 +166,7 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     each(256 * kCellsY * n, [&](int i) { body_fill(B, i); });
     if (aquifer) std::memcpy(aquifer, bl.data(), sizeof(uint16_t) * bl.size());
     each(256 * n, [&](int i) { body_surface1(B, i); });
-    each(256 * kZoomGroups * n, [&](int i) { body_block_biome(B, i); });
+    each(256 * n, [&](int i) { body_block_biome(B, i); });
     each(256 * n, [&](int i) { body_surface_walk_rules(B, i); });
     each(256 * n, [&](int i) { body_surface_frozen(B, i); });
     each(kQuartsPerChunk * n, [&](int i) { body_gather(B, i); });
