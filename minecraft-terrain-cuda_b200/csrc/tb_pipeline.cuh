@@ -1580,8 +1580,20 @@ TB_HD inline void body_surface1(const Batch& B, int it) {
 // applying the rule tree to each solid block as the walk reaches it (the blocks below it,
 // which the walk still reads, are untouched; the rules never turn a block into air or a
 // fluid). A warp holds 32 columns of one chunk at the same y, as the per-block pass does.
+// The walk's item order: the 32 lanes of a warp hold a tile of TB_WALK_TILE columns in x by
+// 32 / TB_WALK_TILE in z (a compact tile has closer heights and rule paths than a strip).
+#ifndef TB_WALK_TILE
+#define TB_WALK_TILE 8
+#endif
+static_assert(TB_WALK_TILE == 4 || TB_WALK_TILE == 8 || TB_WALK_TILE == 16, "walk tile width");
+TB_HD TB_FI int walk_column(int it) {
+    constexpr int tw = TB_WALK_TILE, th = 32 / tw, across = 16 / tw;
+    const int w = (it >> 5) & 7, l = it & 31;
+    return (th * (w / across) + l / tw) * 16 + tw * (w % across) + l % tw;
+}
 TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
-    const int c = it >> 8, lz = (it >> 4) & 15, lx = it & 15;
+    const int wcol = walk_column(it);
+    const int c = it >> 8, lz = wcol >> 4, lx = wcol & 15;
     const int ci = (c << 8) | (lx << 4) | lz;   // x * 16 + z column index
     const size_t hb = static_cast<size_t>(c) * 256;
     Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
@@ -1616,7 +1628,7 @@ TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
     // The walk reads the column's air and fluid bits, which stay true while it runs (the rules
     // never make air or fluid). All lanes of a warp walk the same height: above its own
     // height a column holds air, which leaves the walk state as it starts.
-    const uint32_t* cm = B.colmask + static_cast<size_t>(c) * 2 * kMaskWords * 256 + (it & 255);
+    const uint32_t* cm = B.colmask + static_cast<size_t>(c) * 2 * kMaskWords * 256 + wcol;
     const int height = C.hm;
 #if defined(__CUDA_ARCH__)
     const int start = warp_max(height > kMaxY ? kMaxY : height);
@@ -1624,14 +1636,15 @@ TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
     // the host build takes the maximum over the same 32 items a device warp holds
     int start = INT_MIN;
     for (int j = it & ~31; j < (it & ~31) + 32; ++j) {
-        const int h = B.h1[(static_cast<size_t>(c) << 8) | ((j & 15) << 4) | ((j >> 4) & 15)];
+        const int jc = walk_column(j);
+        const int h = B.h1[(static_cast<size_t>(c) << 8) | ((jc & 15) << 4) | (jc >> 4)];
         start = imax(start, h > kMaxY ? kMaxY : h);
     }
 #endif
     // Zoomed biomes and ore bits, 4 heights per word: the walk descends one height at a time,
     // so the word below is loaded while the current one is in use.
-    const uint32_t* bwords = reinterpret_cast<const uint32_t*>(B.bbiome) + static_cast<size_t>(c) * kColWords * 256 + (it & 255);
-    const uint32_t* owords = reinterpret_cast<const uint32_t*>(B.oremask) + static_cast<size_t>(c) * kColWords * 256 + (it & 255);
+    const uint32_t* bwords = reinterpret_cast<const uint32_t*>(B.bbiome) + static_cast<size_t>(c) * kColWords * 256 + wcol;
+    const uint32_t* owords = reinterpret_cast<const uint32_t*>(B.oremask) + static_cast<size_t>(c) * kColWords * 256 + wcol;
     int wq = (start - tbm::kMinY) >> 2;
     uint32_t bq = bwords[wq * 256], oq = TB_ORE_MASK ? owords[wq * 256] : 0u;
     uint32_t bq_next = 0, oq_next = 0;
