@@ -84,12 +84,16 @@ struct DevSeed {
 
 // Open-addressing table deduplicating 64-bit position keys; unique keys get dense
 // indices in insertion order of the winning thread.
+// Open-addressing key set of one dedupe stage. Inserting records, per slot, the least item
+// that inserted the key; compaction then numbers the keys in the order of those first items
+// (uniq), so neighbouring entries of uniq come from neighbouring items (nearby chunks).
 struct HashTab {
     unsigned long long* keys;   // kEmpty when free
     int32_t* vals;
     unsigned long long* uniq;
     int32_t* count;
     uint32_t mask;
+    int32_t* owner;             // per slot: least inserting item (INT32_MAX-like when free)
 };
 constexpr unsigned long long kEmpty = ~0ull;
 
@@ -197,6 +201,13 @@ TB_HD TB_FI int warp_max(int v) {
     return v;
 #endif
 }
+TB_HD TB_FI void min32(int32_t* p, int32_t v) {
+#if defined(__CUDA_ARCH__)
+    atomicMin(p, v);
+#else
+    if (v < *p) *p = v;
+#endif
+}
 TB_HD TB_FI void max32(int32_t* p, int32_t v) {
 #if defined(__CUDA_ARCH__)
     atomicMax(p, v);
@@ -213,19 +224,38 @@ TB_HD TB_FI uint32_t hash_slot(unsigned long long k, uint32_t mask) {
     return static_cast<uint32_t>(h) & mask;
 }
 
-TB_HD inline void ht_insert(const HashTab& t, unsigned long long key) {
+TB_HD inline void ht_insert(const HashTab& t, unsigned long long key, int32_t item) {
     uint32_t s = hash_slot(key, t.mask);
     for (uint32_t probe = 0; probe <= t.mask; ++probe) {
         const unsigned long long prev = cas64(&t.keys[s], kEmpty, key);
-        if (prev == kEmpty) {
-            const int32_t idx = add32(t.count, 1);
-            t.vals[s] = idx;
-            t.uniq[idx] = key;
+        if (prev == kEmpty || prev == key) {
+            min32(&t.owner[s], item);
             return;
         }
-        if (prev == key) return;
         s = (s + 1) & t.mask;
     }
+}
+
+// The slot holding key (inserted), or the table size when absent.
+TB_HD inline uint32_t ht_slot(const HashTab& t, unsigned long long key) {
+    uint32_t s = hash_slot(key, t.mask);
+    for (uint32_t probe = 0; probe <= t.mask; ++probe) {
+        const unsigned long long k = t.keys[s];
+        if (k == key) return s;
+        if (k == kEmpty) break;
+        s = (s + 1) & t.mask;
+    }
+    return t.mask + 1;
+}
+
+// Compaction, one item at a time in item order (the host build): the key's first item
+// gives it the next index.
+TB_HD inline void ht_number(const HashTab& t, unsigned long long key, int32_t item) {
+    const uint32_t s = ht_slot(t, key);
+    if (s > t.mask || t.owner[s] != item) return;
+    const int32_t idx = add32(t.count, 1);
+    t.vals[s] = idx;
+    t.uniq[idx] = key;
 }
 
 TB_HD inline int32_t ht_find(const HashTab& t, unsigned long long key) {
@@ -253,24 +283,22 @@ TB_HD TB_FI void unpack_key(unsigned long long k, int32_t& slot, int32_t& a, int
 }
 
 // ---- dedupe stages ----------------------------------------------------------------------------
+// Each stage inserts its keys, numbers them (ht_number on the host, k_number on the device),
+// then resolves every item to its key's index.
 // biome chunks (item = chunk * 9 + neighbour)
-TB_HD inline void body_nb_insert(const Batch& B, int i) {
+TB_HD TB_FI unsigned long long nb_key(const Batch& B, int i) {
     const int c = i / 9, k = i % 9;
-    ht_insert(B.hb, pack_key(B.cseed[c], B.cx[c] + k % 3 - 1, B.cz[c] + k / 3 - 1, 0));
+    return pack_key(B.cseed[c], B.cx[c] + k % 3 - 1, B.cz[c] + k / 3 - 1, 0);
 }
-TB_HD inline void body_nb_resolve(const Batch& B, int i) {
-    const int c = i / 9, k = i % 9;
-    B.nb9[i] = ht_find(B.hb, pack_key(B.cseed[c], B.cx[c] + k % 3 - 1, B.cz[c] + k / 3 - 1, 0));
-}
+TB_HD inline void body_nb_insert(const Batch& B, int i) { ht_insert(B.hb, nb_key(B, i), i); }
+TB_HD inline void body_nb_resolve(const Batch& B, int i) { B.nb9[i] = ht_find(B.hb, nb_key(B, i)); }
 // corner columns in quart units (item = chunk * 25 + k * 5 + i)
-TB_HD inline void body_cc_insert(const Batch& B, int it) {
+TB_HD TB_FI unsigned long long cc_key(const Batch& B, int it) {
     const int c = it / 25, k = (it % 25) / 5, i = it % 5;
-    ht_insert(B.hc, pack_key(B.cseed[c], B.cx[c] * 4 + i, B.cz[c] * 4 + k, 0));
+    return pack_key(B.cseed[c], B.cx[c] * 4 + i, B.cz[c] * 4 + k, 0);
 }
-TB_HD inline void body_cc_resolve(const Batch& B, int it) {
-    const int c = it / 25, k = (it % 25) / 5, i = it % 5;
-    B.c25[it] = ht_find(B.hc, pack_key(B.cseed[c], B.cx[c] * 4 + i, B.cz[c] * 4 + k, 0));
-}
+TB_HD inline void body_cc_insert(const Batch& B, int it) { ht_insert(B.hc, cc_key(B, it), it); }
+TB_HD inline void body_cc_resolve(const Batch& B, int it) { B.c25[it] = ht_find(B.hc, cc_key(B, it)); }
 // surface-level quarts: 27 x 19 per chunk; the 11 x 11 window of the aquifer's
 // constructor uses volume semantics (sem 1), the rest the lazy point path (sem 0).
 TB_HD TB_FI unsigned long long sg_key(const Batch& B, int c, int g) {
@@ -279,7 +307,8 @@ TB_HD TB_FI unsigned long long sg_key(const Batch& B, int c, int g) {
     const bool win = qx >= B.cx[c] * 4 - 4 && qx <= B.cx[c] * 4 + 6 && qz >= B.cz[c] * 4 - 4 && qz <= B.cz[c] * 4 + 6;
     return pack_key(B.cseed[c], qx, qz, win ? 1 : 0);
 }
-TB_HD inline void body_sg_insert(const Batch& B, int it) { ht_insert(B.hs, sg_key(B, it / kGrid, it % kGrid)); }
+TB_HD TB_FI unsigned long long sg_key_item(const Batch& B, int it) { return sg_key(B, it / kGrid, it % kGrid); }
+TB_HD inline void body_sg_insert(const Batch& B, int it) { ht_insert(B.hs, sg_key_item(B, it), it); }
 TB_HD inline void body_sg_resolve(const Batch& B, int it) { B.g513[it] = ht_find(B.hs, sg_key(B, it / kGrid, it % kGrid)); }
 
 // ---- biomes -------------------------------------------------------------------------------------

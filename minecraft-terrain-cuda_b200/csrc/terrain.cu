@@ -92,6 +92,54 @@ __global__ void __launch_bounds__(256, MINB) k_dyn(const __grid_constant__ Batch
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) F(B, i);
 }
 
+// Numbers the keys of one dedupe stage (TAB 0 biome chunks, 1 corner columns, 2 surface
+// quarts): within each tile of 256 items, the items that are their key's first insert
+// (ht_insert keeps the least item per key) take consecutive indices from one atomicAdd, so
+// neighbouring entries of uniq come from neighbouring items. The host build numbers in plain
+// item order (ht_number).
+template <int TAB>
+__device__ __forceinline__ const HashTab& dedupe_table(const Batch& B) {
+    return TAB == 0 ? B.hb : (TAB == 1 ? B.hc : B.hs);
+}
+template <int TAB, unsigned long long (*K)(const Batch&, int), int MUL>
+__global__ void __launch_bounds__(256) k_number(const __grid_constant__ Batch B) {
+    const HashTab& t = dedupe_table<TAB>(B);
+    const int n = *B.n_dev * MUL;
+    __shared__ int32_t warp_off[8];
+    __shared__ int32_t tile_base;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int tile = blockIdx.x * 256; tile < n; tile += gridDim.x * 256) {
+        const int it = tile + static_cast<int>(threadIdx.x);
+        bool first = false;
+        unsigned long long key = 0;
+        uint32_t slot = 0;
+        if (it < n) {
+            key = K(B, it);
+            slot = ht_slot(t, key);
+            first = slot <= t.mask && t.owner[slot] == it;
+        }
+        const unsigned ball = __ballot_sync(0xFFFFFFFFu, first);
+        if (lane == 0) warp_off[wid] = __popc(ball);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int32_t sum = 0;
+            for (int w = 0; w < 8; ++w) {
+                const int32_t v = warp_off[w];
+                warp_off[w] = sum;
+                sum += v;
+            }
+            tile_base = sum ? atomicAdd(t.count, sum) : 0;
+        }
+        __syncthreads();
+        if (first) {
+            const int32_t idx = tile_base + warp_off[wid] + __popc(ball & ((1u << lane) - 1u));
+            t.vals[slot] = idx;
+            t.uniq[idx] = key;
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void k_init_heights(const __grid_constant__ Batch B) {
     const int n = *B.n_dev * 256;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) B.h0[i] = tbm::kMinY;
@@ -385,18 +433,23 @@ struct PinBuf {
 };
 
 struct TableBufs {
-    DevBuf keys, vals, uniq, count;
+    DevBuf keys, vals, uniq, count, owner;
     uint32_t cap = 0;
     void alloc(uint64_t max_keys) {
         cap = pow2_at_least(2 * max_keys);
         keys.alloc(sizeof(unsigned long long) * cap);
         vals.alloc(sizeof(int32_t) * cap);
+        owner.alloc(sizeof(int32_t) * cap);
         uniq.alloc(sizeof(unsigned long long) * max_keys);
         count.alloc(sizeof(int32_t));
     }
-    HashTab view() const { return HashTab{keys.as<unsigned long long>(), vals.as<int32_t>(), uniq.as<unsigned long long>(), count.as<int32_t>(), cap - 1}; }
+    HashTab view() const {
+        return HashTab{keys.as<unsigned long long>(), vals.as<int32_t>(), uniq.as<unsigned long long>(), count.as<int32_t>(), cap - 1, owner.as<int32_t>()};
+    }
+    // free slots; owners above every item index (0x7F7F7F7F)
     void reset(cudaStream_t s) const {
         ck(cudaMemsetAsync(keys.p, 0xFF, keys.bytes, s), "memset");
+        ck(cudaMemsetAsync(owner.p, 0x7F, owner.bytes, s), "memset");
         ck(cudaMemsetAsync(count.p, 0, sizeof(int32_t), s), "memset");
     }
 };
@@ -694,6 +747,7 @@ struct Generator {
         const int32_t* cnt_b = W.tb_b.count.as<int32_t>();
         W.tb_b.reset(s);
         launch(k_items<body_nb_insert, 9>, s, 9 * nmax, B);
+        launch(k_number<0, nb_key, 9>, s, 9 * nmax, B);
         launch(k_items<body_nb_resolve, 9>, s, 9 * nmax, B);
         launch(k_dyn<body_climate_col, 16>, s, nmax * 16 * 2, B, cnt_b);
         launch(k_dyn<body_climate_quart, 16 * kRuns, TB_MINB_QUART>, s, nmax * 16 * kRuns * 2, B, cnt_b);
@@ -716,6 +770,7 @@ struct Generator {
         mark(1);
         W.tb_c.reset(s);
         launch(k_items<body_cc_insert, 25>, s, 25 * nmax, B);
+        launch(k_number<1, cc_key, 25>, s, 25 * nmax, B);
         launch(k_items<body_cc_resolve, 25>, s, 25 * nmax, B);
         launch(k_dyn<body_corner_col, 1>, s, 16 * nmax, B, cnt_c);
         launch(k_dyn<body_corner, kRows, TB_MINB_CORNER>, s, 16 * nmax * kRows, B, cnt_c);
@@ -724,6 +779,7 @@ struct Generator {
         mark(2);
         W.tb_s.reset(s);
         launch(k_items<body_sg_insert, kGrid>, s, kGrid * nmax, B);
+        launch(k_number<2, sg_key_item, kGrid>, s, kGrid * nmax, B);
         launch(k_items<body_sg_resolve, kGrid>, s, kGrid * nmax, B);
         launch(k_dyn<body_surface_level, 1>, s, 2 * nmax * 100, B, cnt_s);
         launch(k_items<body_aquifer_cell, kAqCells>, s, kAqCells * nmax, B);

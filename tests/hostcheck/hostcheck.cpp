@@ -62,7 +62,7 @@ struct HostRun {
 
 struct Table {
     std::vector<unsigned long long> keys, uniq;
-    std::vector<int32_t> vals;
+    std::vector<int32_t> vals, owner;
     int32_t count = 0;
     uint32_t cap = 0;
     void init(size_t max_keys) {
@@ -70,10 +70,11 @@ struct Table {
         while (cap < 2 * max_keys) cap <<= 1;
         keys.assign(cap, kEmpty);
         vals.assign(cap, -1);
+        owner.assign(cap, 0x7F7F7F7F);
         uniq.assign(max_keys, 0);
         count = 0;
     }
-    HashTab view() { return HashTab{keys.data(), vals.data(), uniq.data(), &count, cap - 1}; }
+    HashTab view() { return HashTab{keys.data(), vals.data(), uniq.data(), &count, cap - 1, owner.data()}; }
 };
 
 template <class F>
@@ -147,17 +148,20 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     B.colmask = colmask.data();
     B.colrec = colrec.data();
     each(9 * n, [&](int i) { body_nb_insert(B, i); });
+    each(9 * n, [&](int i) { ht_number(B.hb, nb_key(B, i), i); });
     each(9 * n, [&](int i) { body_nb_resolve(B, i); });
     each(hb.count * 16, [&](int i) { body_climate_col(B, i); });
     each(hb.count * 16 * kRuns, [&](int i) { body_climate_quart(B, i); });
     each(hb.count, [&](int i) { body_chain(B, i); });
     each(25 * n, [&](int i) { body_cc_insert(B, i); });
+    each(25 * n, [&](int i) { ht_number(B.hc, cc_key(B, i), i); });
     each(25 * n, [&](int i) { body_cc_resolve(B, i); });
     each(hc.count, [&](int i) { body_corner_col(B, i); });
     each(hc.count * kRows, [&](int i) { body_corner(B, i); });
     each(kZoomVerts * n, [&](int i) { body_zoom_table(B, i); });
     each(kZoomCells * n, [&](int i) { body_zoom_uniform(B, i); });
     each(kGrid * n, [&](int i) { body_sg_insert(B, i); });
+    each(kGrid * n, [&](int i) { ht_number(B.hs, sg_key_item(B, i), i); });
     each(kGrid * n, [&](int i) { body_sg_resolve(B, i); });
     each(hs.count, [&](int i) { body_surface_level(B, i); });
     each(kAqCells * n, [&](int i) { body_aquifer_cell(B, i); });
