@@ -1049,9 +1049,22 @@ TB_HD inline void cell_interp(const Batch& B, int c, int lx, int lz, int cell_y,
     }
 }
 
-// item = (chunk * kCellsY + cell_y) * 256 + z * 16 + x: the 8 blocks of one cell column
+// Column lz * 16 + lx of item `it` when each warp's 32 items cover a tile of TW columns in x by
+// 32 / TW in z (TW 16: two rows of 16, the plain order).
+template <int TW>
+TB_HD TB_FI int tile_column(int it) {
+    static_assert(TW == 4 || TW == 8 || TW == 16, "tile width");
+    constexpr int th = 32 / TW, across = 16 / TW;
+    const int w = (it >> 5) & 7, l = it & 31;
+    return (th * (w / across) + l / TW) * 16 + TW * (w % across) + l % TW;
+}
+#ifndef TB_FILL_TILE
+#define TB_FILL_TILE 16
+#endif
+
+// item = (chunk * kCellsY + cell_y) * 256 + tile_column: the 8 blocks of one cell column
 TB_HD inline void body_fill(const Batch& B, int it) {
-    const int col = it & 255, cell_y = (it >> 8) % kCellsY, c = (it >> 8) / kCellsY;
+    const int col = tile_column<TB_FILL_TILE>(it), cell_y = (it >> 8) % kCellsY, c = (it >> 8) / kCellsY;
     const int lx = col & 15, lz = col >> 4;
     const int bx = B.cx[c] * 16 + lx, bz = B.cz[c] * 16 + lz;
     const DevSeed& S = B.seeds[B.cseed[c]];
@@ -1614,12 +1627,7 @@ TB_HD inline void body_surface1(const Batch& B, int it) {
 #ifndef TB_WALK_TILE
 #define TB_WALK_TILE 8
 #endif
-static_assert(TB_WALK_TILE == 4 || TB_WALK_TILE == 8 || TB_WALK_TILE == 16, "walk tile width");
-TB_HD TB_FI int walk_column(int it) {
-    constexpr int tw = TB_WALK_TILE, th = 32 / tw, across = 16 / tw;
-    const int w = (it >> 5) & 7, l = it & 31;
-    return (th * (w / across) + l / tw) * 16 + tw * (w % across) + l % tw;
-}
+TB_HD TB_FI int walk_column(int it) { return tile_column<TB_WALK_TILE>(it); }
 TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
     const int wcol = walk_column(it);
     const int c = it >> 8, lz = wcol >> 4, lx = wcol & 15;
