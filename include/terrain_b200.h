@@ -78,7 +78,9 @@ tg_status tg_set_seed(struct tg_generator* gen, int64_t seed);
 /* The TERRAIN step for count chunks. blocks_out: count * 16 * 16 * height u16 (required);
  * biomes_out: count * 16 * height / 4 u8 (may be NULL); aquifer_out: the blocks after the
  * aquifer fill and before the material rules (may be NULL); timing may be NULL.
- * Host buffers; pinned ones (tg_alloc_pinned) copy fastest.
+ * Host buffers; pinned ones (tg_alloc_pinned) copy fastest. The chunks go in device
+ * batches of at most min(max_batch_chunks, 2048), each batch's copy to the host running
+ * while the next one computes.
  * reference: FullTerrainGenerator::generate (cuda/src/terrain.cu:1392-1417) */
 tg_status tg_generate(struct tg_generator* gen, const tg_chunk_xz* chunks, int32_t count, uint16_t* blocks_out, uint8_t* biomes_out,
                       uint16_t* aquifer_out, tg_timing* timing);
