@@ -46,6 +46,33 @@ def test_batch_larger_than_one_device_batch(ref_model):
         g.close()
 
 
+def test_host_batches_equal_whole_device_batches(ref_model):
+    """tg_generate cuts host-output work into batches of at most 2,048 chunks (then halving
+    tail batches, down to 512); on a generator of capacity 4,096 its result for 5,100 chunks
+    equals the device-resident form run on whole 4,096-chunk batches, and its last chunks
+    equal the reference."""
+    import torch
+    g = terrain_b200.TerrainGenerator(max_batch_chunks=4096)
+    try:
+        g.set_seed(777)
+        chunks = np.array([(x, z) for z in range(-30, 30) for x in range(-43, 42)], np.int32)[:5100]
+        b, q = g.generate(chunks)
+        dev_b = torch.empty((4096, g.height, 16, 16), dtype=torch.int16, device='cuda')
+        dev_q = torch.empty((4096, g.qper), dtype=torch.uint8, device='cuda')
+        for off in (0, 4096):
+            part = torch.from_numpy(np.ascontiguousarray(chunks[off:off + 4096])).cuda()
+            n = part.shape[0]
+            g.generate_device(part.data_ptr(), n, dev_b.data_ptr(), dev_q.data_ptr(), timing=False)
+            torch.cuda.synchronize()
+            assert (dev_b[:n].cpu().numpy().view(np.uint16) == b[off:off + n]).all(), off
+            assert (dev_q[:n].cpu().numpy() == q[off:off + n]).all(), off
+        tail = [tuple(int(v) for v in c) for c in chunks[-6:]]
+        rb, rq = ref_model.seed(777).generate(tail)
+        assert (b[-6:] == rb).all() and (q[-6:] == rq).all()
+    finally:
+        g.close()
+
+
 def test_server_alone_equals_mixed(ref_model):
     """Each served result is byte-identical alone and in a mix of concurrent requests."""
     g = terrain_b200.TerrainGenerator(max_batch_chunks=64)
