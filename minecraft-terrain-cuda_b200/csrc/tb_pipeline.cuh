@@ -462,6 +462,66 @@ TB_HD inline int tree_first_min32_levels(const DevModel& M, const int32_t* t, in
 #define TB_SEARCH_LEVELS 1
 #endif
 
+#if defined(__CUDA_ARCH__)
+// The first minimal leaf for one target t held by every lane, searched by the whole warp: lane
+// k tests child k of a node (a node has at most 31 children), the warp takes the least
+// (distance, rank) among the leaf children, then enters the other children in order while
+// they can still hold a better leaf. The same result as tree_first_min32; every lane ends
+// with it. All 32 lanes must take part (full mask).
+#ifndef TB_WARP_START
+#define TB_WARP_START 1
+#endif
+template <int L>
+__device__ __forceinline__ void warp_search32(const DevModel& M, const int32_t* t, int node, int lane, long long& best_d, int& best_rank, int& best_leaf) {
+    const unsigned full = 0xFFFFFFFFu;
+    const int info = M.boxes[node].info;
+    const int first = info >> 5, cnt = info & 31;
+    long long d = LLONG_MAX;
+    int rank = INT_MAX, cinfo = 0;
+    if (lane < cnt) {
+        const RBox ch = M.boxes[first + lane];
+        d = box_dist32(ch, t);
+        rank = ch.rank;
+        cinfo = ch.info;
+    }
+    // least (distance, rank, leaf) over the leaf children
+    long long ld = (lane < cnt && cinfo < 0) ? d : LLONG_MAX;
+    int lr = (lane < cnt && cinfo < 0) ? rank : INT_MAX, ll = (lane < cnt && cinfo < 0) ? ~cinfo : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const long long od = __shfl_xor_sync(full, ld, o);
+        const int orr = __shfl_xor_sync(full, lr, o), ol = __shfl_xor_sync(full, ll, o);
+        if (od < ld || (od == ld && orr < lr)) {
+            ld = od;
+            lr = orr;
+            ll = ol;
+        }
+    }
+    if (ld < best_d || (ld == best_d && lr < best_rank)) {
+        best_d = ld;
+        best_rank = lr;
+        best_leaf = ll;
+    }
+    if constexpr (L > 1) {
+        unsigned todo = __ballot_sync(full, lane < cnt && cinfo >= 0);
+        while (todo) {
+            const int k = __ffs(static_cast<int>(todo)) - 1;
+            todo &= todo - 1u;
+            const long long dk = __shfl_sync(full, d, k);
+            const int rk = __shfl_sync(full, rank, k);
+            if (dk < best_d || (dk == best_d && rk < best_rank)) warp_search32<L - 1>(M, t, first + k, lane, best_d, best_rank, best_leaf);
+        }
+    }
+}
+__device__ inline int warp_first_min32(const DevModel& M, const int32_t* t) {
+    const int lane = static_cast<int>(threadIdx.x & 31u);
+    long long best_d = LLONG_MAX;
+    int best_rank = INT_MAX, best_leaf = 0;
+    warp_search32<kRecDepth - 1>(M, t, 0, lane, best_d, best_rank, best_leaf);
+    return best_leaf;
+}
+#endif
+
 // The first minimal leaf for G targets that agree in every coordinate but depth (index 4),
 // in one descent of the tree: a box's terms of the other coordinates are summed once, each
 // target adds its own depth term and keeps its own best (distance, rank, leaf), and a box is
@@ -659,6 +719,20 @@ TB_HD inline void body_climate_quart(const Batch& B, int it) {
                 if (k == 4) depth[g] = static_cast<int32_t>(v);
             }
         }
+#if defined(__CUDA_ARCH__)
+        // A run's first group has no previous result; neighbouring columns (the warp's lanes)
+        // have close climates, so the warp searches lane 0's first target once and every
+        // lane starts from that leaf (the results do not depend on the starting leaf).
+        if (TB_WARP_START && r0 == 0 && B.M.boxes != nullptr && B.M.depth <= kRecDepth) {
+            const unsigned m = __activemask();
+            if (m == 0xFFFFFFFFu) {
+                int32_t tr[6];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) tr[k] = __shfl_sync(m, k == 4 ? depth[0] : t32[k], 0);
+                prev = warp_first_min32(B.M, tr);
+            }
+        }
+#endif
         if (shared) {
             MultiBest<kQuartGroup> mb;
             tree_first_min32_multi<kQuartGroup>(B.M, t32, depth, prev, mb);
