@@ -52,3 +52,25 @@ def test_extreme_seeds(gpu_gen, ref_model):
         blocks, biomes = gpu_gen.generate(chunks)
         rb, rq = ref_model.seed(seed).generate(chunks)
         compare(blocks, biomes, rb, rq, chunks)
+
+
+def test_random_seeds_scattered_and_far_chunks(ref_model):
+    """Random seeds, chunks scattered over +/-2M and across the whole accepted range (past
+    the BlockPos wrap of the aquifer locations), and a small square, through tg_generate on
+    a 4,096-chunk generator (host-output batches): every block and biome equals the
+    reference."""
+    import terrain_b200
+    g = terrain_b200.TerrainGenerator(max_batch_chunks=4096)
+    try:
+        rng = np.random.default_rng(2026)
+        for seed in [int(v) for v in rng.integers(-(1 << 63), (1 << 63) - 1, 4, dtype=np.int64)]:
+            near = rng.integers(-2000000, 2000000, (160, 2))
+            far = rng.integers(-8388607, 8388608, (24, 2))
+            square = np.array([(x, z) for z in range(4) for x in range(4)]) + rng.integers(-100000, 100000, 2)
+            chunks = np.concatenate([near, far, square]).astype(np.int32)
+            g.set_seed(seed)
+            b, q = g.generate(chunks)
+            rb, rq = ref_model.seed(seed).generate([tuple(int(v) for v in c) for c in chunks])
+            compare(b, q, rb, rq, [tuple(c) for c in chunks])
+    finally:
+        g.close()
