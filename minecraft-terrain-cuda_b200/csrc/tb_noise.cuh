@@ -70,9 +70,11 @@ TB_HD TB_FI float grad_pair(uint32_t h, float dx, float dy, float dz) {
 
 constexpr double kWrapLimit = 0x1.fffffffffffffp+23;   // largest double below 2^24
 
-// GradientNoise.wrap: values inside [-L, L) pass unchanged; the rest fold by 2^25.
+// GradientNoise.wrap: values inside [-L, L) pass unchanged; the rest fold by 2^25. One
+// compare on |v|: at v = -L the fold gives v back (floor(-L / 2^25 + 0.5) = 0), and NaN,
+// the infinities and L take the fold as before.
 TB_HD TB_FI double nwrap(double v) {
-    if (v >= -kWrapLimit && v < kWrapLimit) return v;
+    if (dabs(v) < kWrapLimit) return v;
     return v - dfloor(v / 33554432.0 + 0.5) * 33554432.0;
 }
 
