@@ -40,8 +40,8 @@ BYTES_PER_CHUNK = 98304 * 2 + 1536
 # block read, its u16 state written, and the column air / fluid masks (2 x 12 words x 256 columns)
 WALK_BYTES_PER_CHUNK = 98304 * (1 + 1 + 2) + 2 * 12 * 4 * 256
 # dram__bytes_read.sum + dram__bytes_write.sum of one 4,096-chunk launch of the walk-rules
-# kernel in this workload (539.13 MB + 277.87 MB), from profiles/walk_rules_traffic.md
-WALK_TRAFFIC_PER_LAUNCH = 817000000
+# kernel in this workload (538.80 MB + 277.87 MB), from profiles/walk_rules_traffic.md
+WALK_TRAFFIC_PER_LAUNCH = 816670000
 METRIC = 'bit-exact TERRAIN chunks/s on 1 B200, served vs plain; p50/p99 request latency'
 
 
