@@ -1152,6 +1152,10 @@ TB_HD inline void body_fill(const Batch& B, int it) {
     uint16_t* out = B.blocks + static_cast<size_t>(c) * kBlocksPerChunk;
     int top = INT_MIN;
     uint32_t air = 0, fluid = 0, ore_lo = 0, ore_hi = 0;
+    // the fill's blocks are the default block, air or a fluid: the flags of states 0..3 in
+    // one register word instead of a table load per block
+    const uint32_t flags4 = static_cast<uint32_t>(B.M.block_flags[0]) | (static_cast<uint32_t>(B.M.block_flags[1]) << 8) |
+                            (static_cast<uint32_t>(B.M.block_flags[2]) << 16) | (static_cast<uint32_t>(B.M.block_flags[3]) << 24);
     for (int k = 0; k < 8; ++k) {
         const int y = tbm::kMinY + cell_y * 8 + k;
         const float d = tbgen::gen_final_density(S.nt, bx, y, bz, ch);
@@ -1166,7 +1170,7 @@ TB_HD inline void body_fill(const Batch& B, int it) {
             if (k < 4) ore_lo |= om << (8 * k);
             else ore_hi |= om << (8 * (k - 4));
         }
-        const uint8_t f = B.M.block_flags[s];
+        const uint8_t f = s < 4 ? static_cast<uint8_t>(flags4 >> (8 * s)) : B.M.block_flags[s];
         if (!(f & 1)) top = y;
         air |= static_cast<uint32_t>(f & 1) << k;
         fluid |= static_cast<uint32_t>((f >> 3) & 1) << k;
