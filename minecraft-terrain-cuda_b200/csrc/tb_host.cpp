@@ -33,12 +33,15 @@ std::vector<uint8_t> md_pad(const uint8_t* data, size_t len, bool big_endian_len
 void md5(const uint8_t* data, size_t len, uint8_t out[16]) {
     // RFC 1321: per-round shift amounts and the sine-derived constants floor(|sin(i+1)| * 2^32)
     static const int S[4][4] = {{7, 12, 17, 22}, {5, 9, 14, 20}, {4, 11, 16, 23}, {6, 10, 15, 21}};
-    static uint32_t K[64];
-    static bool init = false;
-    if (!init) {
-        for (int i = 0; i < 64; ++i) K[i] = static_cast<uint32_t>(std::floor(std::fabs(std::sin(static_cast<double>(i + 1))) * 4294967296.0));
-        init = true;
-    }
+    // a function-local static is built once even when seed tables are built on several threads
+    struct Table {
+        uint32_t v[64];
+        Table() {
+            for (int i = 0; i < 64; ++i) v[i] = static_cast<uint32_t>(std::floor(std::fabs(std::sin(static_cast<double>(i + 1))) * 4294967296.0));
+        }
+    };
+    static const Table T;
+    const uint32_t* K = T.v;
     uint32_t h[4] = {0x67452301u, 0xefcdab89u, 0x98badcfeu, 0x10325476u};
     const std::vector<uint8_t> m = md_pad(data, len, false);
     for (size_t blk = 0; blk < m.size(); blk += 64) {
@@ -76,31 +79,33 @@ void md5(const uint8_t* data, size_t len, uint8_t out[16]) {
 void sha256(const uint8_t* data, size_t len, uint8_t out[32]) {
     // FIPS 180-4: K = first 32 bits of the fractional parts of the cube roots of the
     // first 64 primes, H0 = the same for the square roots of the first 8 primes.
-    static uint32_t K[64], H0[8];
-    static bool init = false;
-    if (!init) {
-        int primes[64], n = 0;
-        for (int c = 2; n < 64; ++c) {
-            bool p = true;
-            for (int d = 2; d * d <= c; ++d)
-                if (c % d == 0) p = false;
-            if (p) primes[n++] = c;
+    struct Table {
+        uint32_t K[64], H0[8];
+        Table() {
+            int primes[64], n = 0;
+            for (int c = 2; n < 64; ++c) {
+                bool p = true;
+                for (int d = 2; d * d <= c; ++d)
+                    if (c % d == 0) p = false;
+                if (p) primes[n++] = c;
+            }
+            auto frac32 = [](long double v) {
+                long double f = v - std::floor(v);
+                return static_cast<uint32_t>(static_cast<uint64_t>(std::floor(f * 4294967296.0L)));
+            };
+            for (int i = 0; i < 64; ++i) {
+                // long double cube root: 61 fraction bits, far more than the 32 kept; the MD5 /
+                // SHA-256 known-answer tests pin every constant
+                long double r = std::cbrt(static_cast<long double>(primes[i]));
+                K[i] = frac32(r);
+            }
+            for (int i = 0; i < 8; ++i) H0[i] = frac32(std::sqrt(static_cast<long double>(primes[i])));
         }
-        auto frac32 = [](long double v) {
-            long double f = v - std::floor(v);
-            return static_cast<uint32_t>(static_cast<uint64_t>(std::floor(f * 4294967296.0L)));
-        };
-        for (int i = 0; i < 64; ++i) {
-            // long double cube root: 61 fraction bits, far more than the 32 kept; the MD5 /
-            // SHA-256 known-answer tests pin every constant
-            long double r = std::cbrt(static_cast<long double>(primes[i]));
-            K[i] = frac32(r);
-        }
-        for (int i = 0; i < 8; ++i) H0[i] = frac32(std::sqrt(static_cast<long double>(primes[i])));
-        init = true;
-    }
+    };
+    static const Table T;   // built once, also when seed tables are built on several threads
+    const uint32_t* K = T.K;
     uint32_t h[8];
-    std::memcpy(h, H0, sizeof h);
+    std::memcpy(h, T.H0, sizeof h);
     const std::vector<uint8_t> m = md_pad(data, len, true);
     for (size_t blk = 0; blk < m.size(); blk += 64) {
         uint32_t w[64];

@@ -651,16 +651,21 @@ struct QuartLeaf {
     long long m;
     long long t[6];
 };
-TB_HD TB_NOINLINE inline QuartLeaf quart_leaf(const DevModel& M, const DevSeed& S, int X, int qy, int Z) {
-    const int x = 4 * X, y = tbm::kMinY + 4 * qy, z = 4 * Z;
-    float col[tbm::kClimateCols], cl[6];
-    tbgen::gen_climate_col(S.nt, x, z, col);
-    tbgen::gen_climate(S.nt, x, y, z, col, cl);
+// Quantized climate target of quart (X, qy, Z) from its column's climate terms col.
+TB_HD TB_FI void quart_target(const DevSeed& S, const float* col, int X, int qy, int Z, long long* t) {
+    float cl[6];
+    tbgen::gen_climate(S.nt, 4 * X, tbm::kMinY + 4 * qy, 4 * Z, col, cl);
+    for (int k = 0; k < 6; ++k) t[k] = f2l(cl[k] * 10000.0f);
+}
+
+// First minimal leaf of quart (X, qy, Z) and whether another leaf ties it, from the quart
+// column's climate terms col (gen_climate_col at x = 4 X, z = 4 Z).
+TB_HD TB_NOINLINE inline QuartLeaf quart_leaf_col(const DevModel& M, const DevSeed& S, const float* col, int X, int qy, int Z) {
     QuartLeaf q;
+    quart_target(S, col, X, qy, Z, q.t);
     bool small = M.boxes != nullptr && M.depth <= kRecDepth;
     int32_t t32[6];
     for (int k = 0; k < 6; ++k) {
-        q.t[k] = f2l(cl[k] * 10000.0f);
         small = small && q.t[k] >= -kBox32Limit && q.t[k] <= kBox32Limit;
         t32[k] = static_cast<int32_t>(q.t[k]);
     }
@@ -672,6 +677,11 @@ TB_HD TB_NOINLINE inline QuartLeaf quart_leaf(const DevModel& M, const DevSeed& 
         q.tie = tree_other_min(M, q.t, q.leaf, q.m);
     }
     return q;
+}
+TB_HD TB_NOINLINE inline QuartLeaf quart_leaf(const DevModel& M, const DevSeed& S, int X, int qy, int Z) {
+    float col[tbm::kClimateCols];
+    tbgen::gen_climate_col(S.nt, 4 * X, 4 * Z, col);
+    return quart_leaf_col(M, S, col, X, qy, Z);
 }
 
 // One quart column run: climate per quart, quantized targets, first minimal leaf.

@@ -234,21 +234,43 @@ __global__ void k_biome_point1(const __grid_constant__ DevModel M, const DevSeed
     }
 }
 
-__device__ int tied_chain(const DevModel& M, const DevSeed& S, const TiedLookup& T, int lane) {
+// Leaves of the quarts a tied lookup walks back over, one 16-bit entry per chain position
+// (index p - j), per warp of a 256-thread block.
+constexpr int kTiedWarps = 8;
+static_assert(tbm::kNumParams < 32768, "leaves are kept as 16-bit indices");
+
+// The zoomed lookup of a tied quart (chain position p of its chunk): the reference's
+// last-result chain from the nearest earlier quart whose result is fixed (unique minimum, or
+// position 0). Only the column climate terms carry noise, so the chunk's 16 quart columns are
+// evaluated once, lane c < 16 holding column (c >> 2, c & 3); the walk back keeps each quart's
+// first minimal leaf in lf, and the replay needs per quart only its target and one leaf
+// distance (the minimum it is compared with is the distance of that quart's own leaf).
+__device__ int tied_chain(const DevModel& M, const DevSeed& S, const TiedLookup& T, int lane, int16_t* lf) {
     const unsigned full = 0xFFFFFFFFu;
     const int X0 = (T.qx >> 2) * 4, Z0 = (T.qz >> 2) * 4;
     const int p = chain_pos(T.qx & 3, T.cqy, T.qz & 3);
-    int a, b, c;
-    // walk back: the nearest j < p whose result is fixed (unique minimum, or j = 0)
+    float colv[tbm::kClimateCols];
+    for (int k = 0; k < tbm::kClimateCols; ++k) colv[k] = 0.0f;
+    if (lane < 16) tbgen::gen_climate_col(S.nt, 4 * (X0 + (lane >> 2)), 4 * (Z0 + (lane & 3)), colv);
+    auto column_of = [&](int j, float* c) {
+        const int src = ((j >> 4) & 3) * 4 + (j & 3);
+        for (int k = 0; k < tbm::kClimateCols; ++k) c[k] = __shfl_sync(full, colv[k], src);
+    };
+    int a, b, cz;
+    float c[tbm::kClimateCols];
+    // walk back from p itself (lane 0 of the first window) to the nearest fixed j < p
     int anchor = -1, r = -1;
-    for (int base = p - 1; anchor < 0; base -= 32) {
+    __syncwarp();
+    for (int base = p; anchor < 0; base -= 32) {
         const int j = base - lane;
+        column_of(j < 0 ? 0 : j, c);
         bool fixed = false;
         int leaf = -1;
         if (j >= 0) {
-            chain_quart(j, a, b, c);
-            const QuartLeaf q = quart_leaf(M, S, X0 + a, b, Z0 + c);
-            fixed = !q.tie || j == 0;
+            chain_quart(j, a, b, cz);
+            const QuartLeaf q = quart_leaf_col(M, S, c, X0 + a, b, Z0 + cz);
+            lf[p - j] = static_cast<int16_t>(q.leaf);
+            fixed = j < p && (!q.tie || j == 0);
             leaf = q.leaf;
         }
         const unsigned m = __ballot_sync(full, fixed);
@@ -258,21 +280,23 @@ __device__ int tied_chain(const DevModel& M, const DevSeed& S, const TiedLookup&
             r = __shfl_sync(full, leaf, k);
         }
     }
+    __syncwarp();
     // replay the chain from the anchor to p, 32 quarts at a time (chain_warp's resolution)
     for (int k0 = anchor + 1; k0 <= p; k0 += 32) {
         const int nvalid = min(32, p - k0 + 1);
         const int k = k0 + lane;
-        QuartLeaf u;
-        u.leaf = -1;
-        u.m = 0;
+        column_of(k > p ? p : k, c);
+        long long t[6] = {0, 0, 0, 0, 0, 0}, um = 0;
+        int ls = -1;
         if (lane < nvalid) {
-            chain_quart(k, a, b, c);
-            u = quart_leaf(M, S, X0 + a, b, Z0 + c);
+            chain_quart(k, a, b, cz);
+            quart_target(S, c, X0 + a, b, Z0 + cz, t);
+            ls = lf[p - k];
+            um = param_dist(M.tree[M.leaf_node[ls]], t);
         }
-        const int ls = u.leaf;
         int prev = __shfl_up_sync(full, ls, 1);
         if (lane == 0) prev = r;
-        const bool keep = lane < nvalid && prev >= 0 && prev != ls && param_dist(M.tree[M.leaf_node[prev]], u.t) == u.m;
+        const bool keep = lane < nvalid && prev >= 0 && prev != ls && param_dist(M.tree[M.leaf_node[prev]], t) == um;
         const unsigned keeps = __ballot_sync(full, keep);
         int res = ls, v = r, pos = 0;
         while (pos < nvalid) {
@@ -292,7 +316,7 @@ __device__ int tied_chain(const DevModel& M, const DevSeed& S, const TiedLookup&
                 v = __shfl_sync(full, prev, jj);
                 pos = jj + 1;
             } else {
-                const bool carry = lane >= pos && lane < nvalid && v != ls && param_dist(M.tree[M.leaf_node[v]], u.t) == u.m;
+                const bool carry = lane >= pos && lane < nvalid && v != ls && param_dist(M.tree[M.leaf_node[v]], t) == um;
                 const unsigned run = __ballot_sync(full, carry) | ~(full << pos);
                 int jj = (~run) ? __ffs(~run) - 1 : 32;
                 if (jj > nvalid) jj = nvalid;
@@ -303,16 +327,18 @@ __device__ int tied_chain(const DevModel& M, const DevSeed& S, const TiedLookup&
         }
         r = __shfl_sync(full, res, nvalid - 1);
     }
+    __syncwarp();
     return r;
 }
 
-__global__ void k_biome_tied(const __grid_constant__ DevModel M, const DevSeed* seeds, const int32_t* slot, const TiedLookup* tied, const int32_t* n_tied,
+__global__ void __launch_bounds__(32 * kTiedWarps) k_biome_tied(const __grid_constant__ DevModel M, const DevSeed* seeds, const int32_t* slot, const TiedLookup* tied, const int32_t* n_tied,
                              uint8_t* out) {
+    __shared__ int16_t lf[kTiedWarps][kQuartsPerChunk];
     const int n = *n_tied, lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
     for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
         const TiedLookup T = tied[w];
-        const int r = tied_chain(M, seeds[slot[T.i]], T, lane);
+        const int r = tied_chain(M, seeds[slot[T.i]], T, lane, lf[threadIdx.x >> 5]);
         if (lane == 0) out[T.i] = static_cast<uint8_t>(M.leaf_biome[r]);
     }
 }
@@ -602,7 +628,8 @@ struct Generator {
 
     template <class T>
     void upload(DevBuf& b, const std::vector<T>& v) {
-        b.alloc(sizeof(T) * std::max<size_t>(v.size(), 1));
+        const size_t bytes = sizeof(T) * std::max<size_t>(v.size(), 1);
+        if (!b.p || b.bytes != bytes) b.alloc(bytes);   // a recycled seed slot keeps its buffers
         if (!v.empty()) ck(cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload");
     }
 
@@ -657,16 +684,31 @@ struct Generator {
 
     // Resident per-seed tables: the slot of a seed, built and uploaded on a miss; slots
     // listed in `keep` are not evicted.
-    int seed_slot(int64_t seed, const std::vector<int>& keep = {}) {
-        ++use_clock;
-        int free_slot = -1, lru = -1;
-        for (int i = 0; i < kMaxSlots; ++i) {
+    // The slot holding seed's tables (refreshing its use), or -1.
+    int resident_slot(int64_t seed) {
+        for (int i = 0; i < kMaxSlots; ++i)
             if (slots[i].valid && slots[i].seed == seed) {
-                slots[i].last_use = use_clock;
+                slots[i].last_use = ++use_clock;
                 return i;
             }
+        return -1;
+    }
+
+    int seed_slot(int64_t seed, const std::vector<int>& keep = {}) {
+        const int r = resident_slot(seed);
+        if (r >= 0) return r;
+        SeedHost h;
+        build_seed_host(seed, h);
+        return install_seed(seed, h, keep);
+    }
+
+    // Puts host tables h of seed into a free slot, else the least recently used one not in
+    // keep, and returns it.
+    int install_seed(int64_t seed, const SeedHost& h, const std::vector<int>& keep) {
+        ++use_clock;
+        int free_slot = -1, lru = -1;
+        for (int i = 0; i < kMaxSlots; ++i)
             if (!slots[i].valid && free_slot < 0) free_slot = i;
-        }
         int s = free_slot;
         if (s < 0) {
             for (int i = 0; i < kMaxSlots; ++i) {
@@ -676,8 +718,6 @@ struct Generator {
             s = lru;
         }
         if (s < 0) throw Error(TG_ERR_INTERNAL, "no free seed slot");
-        SeedHost h;
-        build_seed_host(seed, h);
         // queued work may still read the tables this slot held
         if (slots[s].valid) ck(cudaDeviceSynchronize(), "sync");
         SeedSlot& sl = slots[s];
@@ -983,24 +1023,52 @@ struct Generator {
         std::vector<int32_t> slot_of(cap);
         cudaStream_t s = stream;
         for (int off = 0; off < n;) {
+            // The sub-batch: positions up to cap whose seeds fit the slots. Resident seeds keep
+            // their slots; the new ones' host tables are built side by side on host threads,
+            // then installed (never into a slot this sub-batch uses).
             std::vector<int> used;
-            std::unordered_map<int64_t, int> seen;
+            std::unordered_map<int64_t, int> seen;   // seed -> slot, or -1 - index into fresh
+            std::vector<int64_t> fresh;
             int m = 0;
+            bool have_prev = false;
+            int64_t prev = 0;
             for (; m < cap && off + m < n; ++m) {
                 const int32_t* p = xyz + 3 * static_cast<size_t>(off + m);
                 const int32_t cx = p[0] >> 4, cz = p[2] >> 4;
                 if (cx <= -(1 << 23) || cx >= (1 << 23) || cz <= -(1 << 23) || cz >= (1 << 23)) throw Error(TG_ERR_RANGE, "position out of range");
                 const int64_t sd = seeds[off + m];
-                auto it = seen.find(sd);
-                if (it != seen.end()) {
-                    slot_of[m] = it->second;
-                    continue;
+                if (have_prev && sd == prev) continue;   // runs of one seed: no map lookup
+                have_prev = true;
+                prev = sd;
+                if (seen.count(sd)) continue;
+                if (static_cast<int>(seen.size()) == kMaxSlots) break;
+                const int sl = resident_slot(sd);
+                if (sl >= 0) {
+                    used.push_back(sl);
+                    seen.emplace(sd, sl);
+                } else {
+                    seen.emplace(sd, -1 - static_cast<int>(fresh.size()));
+                    fresh.push_back(sd);
                 }
-                if (static_cast<int>(used.size()) == kMaxSlots) break;
-                const int sl = seed_slot(sd, used);
-                used.push_back(sl);
-                seen.emplace(sd, sl);
-                slot_of[m] = sl;
+            }
+            if (!fresh.empty()) {
+                std::vector<SeedHost> built(fresh.size());
+                const int nt = static_cast<int>(std::min<size_t>(fresh.size(), std::max(1u, std::min(16u, std::thread::hardware_concurrency()))));
+                std::vector<std::thread> pool;
+                for (int w = 0; w < nt; ++w)
+                    pool.emplace_back([&, w] {
+                        for (size_t i = w; i < fresh.size(); i += nt) build_seed_host(fresh[i], built[i]);
+                    });
+                for (auto& th : pool) th.join();
+                for (size_t i = 0; i < fresh.size(); ++i) {
+                    const int sl = install_seed(fresh[i], built[i], used);
+                    used.push_back(sl);
+                    seen[fresh[i]] = sl;
+                }
+            }
+            for (int i = 0; i < m; ++i) {
+                const int64_t sd = seeds[off + i];
+                slot_of[i] = (i > 0 && sd == seeds[off + i - 1]) ? slot_of[i - 1] : seen[sd];
             }
             ck(cudaMemcpyAsync(d_xyz.p, xyz + 3 * static_cast<size_t>(off), sizeof(int32_t) * 3 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s), "h2d");
             ck(cudaMemcpyAsync(d_slot.p, slot_of.data(), sizeof(int32_t) * static_cast<size_t>(m), cudaMemcpyHostToDevice, s), "h2d");
