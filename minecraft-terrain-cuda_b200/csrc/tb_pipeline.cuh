@@ -659,8 +659,9 @@ TB_HD TB_FI void quart_target(const DevSeed& S, const float* col, int X, int qy,
 }
 
 // First minimal leaf of quart (X, qy, Z) and whether another leaf ties it, from the quart
-// column's climate terms col (gen_climate_col at x = 4 X, z = 4 Z).
-TB_HD TB_NOINLINE inline QuartLeaf quart_leaf_col(const DevModel& M, const DevSeed& S, const float* col, int X, int qy, int Z) {
+// column's climate terms col (gen_climate_col at x = 4 X, z = 4 Z). The search starts from
+// leaf start (any leaf: it only bounds the search, the result is the same).
+TB_HD TB_NOINLINE inline QuartLeaf quart_leaf_col(const DevModel& M, const DevSeed& S, const float* col, int X, int qy, int Z, int start = 0) {
     QuartLeaf q;
     quart_target(S, col, X, qy, Z, q.t);
     bool small = M.boxes != nullptr && M.depth <= kRecDepth;
@@ -670,10 +671,10 @@ TB_HD TB_NOINLINE inline QuartLeaf quart_leaf_col(const DevModel& M, const DevSe
         t32[k] = static_cast<int32_t>(q.t[k]);
     }
     if (small) {
-        q.leaf = tree_first_min32_levels(M, t32, 0, q.m);
+        q.leaf = tree_first_min32_levels(M, t32, start, q.m);
         q.tie = other_min_level32<kRecDepth - 1>(M, t32, 0, q.leaf, q.m);
     } else {
-        q.leaf = tree_first_min(M, q.t, 0, q.m);
+        q.leaf = tree_first_min(M, q.t, start, q.m);
         q.tie = tree_other_min(M, q.t, q.leaf, q.m);
     }
     return q;

@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(256) k_chain_warp(const __grid_constant__ Batc
 // fixed, 32 quarts of the walk evaluated at a time (biome_point's result, without one thread
 // walking hundreds of quarts while the rest of its warp waits).
 struct TiedLookup {
-    int32_t i, qx, cqy, qz;
+    int32_t i, qx, cqy, qz, leaf;   // leaf: the quart's own first minimal leaf
 };
 __global__ void k_biome_point1(const __grid_constant__ DevModel M, const DevSeed* seeds, const int32_t* slot, const int32_t* xyz, int n, uint8_t* out,
                                TiedLookup* tied, int32_t* n_tied) {
@@ -229,7 +229,7 @@ __global__ void k_biome_point1(const __grid_constant__ DevModel M, const DevSeed
         if (!q.tie || L.p == 0) {
             out[i] = static_cast<uint8_t>(M.leaf_biome[q.leaf]);
         } else {
-            tied[atomicAdd(n_tied, 1)] = TiedLookup{i, L.qx, L.cqy, L.qz};
+            tied[atomicAdd(n_tied, 1)] = TiedLookup{i, L.qx, L.cqy, L.qz, q.leaf};
         }
     }
 }
@@ -258,8 +258,10 @@ __device__ int tied_chain(const DevModel& M, const DevSeed& S, const TiedLookup&
     };
     int a, b, cz;
     float c[tbm::kClimateCols];
-    // walk back from p itself (lane 0 of the first window) to the nearest fixed j < p
-    int anchor = -1, r = -1;
+    // walk back from p itself (lane 0 of the first window) to the nearest fixed j < p; a
+    // lane's next quart is two layers below its last one in the same column, whose leaf
+    // starts its search
+    int anchor = -1, r = -1, start = T.leaf;
     __syncwarp();
     for (int base = p; anchor < 0; base -= 32) {
         const int j = base - lane;
@@ -268,10 +270,10 @@ __device__ int tied_chain(const DevModel& M, const DevSeed& S, const TiedLookup&
         int leaf = -1;
         if (j >= 0) {
             chain_quart(j, a, b, cz);
-            const QuartLeaf q = quart_leaf_col(M, S, c, X0 + a, b, Z0 + cz);
+            const QuartLeaf q = quart_leaf_col(M, S, c, X0 + a, b, Z0 + cz, start);
             lf[p - j] = static_cast<int16_t>(q.leaf);
             fixed = j < p && (!q.tie || j == 0);
-            leaf = q.leaf;
+            leaf = start = q.leaf;
         }
         const unsigned m = __ballot_sync(full, fixed);
         if (m) {
@@ -486,7 +488,7 @@ struct SeedSlot {
     int64_t seed = 0;
     bool valid = false;
     uint64_t last_use = 0;
-    DevBuf off, perm, layers, perm2;
+    DevBuf tables;   // octave offsets | layers | paired permutations | byte permutations, 256-byte aligned
 };
 
 // one output buffer set (the pipeline's outputs are double-buffered)
@@ -628,10 +630,11 @@ struct Generator {
 
     template <class T>
     void upload(DevBuf& b, const std::vector<T>& v) {
-        const size_t bytes = sizeof(T) * std::max<size_t>(v.size(), 1);
-        if (!b.p || b.bytes != bytes) b.alloc(bytes);   // a recycled seed slot keeps its buffers
+        b.alloc(sizeof(T) * std::max<size_t>(v.size(), 1));
         if (!v.empty()) ck(cudaMemcpy(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice), "upload");
     }
+
+    std::vector<uint8_t> seed_image;   // host image of one seed's tables, reused
 
     void upload_model() {
         ModelHost m;
@@ -721,12 +724,23 @@ struct Generator {
         // queued work may still read the tables this slot held
         if (slots[s].valid) ck(cudaDeviceSynchronize(), "sync");
         SeedSlot& sl = slots[s];
-        upload(sl.off, h.off);
-        upload(sl.perm, h.perm);
-        upload(sl.perm2, h.perm2);
-        upload(sl.layers, h.layers);
+        // one image and one copy per seed; the byte permutation table is read only by the
+        // unpaired hash form
+        auto al = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
+        const size_t b_off = sizeof(OctaveOff) * h.off.size(), b_lay = sizeof(Layer) * h.layers.size(), b_p2 = sizeof(uint16_t) * h.perm2.size();
+        const size_t b_p = TB_PERM_PAIRS ? 0 : h.perm.size();
+        const size_t o_lay = al(b_off), o_p2 = o_lay + al(b_lay), o_p = o_p2 + al(b_p2), total = o_p + al(b_p);
+        seed_image.assign(total, 0);
+        std::memcpy(seed_image.data(), h.off.data(), b_off);
+        std::memcpy(seed_image.data() + o_lay, h.layers.data(), b_lay);
+        std::memcpy(seed_image.data() + o_p2, h.perm2.data(), b_p2);
+        if (b_p) std::memcpy(seed_image.data() + o_p, h.perm.data(), b_p);
+        if (!sl.tables.p || sl.tables.bytes != total) sl.tables.alloc(total);
+        ck(cudaMemcpy(sl.tables.p, seed_image.data(), total, cudaMemcpyHostToDevice), "seed upload");
+        const uint8_t* base = sl.tables.as<uint8_t>();
         DevSeed d{};
-        d.nt = NoiseTables{sl.off.as<OctaveOff>(), sl.perm.as<uint8_t>(), sl.layers.as<Layer>(), sl.perm2.as<uint16_t>()};
+        d.nt = NoiseTables{reinterpret_cast<const OctaveOff*>(base), b_p ? base + o_p : nullptr, reinterpret_cast<const Layer*>(base + o_lay),
+                           reinterpret_cast<const uint16_t*>(base + o_p2)};
         d.random = h.random;
         d.aquifer = h.aquifer;
         d.ore = h.ore;
