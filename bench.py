@@ -8,8 +8,10 @@ material rules, u16 block states and u8 quart biomes out.
 
   value      chunks/s with the chunk lists already in HBM and the outputs left in HBM
              (tg_generate_device), device time from CUDA events on the launching stream
-  e2e        chunks/s through tg_generate with host buffers: the chunk list is copied
-             in and every block/biome byte copied out to pinned memory inside the step
+  e2e        chunks/s through tg_generate_u8 -- the reference generator's own call and output
+             type (u8 palette index per block) -- with host buffers: the chunk list is copied
+             in and every block and biome byte copied out to pinned memory inside the step;
+             e2e_u16 is the same through tg_generate (u16 block states)
   roofline   the dominant kernel (the column walk with the rule tree, timed by its own
              CUDA events): 294,912 B per chunk (u16 blocks + u8 per-block biomes, each read
              once) over its launch time, against the measured HBM copy peak
@@ -36,6 +38,7 @@ SEED = 0x5445525241494E31   # "TERRAIN1"
 REGIONS = [('origin', 0, 0), ('negative', -62500, -62500), ('border', 117124, 117124)]
 SIDE = 64
 BYTES_PER_CHUNK = 98304 * 2 + 1536
+BYTES_PER_CHUNK_U8 = 98304 + 1536
 # data the walk-rules kernel touches once per chunk: the u8 biome and u8 ore-vein bits of each
 # block read, its u16 state written, and the column air / fluid masks (2 x 12 words x 256 columns)
 WALK_BYTES_PER_CHUNK = 98304 * (1 + 1 + 2) + 2 * 12 * 4 * 256
@@ -424,23 +427,30 @@ def run_ours(args, rank, world, local_rank):
     all_chunks = np.concatenate(host_chunks)
     pin_all_blocks = torch.empty(n * nreg * 98304, dtype=torch.int16, pin_memory=True).numpy().view(np.uint16).reshape(n * nreg, -1, 16, 16)
     pin_all_biomes = torch.empty(n * nreg * 1536, dtype=torch.uint8, pin_memory=True).numpy().reshape(n * nreg, -1)
+    pin_all_blocks8 = torch.empty(n * nreg * 98304, dtype=torch.uint8, pin_memory=True).numpy().reshape(n * nreg, -1, 16, 16)
 
     def step_e2e():
         # one call per step: the library pipelines its batches (copies of batch k overlap batch k + 1)
+        g.generate_u8(all_chunks, blocks_out=pin_all_blocks8, biomes_out=pin_all_biomes)
+
+    def step_e2e_u16():
         g.generate(all_chunks, blocks_out=pin_all_blocks, biomes_out=pin_all_biomes)
 
-    for _ in range(max(1, min(args.warmup, 2))):
-        step_e2e()
-    torch.cuda.synchronize()
-    barrier()
-    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    for _ in range(args.steps):
-        step_e2e()
-    e3.record(stream)
-    torch.cuda.synchronize()
-    ms_e2e = max_over_ranks(e2.elapsed_time(e3), world, 'cuda')
-    e2e_value = chunks_total / (ms_e2e / 1000.0)
+    def time_e2e(step):
+        for _ in range(max(1, min(args.warmup, 2))):
+            step()
+        torch.cuda.synchronize()
+        barrier()
+        e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(args.steps):
+            step()
+        e3.record(stream)
+        torch.cuda.synchronize()
+        return chunks_total / (max_over_ranks(e2.elapsed_time(e3), world, 'cuda') / 1000.0)
+
+    e2e_value = time_e2e(step_e2e)
+    e2e_u16 = time_e2e(step_e2e_u16)
     pcie = pcie_d2h_gbs()
 
     if rank != 0:
@@ -469,8 +479,12 @@ def run_ours(args, rank, world, local_rank):
                              'profiles/walk_rules_traffic.md). The kernel is issue- and latency-bound (integer and FP64 rule '
                              'arithmetic), so its HBM fraction is small'},
         'e2e': {'value': round(e2e_value, 1), 'unit': 'chunks/s', 'h2d_bytes_per_step': int(n * nreg * 8),
-                'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK), 'd2h_gbs': round(e2e_value * BYTES_PER_CHUNK / 1e9, 2),
-                'pcie_d2h_gbs_measured': pcie, 'pcie_frac': round(e2e_value * BYTES_PER_CHUNK / 1e9 / pcie, 3) if pcie else None},
+                'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK_U8), 'd2h_gbs': round(e2e_value * BYTES_PER_CHUNK_U8 / 1e9, 2),
+                'pcie_d2h_gbs_measured': pcie, 'pcie_frac': round(e2e_value * BYTES_PER_CHUNK_U8 / 1e9 / pcie, 3) if pcie else None,
+                'api': 'tg_generate_u8 (u8 palette index per block and u8 quart biomes to pinned host memory)'},
+        'e2e_u16': {'value': round(e2e_u16, 1), 'unit': 'chunks/s', 'h2d_bytes_per_step': int(n * nreg * 8),
+                    'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK), 'd2h_gbs': round(e2e_u16 * BYTES_PER_CHUNK / 1e9, 2),
+                    'api': 'tg_generate (u16 block states and u8 quart biomes to pinned host memory)'},
         'gpu_launches': int(launches),
         'clocks': clk.summary(),
     }

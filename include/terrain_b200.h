@@ -85,6 +85,17 @@ tg_status tg_set_seed(struct tg_generator* gen, int64_t seed);
 tg_status tg_generate(struct tg_generator* gen, const tg_chunk_xz* chunks, int32_t count, uint16_t* blocks_out, uint8_t* biomes_out,
                       uint16_t* aquifer_out, tg_timing* timing);
 
+/* The same step in the reference generator's own output form: terrain_out and aquifer_out
+ * (may be NULL) hold one u8 palette index per block, biomes_out u8 per quart (may be NULL),
+ * in the same layouts as tg_generate. Each value is the u16 state of tg_generate narrowed
+ * (every state id is below the palette size); half the bytes cross the host link. The
+ * narrowing runs on the GPU after each batch; batches hold at most min(max_batch, 4096)
+ * chunks, then halving tail batches down to 512.
+ * reference: FullTerrainGenerator::generate (cuda/include/mccuda_cuda/terrain_gpu.h:41-43,
+ * cuda/src/terrain.cu:1392-1417), same argument types and order */
+tg_status tg_generate_u8(struct tg_generator* gen, const tg_chunk_xz* chunks, int32_t count, uint8_t* terrain_out, uint8_t* biomes_out,
+                         uint8_t* aquifer_out, tg_timing* timing);
+
 /* Device-resident form: chunks, blocks_out and biomes_out (may be NULL) are device
  * pointers; count <= max_batch_chunks; runs on the generator's stream and returns
  * when the work is done. No counterpart in the reference (its buffers are host-side);

@@ -53,7 +53,7 @@ class TgServerStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
            'tg_biome_lookup_noalloc',
            'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
            'tg_alloc_pinned', 'tg_free_pinned', 'tg_model_info', 'tg_last_error_string']
@@ -81,6 +81,7 @@ def load(path=LIB_PATH):
     L.tg_set_seed.argtypes = [vp, ctypes.c_int64]
     L.tg_set_stream.argtypes = [vp, vp]
     L.tg_generate.argtypes = [vp, ctypes.POINTER(TgChunk), ctypes.c_int32, vp, vp, vp, ctypes.POINTER(TgTiming)]
+    L.tg_generate_u8.argtypes = [vp, ctypes.POINTER(TgChunk), ctypes.c_int32, vp, vp, vp, ctypes.POINTER(TgTiming)]
     L.tg_generate_device.argtypes = [vp, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(TgTiming)]
     L.tg_generate_batch.argtypes = [vp, ctypes.POINTER(TgRequest), ctypes.c_int32, ctypes.POINTER(TgTiming)]
     L.tg_biome_lookup.argtypes = [vp, vp, vp, ctypes.c_int32, vp]
@@ -96,7 +97,7 @@ def load(path=LIB_PATH):
     L.tg_free_pinned.argtypes = [vp]
     L.tg_model_info.argtypes = [ctypes.POINTER(ctypes.c_int32)] * 5
     L.tg_last_error_string.restype = ctypes.c_char_p
-    for f in ('tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+    for f in ('tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
               'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
               'tg_model_info'):
         getattr(L, f).restype = ctypes.c_int
@@ -166,6 +167,19 @@ class TerrainGenerator:
         t = TgTiming() if timing else None
         self._check(self.L.tg_generate(self.h, a.ctypes.data_as(ctypes.POINTER(TgChunk)), n, _ptr(blocks), _ptr(biomes), _ptr(aq),
                                        ctypes.byref(t) if timing else None))
+        out = (blocks, biomes) + ((aq,) if aquifer else ())
+        return out + (t.as_dict(),) if timing else out
+
+    def generate_u8(self, chunks, blocks_out=None, biomes_out=None, aquifer=False, timing=False):
+        """The reference generator's output form: u8 palette index per block (tg_generate_u8)."""
+        a = chunk_array(chunks)
+        n = a.shape[0]
+        blocks = blocks_out if blocks_out is not None else np.empty((n, self.height, 16, 16), np.uint8)
+        biomes = biomes_out if biomes_out is not None else np.empty((n, self.qper), np.uint8)
+        aq = np.empty((n, self.height, 16, 16), np.uint8) if aquifer else None
+        t = TgTiming() if timing else None
+        self._check(self.L.tg_generate_u8(self.h, a.ctypes.data_as(ctypes.POINTER(TgChunk)), n, _ptr(blocks), _ptr(biomes), _ptr(aq),
+                                          ctypes.byref(t) if timing else None))
         out = (blocks, biomes) + ((aq,) if aquifer else ())
         return out + (t.as_dict(),) if timing else out
 

@@ -73,6 +73,32 @@ def test_host_batches_equal_whole_device_batches(ref_model):
         g.close()
 
 
+def test_u8_form_equals_narrowed_u16(ref_model):
+    """tg_generate_u8 (the reference generator's output type) gives every u16 state of
+    tg_generate as one byte, for blocks and the aquifer fill, over several batches and the
+    halving tail, with graphs and with stage timing, alternating with the u16 form; some of
+    its chunks also equal the reference directly."""
+    g = terrain_b200.TerrainGenerator(max_batch_chunks=256)
+    try:
+        g.set_seed(-4242)
+        chunks = np.array([(x, z) for z in range(-12, 13) for x in range(-14, 14)], np.int32)[:700]
+        chunks[-3:] = [(2097148, -2097149), (-2097152, 4194303), (8388607, -8388607)]
+        b16, q16, a16 = g.generate(chunks, aquifer=True)
+        assert int(b16.max()) < 256 and int(a16.max()) < 256
+        b8, q8, a8 = g.generate_u8(chunks, aquifer=True)
+        assert b8.dtype == np.uint8 and (b8 == b16.astype(np.uint8)).all() and (b8.astype(np.uint16) == b16).all()
+        assert (a8.astype(np.uint16) == a16).all() and (q8 == q16).all()
+        b8t, q8t, t = g.generate_u8(chunks[:300], timing=True)
+        assert (b8t.astype(np.uint16) == b16[:300]).all() and (q8t == q16[:300]).all() and t['launches'] > 0
+        b16b, _ = g.generate(chunks[:40])
+        assert (b16b == b16[:40]).all()
+        part = [tuple(int(v) for v in c) for c in chunks[-4:]]
+        rb, rq = ref_model.seed(-4242).generate(part)
+        assert (b8[-4:].astype(np.uint16) == rb).all() and (q8[-4:] == rq).all()
+    finally:
+        g.close()
+
+
 def test_server_alone_equals_mixed(ref_model):
     """Each served result is byte-identical alone and in a mix of concurrent requests."""
     g = terrain_b200.TerrainGenerator(max_batch_chunks=64)

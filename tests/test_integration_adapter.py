@@ -1,0 +1,37 @@
+"""The drop-in C++ adapter shown in INTEGRATION.md (the reference's FullTerrainGenerator over
+the C ABI) compiles against include/terrain_b200.h, and both generate overloads -- the
+reference's u8 palette-index form and the u16 form -- resolve. No GPU, no link."""
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def adapter_source():
+    text = open(os.path.join(REPO, 'INTEGRATION.md')).read()
+    section = text[text.index('## 2.'):]
+    return re.search(r'```cpp\n(.*?)```', section, flags=re.S).group(1)
+
+
+@pytest.mark.skipif(shutil.which('g++') is None, reason='needs g++')
+def test_adapter_compiles_and_keeps_the_reference_signature(tmp_path):
+    src = adapter_source()
+    assert 'tg_generate_u8' in src
+    use = '''
+#include <cstdint>
+void use(mcc::cuda::FullTerrainGenerator& g, const mcc::cuda::ChunkXZ* c, uint8_t* t8, uint8_t* b8, uint16_t* t16) {
+    g.generate(c, 1, t8, b8, nullptr);            // terrain_gpu.h:43
+    g.generate(c, 1, t8, b8, t8, nullptr);
+    g.generate(c, 1, t16);                        // u16 overload
+    mcc::cuda::TerrainTiming t;
+    g.generate(c, 1, t8, nullptr, nullptr, &t);
+}
+'''
+    f = tmp_path / 'adapter_check.cpp'
+    f.write_text(src + use)
+    r = subprocess.run(['g++', '-std=c++17', '-fsyntax-only', '-Wall', '-I', os.path.join(REPO, 'include'), str(f)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
