@@ -511,12 +511,28 @@ def main():
     ap.add_argument('--no-extra', action='store_true', help='skip the batched-seeds and biome-stream measurements')
     ap.add_argument('--profile-small', action='store_true',
                     help='one untimed step over a 32x32-chunk corner of each region, 1,024-chunk batches (a small case for ncu captures)')
+    ap.add_argument('--profile-lookup', action='store_true',
+                    help='three untimed tg_biome_lookup calls of one 2^20-position sub-batch (64 seeds x 16,384 positions), for ncu launch lists')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
     local_rank = int(os.environ.get('LOCAL_RANK', '0'))
     if args.impl == 'reference':
         run_reference(args, rank)
+        return
+    if args.profile_lookup:
+        import terrain_b200
+        g = terrain_b200.TerrainGenerator(max_batch_chunks=64)
+        rng = np.random.default_rng(5)
+        ns, per = 64, 16384
+        seeds = np.repeat(rng.integers(-(1 << 62), 1 << 62, ns).astype(np.int64), per)
+        xyz = np.empty((ns * per, 3), np.int32)
+        xyz[:, 0] = rng.integers(-1874999, 1875000, ns * per)
+        xyz[:, 1] = rng.integers(-64, 320, ns * per)
+        xyz[:, 2] = rng.integers(-1874999, 1875000, ns * per)
+        for _ in range(3):
+            g.biome_lookup(seeds, xyz)
+        g.close()
         return
     if args.profile_small:
         import terrain_b200
