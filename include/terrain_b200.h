@@ -32,7 +32,8 @@ typedef enum tg_status {
     TG_ERR_RANGE = 5,             /* chunk coordinate outside |c| < 2^23 */
     TG_ERR_NO_SEED = 6,           /* tg_generate before tg_set_seed */
     TG_ERR_DEVICE_TIMEOUT = 7,    /* a bounded device-side wait expired */
-    TG_ERR_INTERNAL = 8
+    TG_ERR_INTERNAL = 8,
+    TG_ERR_IO = 9                 /* a region file could not be written */
 } tg_status;
 
 /* reference: mcc::cuda::ChunkXZ (cuda/include/mccuda_cuda/generator.h:14-16) */
@@ -95,6 +96,23 @@ tg_status tg_generate(struct tg_generator* gen, const tg_chunk_xz* chunks, int32
  * cuda/src/terrain.cu:1392-1417), same argument types and order */
 tg_status tg_generate_u8(struct tg_generator* gen, const tg_chunk_xz* chunks, int32_t count, uint8_t* terrain_out, uint8_t* biomes_out,
                          uint8_t* aquifer_out, tg_timing* timing);
+
+/* Region outputs for consumers. Sets the generator's seed to seed, generates the
+ * region x region chunks from chunk (x0, z0) in u8 form, row-major by chunk
+ * ((cz - z0) * region + (cx - x0)), and writes
+ *   - when dump_dir is not NULL (created if missing): dump_dir/terrain.u8 (u8 palette index
+ *     per block, chunks back to back), dump_dir/biomes.u8 (u8 per quart) and
+ *     dump_dir/meta.json {seed, x0, z0, region, height, min_y, chunk_bytes, biome_bytes};
+ *   - when topdown_path is not NULL: the top-down map, "MCTD", int32 {1, region, x0, z0,
+ *     min_y}, then 8 bytes per block column row-major over the region: u8 top state (highest
+ *     non-air block), u8 floor state (first non-fluid block at or below it), u8 fluid depth
+ *     (at most 255), u8 0, int16 top y, int16 floor y.
+ * region in [1, 2048] (the top-down map of 2,048 is 8.6 GB of host memory); TG_ERR_IO when a
+ * file cannot be written.
+ * reference: write_dump (bench/bench_main.cpp:170-187) and write_topdown (:134-165); the dump
+ * is what the client maps (client/src/main/java/mccuda/client/GpuDump.java:88-104) */
+tg_status tg_write_region(struct tg_generator* gen, int64_t seed, int32_t x0, int32_t z0, int32_t region, const char* dump_dir,
+                          const char* topdown_path);
 
 /* Device-resident form: chunks, blocks_out and biomes_out (may be NULL) are device
  * pointers; count <= max_batch_chunks; runs on the generator's stream and returns

@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <filesystem>
 #include <fstream>
 #include <memory>
 #include <mutex>
@@ -1053,6 +1054,96 @@ struct Generator {
         finish();
     }
 
+    // Region outputs for consumers: the region x region chunks from (x0, z0) for seed, row-major
+    // by chunk ((cz - z0) * region + (cx - x0)), generated in u8 form a slab of chunk rows at a
+    // time. dump_dir gets terrain.u8 (one u8 palette index per block, chunks back to back),
+    // biomes.u8 (one u8 per quart) and meta.json; topdown_path gets the top-down map: "MCTD",
+    // int32 {1, region, x0, z0, min_y}, then per block column (row-major over the region's
+    // blocks) u8 top state, u8 floor state, u8 fluid depth (at most 255), u8 0, int16 top y,
+    // int16 floor y, where top is the highest non-air block (y 0 of the column when all is
+    // air) and floor the first non-fluid block at or below it.
+    // reference: write_dump (bench/bench_main.cpp:170-187), write_topdown (:134-165); the dump's
+    // reader is the client's GpuDump (client/src/main/java/mccuda/client/GpuDump.java:88-104).
+    void write_region(int64_t seed, int x0, int z0, int region, const char* dump_dir, const char* topdown_path) {
+        if (region <= 0 || region > 2048) throw Error(TG_ERR_INVALID_ARGUMENT, "region must be in [1, 2048] chunks");
+        const int64_t lim = 1 << 23;
+        if (x0 <= -lim || z0 <= -lim || static_cast<int64_t>(x0) + region - 1 >= lim || static_cast<int64_t>(z0) + region - 1 >= lim)
+            throw Error(TG_ERR_RANGE, "region outside |c| < 2^23");
+        current_slot = seed_slot(seed);
+        const int rows_per_slab = std::max(1, std::min(region, 4096 / region));
+        const size_t slab_chunks = static_cast<size_t>(rows_per_slab) * region;
+        PinBuf blk, bio;
+        blk.alloc(slab_chunks * kBlocksPerChunk);
+        bio.alloc(slab_chunks * kQuartsPerChunk);
+        std::ofstream ft, fb;
+        if (dump_dir) {
+            std::error_code ec;
+            std::filesystem::create_directories(dump_dir, ec);
+            ft.open(std::filesystem::path(dump_dir) / "terrain.u8", std::ios::binary);
+            fb.open(std::filesystem::path(dump_dir) / "biomes.u8", std::ios::binary);
+            if (!ft || !fb) throw Error(TG_ERR_IO, std::string("cannot write the region dump in ") + dump_dir);
+        }
+        const size_t side = static_cast<size_t>(region) * 16;
+        std::vector<uint8_t> rec(topdown_path ? side * side * 8 : 0, 0);
+        std::vector<tg_chunk_xz> chunks(slab_chunks);
+        for (int r0 = 0; r0 < region; r0 += rows_per_slab) {
+            const int rows = std::min(rows_per_slab, region - r0);
+            const int n = rows * region;
+            for (int r = 0; r < rows; ++r)
+                for (int i = 0; i < region; ++i) chunks[static_cast<size_t>(r) * region + i] = tg_chunk_xz{x0 + i, z0 + r0 + r};
+            generate(chunks.data(), n, nullptr, bio.as<uint8_t>(), nullptr, nullptr, blk.as<uint8_t>(), nullptr);
+            if (dump_dir) {
+                ft.write(blk.as<const char>(), static_cast<std::streamsize>(static_cast<size_t>(n) * kBlocksPerChunk));
+                fb.write(bio.as<const char>(), static_cast<std::streamsize>(static_cast<size_t>(n) * kQuartsPerChunk));
+                if (!ft || !fb) throw Error(TG_ERR_IO, std::string("cannot write the region dump in ") + dump_dir);
+            }
+            if (topdown_path) topdown_records(blk.as<const uint8_t>(), rows, region, r0, side, rec.data());
+        }
+        if (dump_dir) {
+            ft.close();
+            fb.close();
+            std::ofstream m(std::filesystem::path(dump_dir) / "meta.json");
+            m << "{\"seed\": " << seed << ", \"x0\": " << x0 << ", \"z0\": " << z0 << ", \"region\": " << region << ", \"height\": " << tbm::kHeight
+              << ", \"min_y\": " << tbm::kMinY << ", \"chunk_bytes\": " << kBlocksPerChunk << ", \"biome_bytes\": " << kQuartsPerChunk << "}\n";
+            if (!m || ft.fail() || fb.fail()) throw Error(TG_ERR_IO, std::string("cannot write the region dump in ") + dump_dir);
+        }
+        if (topdown_path) {
+            std::ofstream f(topdown_path, std::ios::binary);
+            const int32_t head[5] = {1, region, x0, z0, tbm::kMinY};
+            f.write("MCTD", 4);
+            f.write(reinterpret_cast<const char*>(head), sizeof head);
+            f.write(reinterpret_cast<const char*>(rec.data()), static_cast<std::streamsize>(rec.size()));
+            if (!f) throw Error(TG_ERR_IO, std::string("cannot write the top-down map ") + topdown_path);
+        }
+    }
+
+    // Top-down records of `rows` chunk rows of u8 blocks (row-major, region chunks per row),
+    // the first of them chunk row r0 of the region.
+    static void topdown_records(const uint8_t* blocks, int rows, int region, int r0, size_t side, uint8_t* rec) {
+        auto air = [](int st) { return (tbm::kBlockFlags[st] & 1) != 0; };
+        auto fluid = [](int st) { return (tbm::kBlockFlags[st] & 8) != 0; };
+        for (int r = 0; r < rows; ++r)
+            for (int i = 0; i < region; ++i) {
+                const uint8_t* b = blocks + (static_cast<size_t>(r) * region + i) * kBlocksPerChunk;
+                const size_t rx = static_cast<size_t>(i) * 16, rz = static_cast<size_t>(r0 + r) * 16;
+                for (int z = 0; z < 16; ++z)
+                    for (int x = 0; x < 16; ++x) {
+                        int y = tbm::kHeight - 1;
+                        while (y > 0 && air(b[(y * 16 + z) * 16 + x])) --y;
+                        const int top = b[(y * 16 + z) * 16 + x], top_y = y;
+                        while (y > 0 && fluid(b[(y * 16 + z) * 16 + x])) --y;
+                        uint8_t* o = rec + ((rz + z) * side + rx + x) * 8;
+                        o[0] = static_cast<uint8_t>(top);
+                        o[1] = b[(y * 16 + z) * 16 + x];
+                        o[2] = static_cast<uint8_t>(std::min(255, top_y - y));
+                        o[3] = 0;
+                        const int16_t ty = static_cast<int16_t>(tbm::kMinY + top_y), fy = static_cast<int16_t>(tbm::kMinY + y);
+                        std::memcpy(o + 4, &ty, 2);
+                        std::memcpy(o + 6, &fy, 2);
+                    }
+            }
+    }
+
     void generate_device(const tg_chunk_xz* chunks_dev, int count, uint16_t* blocks_dev, uint8_t* biomes_dev, tg_timing* t) {
         if (current_slot < 0) throw Error(TG_ERR_NO_SEED, "tg_set_seed has not been called");
         if (count > max_batch) throw Error(TG_ERR_INVALID_ARGUMENT, "count exceeds max_batch_chunks");
@@ -1650,6 +1741,14 @@ tg_status tg_biome_lookup(tg_generator* gen, const int64_t* seeds, const int32_t
         usable(gen);
         if (n < 0 || (n > 0 && (!seeds || !xyz || !out))) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
         gen->g->biome_lookup(seeds, xyz, n, out);
+    });
+}
+
+tg_status tg_write_region(tg_generator* gen, int64_t seed, int32_t x0, int32_t z0, int32_t region, const char* dump_dir, const char* topdown_path) {
+    return tb::guarded([&] {
+        usable(gen);
+        if (!dump_dir && !topdown_path) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "nothing to write: dump_dir and topdown_path are both null");
+        gen->g->write_region(seed, x0, z0, region, dump_dir, topdown_path);
     });
 }
 

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'lib', 'libterrain_b200.so')
 
 STATUS = {0: 'TG_OK', 1: 'TG_ERR_INVALID_ARGUMENT', 2: 'TG_ERR_MODEL_MISMATCH', 3: 'TG_ERR_CUDA', 4: 'TG_ERR_OUT_OF_MEMORY', 5: 'TG_ERR_RANGE',
-          6: 'TG_ERR_NO_SEED', 7: 'TG_ERR_DEVICE_TIMEOUT', 8: 'TG_ERR_INTERNAL'}
+          6: 'TG_ERR_NO_SEED', 7: 'TG_ERR_DEVICE_TIMEOUT', 8: 'TG_ERR_INTERNAL', 9: 'TG_ERR_IO'}
 
 
 class TgChunk(ctypes.Structure):
@@ -53,7 +53,7 @@ class TgServerStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_write_region', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
            'tg_biome_lookup_noalloc',
            'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
            'tg_alloc_pinned', 'tg_free_pinned', 'tg_model_info', 'tg_last_error_string']
@@ -82,6 +82,7 @@ def load(path=LIB_PATH):
     L.tg_set_stream.argtypes = [vp, vp]
     L.tg_generate.argtypes = [vp, ctypes.POINTER(TgChunk), ctypes.c_int32, vp, vp, vp, ctypes.POINTER(TgTiming)]
     L.tg_generate_u8.argtypes = [vp, ctypes.POINTER(TgChunk), ctypes.c_int32, vp, vp, vp, ctypes.POINTER(TgTiming)]
+    L.tg_write_region.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_char_p, ctypes.c_char_p]
     L.tg_generate_device.argtypes = [vp, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(TgTiming)]
     L.tg_generate_batch.argtypes = [vp, ctypes.POINTER(TgRequest), ctypes.c_int32, ctypes.POINTER(TgTiming)]
     L.tg_biome_lookup.argtypes = [vp, vp, vp, ctypes.c_int32, vp]
@@ -97,7 +98,7 @@ def load(path=LIB_PATH):
     L.tg_free_pinned.argtypes = [vp]
     L.tg_model_info.argtypes = [ctypes.POINTER(ctypes.c_int32)] * 5
     L.tg_last_error_string.restype = ctypes.c_char_p
-    for f in ('tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+    for f in ('tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_write_region', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
               'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
               'tg_model_info'):
         getattr(L, f).restype = ctypes.c_int
@@ -182,6 +183,12 @@ class TerrainGenerator:
                                           ctypes.byref(t) if timing else None))
         out = (blocks, biomes) + ((aq,) if aquifer else ())
         return out + (t.as_dict(),) if timing else out
+
+    def write_region(self, seed, x0, z0, region, dump_dir=None, topdown_path=None):
+        """Region dump (terrain.u8, biomes.u8, meta.json in dump_dir) and / or top-down map
+        (topdown_path) of the region x region chunks from (x0, z0); sets the seed."""
+        enc = lambda p: os.fsencode(p) if p is not None else None
+        self._check(self.L.tg_write_region(self.h, int(seed), int(x0), int(z0), int(region), enc(dump_dir), enc(topdown_path)))
 
     def generate_device(self, chunks_ptr, count, blocks_ptr, biomes_ptr=None, timing=True):
         """Device pointers (ints); returns the stage timing dict (None with timing=False, which
