@@ -730,7 +730,8 @@ struct Generator {
 
     // Puts host tables h of seed into a free slot, else the least recently used one not in
     // keep, and returns it.
-    int install_seed(int64_t seed, const SeedHost& h, const std::vector<int>& keep) {
+    // sync = false: the caller guarantees that no queued work reads a slot outside keep.
+    int install_seed(int64_t seed, const SeedHost& h, const std::vector<int>& keep, bool sync = true) {
         ++use_clock;
         int free_slot = -1, lru = -1;
         for (int i = 0; i < kMaxSlots; ++i)
@@ -745,7 +746,7 @@ struct Generator {
         }
         if (s < 0) throw Error(TG_ERR_INTERNAL, "no free seed slot");
         // queued work may still read the tables this slot held
-        if (slots[s].valid) ck(cudaDeviceSynchronize(), "sync");
+        if (slots[s].valid && sync) ck(cudaDeviceSynchronize(), "sync");
         SeedSlot& sl = slots[s];
         // one image and one copy per seed; the byte permutation table is read only by the
         // unpaired hash form
@@ -1170,73 +1171,117 @@ struct Generator {
         const int cap = std::min(n, 1 << 20);
         if (cap <= 0) return;
         finish();
-        DevBuf d_xyz, d_slot, d_res, d_tied, d_ntied;
-        d_tied.alloc(sizeof(TiedLookup) * static_cast<size_t>(cap));
-        d_ntied.alloc(sizeof(int32_t));
-        d_xyz.alloc(sizeof(int32_t) * 3 * static_cast<size_t>(cap));
-        d_slot.alloc(sizeof(int32_t) * static_cast<size_t>(cap));
-        d_res.alloc(static_cast<size_t>(cap));
-        std::vector<int32_t> slot_of(cap);
+        // Two sub-batches in flight: while one runs on the GPU the host prepares the next
+        // (positions checked and staged, slots assigned, new seeds built and installed).
+        struct Sub {
+            DevBuf xyz, slot, res, tied, ntied;
+            PinBuf hxyz, hslot, hres;
+            cudaEvent_t done = nullptr;
+            std::vector<int> used;   // seed slots its kernels read
+            int off = 0, m = 0;
+            bool busy = false;
+            ~Sub() {
+                if (done) cudaEventDestroy(done);
+            }
+        };
+        Sub sub[2];
+        for (Sub& S : sub) {
+            S.tied.alloc(sizeof(TiedLookup) * static_cast<size_t>(cap));
+            S.ntied.alloc(sizeof(int32_t));
+            S.xyz.alloc(sizeof(int32_t) * 3 * static_cast<size_t>(cap));
+            S.slot.alloc(sizeof(int32_t) * static_cast<size_t>(cap));
+            S.res.alloc(static_cast<size_t>(cap));
+            S.hxyz.alloc(sizeof(int32_t) * 3 * static_cast<size_t>(cap));
+            S.hslot.alloc(sizeof(int32_t) * static_cast<size_t>(cap));
+            S.hres.alloc(static_cast<size_t>(cap));
+            ck(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming), "event");
+        }
         cudaStream_t s = stream;
-        for (int off = 0; off < n;) {
-            // The sub-batch: positions up to cap whose seeds fit the slots. Resident seeds keep
-            // their slots; the new ones' host tables are built side by side on host threads,
-            // then installed (never into a slot this sub-batch uses).
-            std::vector<int> used;
-            std::unordered_map<int64_t, int> seen;   // seed -> slot, or -1 - index into fresh
-            std::vector<int64_t> fresh;
-            int m = 0;
-            bool have_prev = false;
-            int64_t prev = 0;
-            for (; m < cap && off + m < n; ++m) {
-                const int32_t* p = xyz + 3 * static_cast<size_t>(off + m);
-                const int32_t cx = p[0] >> 4, cz = p[2] >> 4;
-                if (cx <= -(1 << 23) || cx >= (1 << 23) || cz <= -(1 << 23) || cz >= (1 << 23)) throw Error(TG_ERR_RANGE, "position out of range");
-                const int64_t sd = seeds[off + m];
-                if (have_prev && sd == prev) continue;   // runs of one seed: no map lookup
-                have_prev = true;
-                prev = sd;
-                if (seen.count(sd)) continue;
-                if (static_cast<int>(seen.size()) == kMaxSlots) break;
-                const int sl = resident_slot(sd);
-                if (sl >= 0) {
-                    used.push_back(sl);
-                    seen.emplace(sd, sl);
-                } else {
-                    seen.emplace(sd, -1 - static_cast<int>(fresh.size()));
-                    fresh.push_back(sd);
+        auto collect = [&](Sub& S) {
+            ck(cudaEventSynchronize(S.done), "sync");
+            std::memcpy(res + S.off, S.hres.p, static_cast<size_t>(S.m));
+            S.busy = false;
+        };
+        try {
+            int k = 0;
+            for (int off = 0; off < n; k ^= 1) {
+                Sub& S = sub[k];
+                const Sub& P = sub[k ^ 1];   // in flight, if busy
+                if (S.busy) collect(S);
+                // The sub-batch: positions up to cap whose seeds fit the slots. Resident seeds
+                // keep their slots; the new ones' host tables are built side by side on host
+                // threads, then installed into slots neither this sub-batch nor the one in
+                // flight reads (so no device sync is needed).
+                std::vector<int> used;
+                std::unordered_map<int64_t, int> seen;   // seed -> slot, or -1 - index into fresh
+                std::vector<int64_t> fresh;
+                int m = 0;
+                bool have_prev = false;
+                int64_t prev = 0;
+                for (; m < cap && off + m < n; ++m) {
+                    const int32_t* p = xyz + 3 * static_cast<size_t>(off + m);
+                    const int32_t cx = p[0] >> 4, cz = p[2] >> 4;
+                    if (cx <= -(1 << 23) || cx >= (1 << 23) || cz <= -(1 << 23) || cz >= (1 << 23)) throw Error(TG_ERR_RANGE, "position out of range");
+                    const int64_t sd = seeds[off + m];
+                    if (have_prev && sd == prev) continue;   // runs of one seed: no map lookup
+                    have_prev = true;
+                    prev = sd;
+                    if (seen.count(sd)) continue;
+                    if (static_cast<int>(seen.size()) == kMaxSlots / 2) break;   // the two sub-batches' slots stay disjoint
+                    const int sl = resident_slot(sd);
+                    if (sl >= 0) {
+                        used.push_back(sl);
+                        seen.emplace(sd, sl);
+                    } else {
+                        seen.emplace(sd, -1 - static_cast<int>(fresh.size()));
+                        fresh.push_back(sd);
+                    }
                 }
-            }
-            if (!fresh.empty()) {
-                std::vector<SeedHost> built(fresh.size());
-                const int nt = static_cast<int>(std::min<size_t>(fresh.size(), std::max(1u, std::min(16u, std::thread::hardware_concurrency()))));
-                std::vector<std::thread> pool;
-                for (int w = 0; w < nt; ++w)
-                    pool.emplace_back([&, w] {
-                        for (size_t i = w; i < fresh.size(); i += nt) build_seed_host(fresh[i], built[i]);
-                    });
-                for (auto& th : pool) th.join();
-                for (size_t i = 0; i < fresh.size(); ++i) {
-                    const int sl = install_seed(fresh[i], built[i], used);
-                    used.push_back(sl);
-                    seen[fresh[i]] = sl;
+                if (!fresh.empty()) {
+                    std::vector<SeedHost> built(fresh.size());
+                    const int nt = static_cast<int>(std::min<size_t>(fresh.size(), std::max(1u, std::min(16u, std::thread::hardware_concurrency()))));
+                    std::vector<std::thread> pool;
+                    for (int w = 0; w < nt; ++w)
+                        pool.emplace_back([&, w] {
+                            for (size_t i = w; i < fresh.size(); i += nt) build_seed_host(fresh[i], built[i]);
+                        });
+                    for (auto& th : pool) th.join();
+                    std::vector<int> keep = used;
+                    if (P.busy) keep.insert(keep.end(), P.used.begin(), P.used.end());
+                    for (size_t i = 0; i < fresh.size(); ++i) {
+                        const int sl = install_seed(fresh[i], built[i], keep, /*sync=*/false);
+                        keep.push_back(sl);
+                        used.push_back(sl);
+                        seen[fresh[i]] = sl;
+                    }
                 }
+                int32_t* slot_of = S.hslot.as<int32_t>();
+                for (int i = 0; i < m; ++i) {
+                    const int64_t sd = seeds[off + i];
+                    slot_of[i] = (i > 0 && sd == seeds[off + i - 1]) ? slot_of[i - 1] : seen[sd];
+                }
+                std::memcpy(S.hxyz.p, xyz + 3 * static_cast<size_t>(off), sizeof(int32_t) * 3 * static_cast<size_t>(m));
+                ck(cudaMemcpyAsync(S.xyz.p, S.hxyz.p, sizeof(int32_t) * 3 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s), "h2d");
+                ck(cudaMemcpyAsync(S.slot.p, S.hslot.p, sizeof(int32_t) * static_cast<size_t>(m), cudaMemcpyHostToDevice, s), "h2d");
+                ck(cudaMemsetAsync(S.ntied.p, 0, sizeof(int32_t), s), "memset");
+                launch(k_biome_point1, s, m, model, d_seeds.as<DevSeed>(), S.slot.as<int32_t>(), S.xyz.as<int32_t>(), m, S.res.as<uint8_t>(),
+                       S.tied.as<TiedLookup>(), S.ntied.as<int32_t>());
+                launch(k_biome_tied, s, 32L * m, model, d_seeds.as<DevSeed>(), S.slot.as<int32_t>(), S.tied.as<TiedLookup>(), S.ntied.as<int32_t>(),
+                       S.res.as<uint8_t>());
+                ck(cudaGetLastError(), "kernel launch");
+                ck(cudaMemcpyAsync(S.hres.p, S.res.p, static_cast<size_t>(m), cudaMemcpyDeviceToHost, s), "d2h");
+                ck(cudaEventRecord(S.done, s), "event");
+                S.used = std::move(used);
+                S.off = off;
+                S.m = m;
+                S.busy = true;
+                off += m;
             }
-            for (int i = 0; i < m; ++i) {
-                const int64_t sd = seeds[off + i];
-                slot_of[i] = (i > 0 && sd == seeds[off + i - 1]) ? slot_of[i - 1] : seen[sd];
-            }
-            ck(cudaMemcpyAsync(d_xyz.p, xyz + 3 * static_cast<size_t>(off), sizeof(int32_t) * 3 * static_cast<size_t>(m), cudaMemcpyHostToDevice, s), "h2d");
-            ck(cudaMemcpyAsync(d_slot.p, slot_of.data(), sizeof(int32_t) * static_cast<size_t>(m), cudaMemcpyHostToDevice, s), "h2d");
-            ck(cudaMemsetAsync(d_ntied.p, 0, sizeof(int32_t), s), "memset");
-            launch(k_biome_point1, s, m, model, d_seeds.as<DevSeed>(), d_slot.as<int32_t>(), d_xyz.as<int32_t>(), m, d_res.as<uint8_t>(),
-                   d_tied.as<TiedLookup>(), d_ntied.as<int32_t>());
-            launch(k_biome_tied, s, 32L * m, model, d_seeds.as<DevSeed>(), d_slot.as<int32_t>(), d_tied.as<TiedLookup>(), d_ntied.as<int32_t>(),
-                   d_res.as<uint8_t>());
-            ck(cudaGetLastError(), "kernel launch");
-            ck(cudaMemcpyAsync(res + off, d_res.p, static_cast<size_t>(m), cudaMemcpyDeviceToHost, s), "d2h");
-            ck(cudaStreamSynchronize(s), "sync");
-            off += m;
+            for (Sub& S : sub)
+                if (S.busy) collect(S);   // the last two sub-batches
+        } catch (...) {
+            cudaStreamSynchronize(s);   // nothing in flight may outlive the buffers
+            throw;
         }
     }
 

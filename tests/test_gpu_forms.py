@@ -154,6 +154,41 @@ def test_biome_lookup_dense_and_many_seeds(gpu_gen, ref_model):
         assert (got[sel] == want).all(), 'seed %d' % s
 
 
+def test_biome_lookup_many_seeds_across_sub_batches(gpu_gen, ref_model):
+    """700 seeds interleaved position by position: each sub-batch holds at most 256 distinct
+    seeds (11 sub-batches, two in flight at a time), and there are more seeds than resident
+    slots, so slots are recycled while the previous sub-batch runs. Every position equals
+    the lookup of its seed alone, 24 seeds equal the reference, and a second call in reverse
+    order (some seeds resident, others rebuilt) gives the same bytes."""
+    rng = np.random.default_rng(12)
+    pool = np.array([int(v) for v in rng.integers(-(1 << 62), 1 << 62, 700)], np.int64)
+    n = 2800
+    seeds = pool[np.arange(n) % 700]
+    xyz = np.stack([rng.integers(-1874999, 1875000, n), rng.integers(-64, 320, n), rng.integers(-1874999, 1875000, n)], 1).astype(np.int32)
+    got = gpu_gen.biome_lookup(seeds, xyz)
+    assert (gpu_gen.biome_lookup(seeds[::-1], xyz[::-1]) == got[::-1]).all()
+    for s in pool:
+        sel = seeds == s
+        assert (gpu_gen.biome_lookup(np.full(int(sel.sum()), s), xyz[sel]) == got[sel]).all(), int(s)
+    for s in pool[:24]:
+        sel = seeds == s
+        assert (ref_model.seed(int(s)).biome_lookup(xyz[sel]) == got[sel]).all(), int(s)
+
+
+def test_biome_lookup_beyond_one_sub_batch(gpu_gen):
+    """2^20 + 70,000 positions of 3 seeds (two sub-batches by size): the tail equals the same
+    positions looked up alone."""
+    rng = np.random.default_rng(13)
+    n = (1 << 20) + 70000
+    pool = np.array([5, -77, 1 << 40], np.int64)
+    seeds = pool[rng.integers(0, 3, n)]
+    xyz = np.stack([rng.integers(-300000, 300000, n), rng.integers(-64, 320, n), rng.integers(-300000, 300000, n)], 1).astype(np.int32)
+    got = gpu_gen.biome_lookup(seeds, xyz)
+    k = (1 << 20) - 30000
+    assert (gpu_gen.biome_lookup(seeds[k:], xyz[k:]) == got[k:]).all()
+    assert (gpu_gen.biome_lookup(seeds[:50000], xyz[:50000]) == got[:50000]).all()
+
+
 def test_errors_are_status_codes(gpu_gen):
     with pytest.raises(terrain_b200.TerrainError) as e:
         gpu_gen.generate([(1 << 23, 0)])
