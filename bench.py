@@ -510,7 +510,8 @@ def main():
     ap.add_argument('--no-serve', action='store_true', help='skip the served-versus-plain request-stream measurement')
     ap.add_argument('--no-extra', action='store_true', help='skip the batched-seeds and biome-stream measurements')
     ap.add_argument('--profile-small', action='store_true',
-                    help='one untimed step over a 32x32-chunk corner of each region, 1,024-chunk batches (a small case for ncu captures)')
+                    help='one untimed step over a 32x32-chunk corner of each region, 1,024-chunk batches (a small case for ncu captures), '
+                         'then the first corner again in the u8 form')
     ap.add_argument('--profile-lookup', action='store_true',
                     help='three untimed tg_biome_lookup calls of one 2^20-position sub-batch (64 seeds x 16,384 positions), for ncu launch lists')
     args = ap.parse_args()
@@ -540,6 +541,7 @@ def main():
         g.set_seed(SEED)
         for _, x0, z0 in REGIONS:
             g.generate(region_chunks(x0, z0, 32))
+        g.generate_u8(region_chunks(0, 0, 32))   # last, so the launches before it are unchanged
         g.close()
         return
     if world > 1:
