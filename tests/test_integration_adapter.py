@@ -1,6 +1,7 @@
-"""The drop-in C++ adapter shown in INTEGRATION.md (the reference's FullTerrainGenerator over
-the C ABI) compiles against include/terrain_b200.h, and both generate overloads -- the
-reference's u8 palette-index form and the u16 form -- resolve. No GPU, no link."""
+"""The drop-in C++ adapter of the integration guide (section 2: the reference's
+FullTerrainGenerator over the C ABI) compiles against include/terrain_b200.h, and both
+generate overloads -- the reference's u8 palette-index form and the u16 form -- resolve.
+No GPU, no link."""
 import os
 import re
 import shutil
