@@ -361,6 +361,31 @@ __global__ void k_narrow_u8(const uint4* in, uint2* out, long n8) {
     }
 }
 
+// Top-down records (the region writer's map) of n chunks of u16 states in HBM: chunk c is
+// number first + c of a slab of whole chunk rows, region chunks per row, and its records go
+// to rec (the slab's block rows, region * 16 columns each, 8 bytes per column). One thread
+// per block column; a warp reads 32 neighbouring columns (64 contiguous bytes) per height.
+// Per column: the highest non-air block (y 0 when all is air), then down while fluid and
+// y > 0; u8 top, u8 floor, u8 min(255, depth), u8 0, int16 top y, int16 floor y.
+__global__ void k_topdown(const uint16_t* blocks, const uint8_t* flags, int n, int first, int region, uint2* rec) {
+    const long total = static_cast<long>(n) * 256;
+    for (long t = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; t < total; t += static_cast<long>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(t >> 8), z = static_cast<int>(t >> 4) & 15, x = static_cast<int>(t) & 15;
+        const uint16_t* b = blocks + static_cast<size_t>(c) * kBlocksPerChunk + z * 16 + x;
+        int y = tbm::kHeight - 1;
+        while (y > 0 && (flags[b[y * 256]] & 1)) --y;
+        const uint32_t top = b[y * 256];
+        const int top_y = y;
+        while (y > 0 && (flags[b[y * 256]] & 8)) --y;
+        const int g = first + c, r = g / region, i = g % region;
+        const size_t side = static_cast<size_t>(region) * 16;
+        uint2 v;
+        v.x = top | (static_cast<uint32_t>(b[y * 256]) << 8) | (static_cast<uint32_t>(min(255, top_y - y)) << 16);
+        v.y = static_cast<uint32_t>(static_cast<uint16_t>(tbm::kMinY + top_y)) | (static_cast<uint32_t>(static_cast<uint16_t>(tbm::kMinY + y)) << 16);
+        rec[(static_cast<size_t>(r) * 16 + z) * side + static_cast<size_t>(i) * 16 + x] = v;
+    }
+}
+
 // ---- scratch of the no-allocation biome lookup ---------------------------------------------------
 // tg_biome_lookup_noalloc stages its positions and results in this fixed device array
 // instead of device buffers allocated per call. Callers that cannot allocate device
@@ -1071,6 +1096,7 @@ struct Generator {
         if (x0 <= -lim || z0 <= -lim || static_cast<int64_t>(x0) + region - 1 >= lim || static_cast<int64_t>(z0) + region - 1 >= lim)
             throw Error(TG_ERR_RANGE, "region outside |c| < 2^23");
         current_slot = seed_slot(seed);
+        if (!dump_dir) return topdown_on_device(x0, z0, region, topdown_path);
         const int rows_per_slab = std::max(1, std::min(region, 4096 / region));
         const size_t slab_chunks = static_cast<size_t>(rows_per_slab) * region;
         PinBuf blk, bio;
@@ -1108,14 +1134,50 @@ struct Generator {
               << ", \"min_y\": " << tbm::kMinY << ", \"chunk_bytes\": " << kBlocksPerChunk << ", \"biome_bytes\": " << kQuartsPerChunk << "}\n";
             if (!m || ft.fail() || fb.fail()) throw Error(TG_ERR_IO, std::string("cannot write the region dump in ") + dump_dir);
         }
-        if (topdown_path) {
-            std::ofstream f(topdown_path, std::ios::binary);
-            const int32_t head[5] = {1, region, x0, z0, tbm::kMinY};
-            f.write("MCTD", 4);
-            f.write(reinterpret_cast<const char*>(head), sizeof head);
-            f.write(reinterpret_cast<const char*>(rec.data()), static_cast<std::streamsize>(rec.size()));
-            if (!f) throw Error(TG_ERR_IO, std::string("cannot write the top-down map ") + topdown_path);
+        if (topdown_path) write_topdown_file(topdown_path, region, x0, z0, rec);
+    }
+
+    // The top-down map alone: each slab of chunk rows is generated into HBM (pieces of at most
+    // max_batch chunks) and k_topdown reduces it to 8 bytes per block column, so only the
+    // records cross the host link.
+    void topdown_on_device(int x0, int z0, int region, const char* path) {
+        const int rows_per_slab = std::max(1, std::min(region, 4096 / region));
+        const size_t slab_chunks = static_cast<size_t>(rows_per_slab) * region;
+        const size_t side = static_cast<size_t>(region) * 16;
+        const int piece_max = std::min<int>(max_batch, static_cast<int>(slab_chunks));
+        std::vector<uint8_t> rec(side * side * 8);
+        std::vector<tg_chunk_xz> chunks(slab_chunks);
+        DevBuf d_chunks, d_blocks, d_rec;
+        d_chunks.alloc(sizeof(tg_chunk_xz) * slab_chunks);
+        d_blocks.alloc(sizeof(uint16_t) * static_cast<size_t>(piece_max) * kBlocksPerChunk);
+        d_rec.alloc(static_cast<size_t>(rows_per_slab) * 16 * side * 8);
+        for (int r0 = 0; r0 < region; r0 += rows_per_slab) {
+            const int rows = std::min(rows_per_slab, region - r0);
+            const int n = rows * region;
+            for (int r = 0; r < rows; ++r)
+                for (int i = 0; i < region; ++i) chunks[static_cast<size_t>(r) * region + i] = tg_chunk_xz{x0 + i, z0 + r0 + r};
+            check_chunks(chunks.data(), n);
+            ck(cudaMemcpy(d_chunks.p, chunks.data(), sizeof(tg_chunk_xz) * n, cudaMemcpyHostToDevice), "h2d");
+            for (int first = 0; first < n; first += piece_max) {
+                const int cnt = std::min(piece_max, n - first);
+                generate_device(d_chunks.as<tg_chunk_xz>() + first, cnt, d_blocks.as<uint16_t>(), nullptr, nullptr);
+                launch(k_topdown, stream, 256L * cnt, d_blocks.as<const uint16_t>(), model.block_flags, cnt, first, region, d_rec.as<uint2>());
+                ck(cudaGetLastError(), "kernel launch");
+            }
+            const size_t bytes = static_cast<size_t>(rows) * 16 * side * 8;
+            ck(cudaMemcpyAsync(rec.data() + static_cast<size_t>(r0) * 16 * side * 8, d_rec.p, bytes, cudaMemcpyDeviceToHost, stream), "d2h");
+            ck(cudaStreamSynchronize(stream), "sync");
         }
+        write_topdown_file(path, region, x0, z0, rec);
+    }
+
+    static void write_topdown_file(const char* path, int region, int x0, int z0, const std::vector<uint8_t>& rec) {
+        std::ofstream f(path, std::ios::binary);
+        const int32_t head[5] = {1, region, x0, z0, tbm::kMinY};
+        f.write("MCTD", 4);
+        f.write(reinterpret_cast<const char*>(head), sizeof head);
+        f.write(reinterpret_cast<const char*>(rec.data()), static_cast<std::streamsize>(rec.size()));
+        if (!f) throw Error(TG_ERR_IO, std::string("cannot write the top-down map ") + path);
     }
 
     // Top-down records of `rows` chunk rows of u8 blocks (row-major, region chunks per row),

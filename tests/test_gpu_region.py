@@ -2,7 +2,8 @@
 (terrain.u8, biomes.u8, meta.json; reference bench/bench_main.cpp:170-187, read by the
 client's GpuDump.java:88-104) and the top-down map (bench_main.cpp:134-165). The files must
 hold the u8 form of the same chunks in row-major order, and the top-down records the
-reference's column rule, restated here over numpy arrays."""
+reference's column rule, restated here over numpy arrays, whether computed on the host from
+the dumped blocks or on the device when the map is asked for alone."""
 import json
 import os
 import struct
@@ -73,6 +74,11 @@ def test_region_dump_and_topdown(tmp_path, ref_model, x0, z0, region):
         assert raw[:4] == b'MCTD' and struct.unpack('<5i', raw[4:24]) == (1, region, x0, z0, g.min_y)
         rec = np.frombuffer(raw[24:], np.uint8)
         assert (rec == topdown_records(b8, region, g.min_y)).all()
+        # the map alone is computed on the device (k_topdown over the u16 states in HBM, in
+        # pieces of at most max_batch_chunks that cross chunk-row boundaries): same bytes
+        td2 = tmp_path / 'top_device.mctd'
+        g.write_region(seed, x0, z0, region, topdown_path=str(td2))
+        assert open(td2, 'rb').read() == raw
         # one chunk of the dump against the reference port directly
         k = n // 2
         rb, rq = ref_model.seed(seed).generate([chunks[k]])
