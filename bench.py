@@ -11,12 +11,16 @@ material rules, u16 block states and u8 quart biomes out.
   e2e        chunks/s through tg_generate_u8 -- the reference generator's own call and output
              type (u8 palette index per block) -- with host buffers: the chunk list is copied
              in and every block and biome byte copied out to pinned memory inside the step;
-             e2e_u16 is the same through tg_generate (u16 block states)
-  roofline   the dominant kernel (the column walk with the rule tree, timed by its own
-             CUDA events): 294,912 B per chunk (u16 blocks + u8 per-block biomes, each read
-             once) over its launch time, against the measured HBM copy peak
-  cpu_baseline  the reference's own C++ port (oracle/_ref) on this host's cores, on a
-             bounded sample of the same regions
+             e2e_u16 is the same through tg_generate (u16 block states, the CPU port's type)
+  roofline   the largest kernel, the channel corners, against the issue rate: its work
+             counted in the reference port (octave samples of the corner phase, per distinct
+             corner point) times a minimal instruction recipe per sample, over its CUDA-event
+             launch time; roofline_walk_hbm gives the column walk's HBM fraction (417,792 B
+             per chunk over its launch time, against the measured HBM copy peak)
+  reference_gpu  the reference's own GPU generator built for sm_100a on the same step and
+             model (baseline/): end to end and kernels only, with our ratios
+  cpu_baseline  the reference's own C++ port (oracle/_ref) on this host's cores: a 16x16
+             region on 1 thread and a 32x32 region on all threads, as its bench does
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -43,8 +47,16 @@ BYTES_PER_CHUNK_U8 = 98304 + 1536
 # block read, its u16 state written, and the column air / fluid masks (2 x 12 words x 256 columns)
 WALK_BYTES_PER_CHUNK = 98304 * (1 + 1 + 2) + 2 * 12 * 4 * 256
 # dram__bytes_read.sum + dram__bytes_write.sum of one 4,096-chunk launch of the walk-rules
-# kernel in this workload (538.80 MB + 277.87 MB), from profiles/walk_rules_traffic.md
+# kernel in this workload (538.80 MB + 277.87 MB), from an ncu capture of that launch
 WALK_TRAFFIC_PER_LAUNCH = 816670000
+# Instructions (per thread) one volume-path octave sample needs at least, by pipe, following the
+# reference's perlin_volume (cpu/include/mccuda/noise_eval.h:163-178): per axis the coordinate
+# in FP64 (int-to-double, scale multiply, wrap test, offset add, floor, floor back to double,
+# subtract, double-to-float: 8) and its smoothstep (7 FP32); 14 permutation-table loads with
+# their 14 index adds; 8 lattice gradients of two non-zero unit components (2 FP32 and 3
+# integer selects each); the trilinear lerp (7 x 3 FP32); the amplitude accumulate (3 FP32).
+VOL_OCTAVE_INSTR = {'fp64': 24, 'fp32': 21 + 16 + 21 + 3, 'alu': 14 + 24, 'lsu': 14}
+OP_COUNTS = os.path.join(REPO, 'minecraft-terrain-cuda_b200', 'model', 'op_counts.json')
 METRIC = 'bit-exact TERRAIN chunks/s on 1 B200, served vs plain; p50/p99 request latency'
 
 
@@ -111,33 +123,53 @@ class ClockSampler:
         return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
-def cpu_baseline(threads=None, sample_side=8):
-    """The reference C++ port on this host: an 8x8-chunk square of each region on all threads,
-    and a 2x2 square of each region on one thread."""
+def host_cores():
+    """(hardware threads usable by this process, physical cores of the host)."""
+    try:
+        threads = len(os.sched_getaffinity(0))
+    except AttributeError:
+        threads = os.cpu_count()
+    try:
+        import psutil
+        physical = psutil.cpu_count(logical=False)
+    except Exception:
+        physical = None
+    return threads, physical
+
+
+def cpu_baseline(threads=None):
+    """The reference C++ port on this host, sized as the reference's own bench times it
+    (bench/bench_main.cpp:253-304, README.md:30-31): region form (biomes of the region plus a
+    one-chunk border computed once per chunk, then fill + surface per chunk), a 16x16-chunk
+    region on one thread and a 32x32-chunk region on all hardware threads, each at the corner
+    of the ladder's origin region."""
     import ref_oracle
     if not ref_oracle.available():
         return None
     m = ref_oracle.RefModel()
     s = m.seed(SEED)
-    threads = threads or os.cpu_count()
-    chunks = np.concatenate([region_chunks(x0, z0, sample_side) for _, x0, z0 in REGIONS])
-    s.generate(chunks[:threads], threads=threads)   # warm the caches / page in
+    hw, physical = host_cores()
+    threads = threads or hw
+    big = region_chunks(0, 0, 32)
+    s.generate(big[:threads], threads=threads)   # warm the caches / page in
     t0 = time.perf_counter()
-    s.generate(chunks, threads=threads)
+    s.generate(big, threads=threads)
     dt = time.perf_counter() - t0
-    one = np.concatenate([region_chunks(x0, z0, 2) for _, x0, z0 in REGIONS])
+    one = region_chunks(0, 0, 16)
     t0 = time.perf_counter()
     s.generate(one, threads=1)
     dt1 = time.perf_counter() - t0
-    return {'value': round(len(chunks) / dt, 2), 'unit': 'chunks/s', 'cores': threads, 'kind': 'reference',
-            'value_1_thread': round(len(one) / dt1, 2),
-            'sample': '%d chunks: an %dx%d square at the corner of each of the three regions, region form (biomes of the '
-                      'square plus a 1-chunk border, then fill + surface per chunk), %d threads; 1-thread figure from a 2x2 square '
-                      'per region (%d chunks)' % (len(chunks), sample_side, sample_side, threads, len(one))}
+    return {'value': round(len(big) / dt, 2), 'unit': 'chunks/s', 'cores': threads, 'kind': 'reference',
+            'value_1_thread': round(len(one) / dt1, 2), 'hardware_threads': hw, 'physical_cores': physical,
+            'sample': '32x32-chunk region at the origin on %d threads (%d chunks, %.1f s); 1-thread figure from the 16x16-chunk '
+                      'region at the origin (%d chunks, %.1f s); region form, biomes of the region plus a one-chunk border'
+                      % (threads, len(big), dt, len(one), dt1)}
 
 
 def run_reference(args, rank):
-    """Reference arm: the reference's own C++ port (oracle/_ref) on the host cores."""
+    """Reference arm: the reference's own C++ port (oracle/_ref) on all host threads. Each step
+    is a 32x32-chunk region (the size the reference's own bench times on all threads), in
+    region form, taken in turn from a quadrant of each of the three ladder regions."""
     if rank != 0:
         return
     import ref_oracle
@@ -146,29 +178,28 @@ def run_reference(args, rank):
         return
     m = ref_oracle.RefModel()
     s = m.seed(SEED)
-    threads = os.cpu_count()
-    per_step = 96   # bounded sample per step: a 4x8 block of chunks from each region
-    rng_sets = []
+    threads, physical = host_cores()
+    sets = []
     for k in range(args.warmup + args.steps):
-        sets = []
-        for _, x0, z0 in REGIONS:
-            ox, oz = (k * 8) % SIDE, (k * 4) % SIDE
-            sets.append(np.array([(x0 + ox + x, z0 + oz + z) for z in range(4) for x in range(8)], np.int32))
-        rng_sets.append(np.concatenate(sets))
+        _, x0, z0 = REGIONS[k % len(REGIONS)]
+        q = (k // len(REGIONS)) % 4
+        sets.append(region_chunks(x0 + 32 * (q % 2), z0 + 32 * (q // 2), 32))
+    per_step = sets[0].shape[0]
     for k in range(args.warmup):
-        s.generate(rng_sets[k], threads=threads)
+        s.generate(sets[k], threads=threads)
     t0 = time.perf_counter()
     for k in range(args.steps):
-        s.generate(rng_sets[args.warmup + k], threads=threads)
+        s.generate(sets[args.warmup + k], threads=threads)
     dt = time.perf_counter() - t0
     v = per_step * args.steps / dt
     line = {'metric': METRIC, 'value': round(v, 2), 'unit': 'chunks/s', 'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
             'ms_per_step': round(1000 * dt / args.steps, 3), 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32+f64+int',
             'data': 'synthetic world model (project-authored, reference JSON formats); seeded chunk lists', 'impl': 'reference',
             'config': {'workload': 'ladder: one seed, three 64x64-chunk regions (origin, -1,000,000 blocks, +1,874,999-block border)',
-                       'per_step_sample': '%d chunks (4x8 per region), the reference C++ port, %d host threads' % (per_step, threads)},
-            'cpu_baseline': {'value': round(v, 2), 'unit': 'chunks/s', 'cores': threads, 'kind': 'reference',
-                             'sample': '%d chunks per step, 4x8 per region' % per_step},
+                       'per_step_sample': '%d chunks: a 32x32-chunk quadrant of one ladder region per step, in turn, region form, '
+                                          'the reference C++ port on %d host threads' % (per_step, threads)},
+            'cpu_baseline': {'value': round(v, 2), 'unit': 'chunks/s', 'cores': threads, 'kind': 'reference', 'hardware_threads': threads,
+                             'physical_cores': physical, 'sample': '%d chunks per step (a 32x32 region)' % per_step},
             'e2e': {'value': round(v, 2), 'unit': 'chunks/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line))
 
@@ -297,14 +328,10 @@ def served_bench(g, n_unique=96, repeats=4, batch_sizes=(512, 768, 1024), loads=
     return out
 
 
-def batched_bench(g, n_seeds=256, seed=3):
-    """Many seeds and uneven chunk lists in one tg_generate_batch call: 256 seeds, list sizes
-    log-uniform in [1, 1024]; each list a contiguous square, scattered chunks within +/-117,187,
-    or chunks straddling the noise-lattice wrap at chunk 6128 / -6129. Outputs to pinned host
-    memory (requests share one pool; only the time is used)."""
-    import ctypes
-    import torch
-    import terrain_b200
+def batched_lists(n_seeds=256, seed=3):
+    """The batched workload: n_seeds random seeds, each with a chunk list of log-uniform size in
+    [1, 1024]; each list a contiguous square, scattered chunks within +/-117,187, or chunks
+    straddling the noise-lattice wrap at chunk 6128 / -6129. Returns (seeds, lists)."""
     rng = np.random.default_rng(seed)
     seeds = [int(v) for v in rng.integers(-(1 << 62), 1 << 62, n_seeds)]
     lists = []
@@ -321,6 +348,16 @@ def batched_bench(g, n_seeds=256, seed=3):
             xs = rng.choice(np.array([6127, 6128, 6129, -6128, -6129, -6130]), n)
             c = [(int(a), int(b)) for a, b in zip(xs, rng.integers(-117187, 117188, n))]
         lists.append(np.array(c, np.int32))
+    return seeds, lists
+
+
+def batched_bench(g, n_seeds=256, seed=3):
+    """Many seeds and uneven chunk lists in one tg_generate_batch call (batched_lists). Outputs
+    to pinned host memory (requests share one pool; only the time is used)."""
+    import ctypes
+    import torch
+    import terrain_b200
+    seeds, lists = batched_lists(n_seeds, seed)
     total = sum(len(c) for c in lists)
     biggest = max(len(c) for c in lists)
     pool_b = torch.empty(biggest * 98304, dtype=torch.int16, pin_memory=True).numpy().view(np.uint16)
@@ -372,6 +409,92 @@ def biome_stream_bench(g, n_seeds=1024, per_seed=16384, seed=5):
             'resident_lookups_per_s': round(k / dt_res, 1),
             'form': 'tg_biome_lookup: one thread per position, zoom corner then that quart\'s climate, R-tree minimum and tie test, '
                     'replaying the chunk chain only from the nearest earlier quart whose result is fixed'}
+
+
+def reference_gpu_bench(steps=3, warmup=2):
+    """The reference's own GPU generator (FullTerrainGenerator, built unchanged for sm_100a by
+    baseline/Makefile, evaluators generated by its own code generator from the same model
+    files) on this B200, on the same 12,288-chunk ladder step: end to end as the reference's
+    bench runs it (one generate() call per step, u8 blocks and u8 biomes into pinned host
+    memory, 2,048-chunk batches, 2 pipeline slots: its headline setting), and kernels only
+    (the sum of its per-stage CUDA-event times at 4,096-chunk batches, 1 slot). Returns None
+    when the side arm is not built."""
+    sys.path.insert(0, os.path.join(REPO, 'baseline'))
+    import refgpu
+    if not refgpu.available():
+        return None
+    import torch
+    chunks = np.concatenate([region_chunks(x0, z0) for _, x0, z0 in REGIONS])
+    n = chunks.shape[0]
+    t8 = torch.empty(n * 98304, dtype=torch.uint8, pin_memory=True).numpy().reshape(n, 384, 16, 16)
+    b8 = torch.empty(n * 1536, dtype=torch.uint8, pin_memory=True).numpy().reshape(n, 1536)
+    out = {'form': 'mcc::cuda::FullTerrainGenerator of the reference, compiled for sm_100a with its exactness flags, '
+                   'evaluators from its gen_router.py over the same model files'}
+    g = refgpu.RefGpuGenerator(max_batch_chunks=2048, pipeline_slots=2)
+    try:
+        g.set_seed(SEED)
+        for _ in range(warmup):
+            g.generate(chunks, t8, b8)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            g.generate(chunks, t8, b8)
+        dt = (time.perf_counter() - t0) / steps
+        out['e2e_chunks_per_s'] = round(n / dt, 1)
+        out['e2e_setting'] = 'batch 2048, 2 slots, pinned u8 blocks + biomes'
+    finally:
+        g.close()
+    g = refgpu.RefGpuGenerator(max_batch_chunks=4096, pipeline_slots=1)
+    try:
+        g.set_seed(SEED)
+        g.generate(chunks, t8, b8, timing=True)
+        ks = []
+        for _ in range(steps):
+            _, _, st = g.generate(chunks, t8, b8, timing=True)
+            ks.append(sum(st[k] for k in ('biome_ms', 'noise_ms', 'aquifer_ms', 'fill_ms', 'surface_ms')))
+            stages = st
+        ms = min(ks)
+        out['kernel_chunks_per_s'] = round(n / (ms / 1000.0), 1)
+        out['kernel_ms_per_step'] = round(ms, 3)
+        out['stage_ms_per_step'] = {k: round(v, 3) for k, v in stages.items()}
+        out['kernel_setting'] = 'batch 4096, 1 slot, sum of the per-stage CUDA-event times'
+    finally:
+        g.close()
+    return out
+
+
+def corner_roofline(stats, n, sms, clocks):
+    """Issue roofline of the channel-corner kernel, the largest kernel of the step. Its work is
+    counted, not guessed: the reference port's volume-path octave samples per chunk in its
+    corner phase (the interpolated channels' cell corners; oracle/count_ops.py, counting build
+    of the port), 25 corner columns x 49 rows per chunk there, scaled to the distinct corner
+    columns of one 64 x 64-chunk launch (257 x 257, each computed once), times the minimal
+    instruction recipe of one sample (VOL_OCTAVE_INSTR). Peak: 4 warp instructions per clock
+    per SM (32 threads each) at the SM clock sampled during the timed steps; the FP64 pipe (64
+    lanes per SM per clock) is reported beside it."""
+    try:
+        with open(OP_COUNTS) as f:
+            oc = json.load(f)
+    except OSError:
+        return None
+    per_point = oc['per_chunk']['corners']['vol_octave'] / (25 * 49)
+    side = int(round(n ** 0.5))
+    points = (side * 4 + 1) ** 2 * 49
+    samples = points * per_point
+    instr = samples * sum(VOL_OCTAVE_INSTR.values())
+    launch_ms = sum(t['corner_ms'] for t in stats) / len(stats)
+    mhz = clocks.get('sm_mhz') or 1965.0
+    peak = sms * 4 * 32 * mhz * 1e6 / 1e12                      # T thread-instructions / s
+    achieved = instr / (launch_ms / 1000.0) / 1e12
+    fp64_peak = sms * 64 * mhz * 1e6 / 1e12
+    fp64 = samples * VOL_OCTAVE_INSTR['fp64'] / (launch_ms / 1000.0) / 1e12
+    return {'bound': 'issue', 'kernel': 'corner (k_dyn<body_corner>)', 'achieved': round(achieved, 3), 'peak': round(peak, 3),
+            'unit': 'T thread-instructions/s', 'frac': round(achieved / peak, 4), 'traffic': None, 'launch_ms': round(launch_ms, 3),
+            'octave_samples_per_launch': int(samples), 'instructions_per_sample': VOL_OCTAVE_INSTR,
+            'fp64_pipe': {'achieved': round(fp64, 3), 'peak': round(fp64_peak, 3), 'frac': round(fp64 / fp64_peak, 4), 'unit': 'T FP64 ops/s'},
+            'peak_source': 'issue rate at the sampled SM clock (%s MHz), %d SMs' % (mhz, sms),
+            'note': 'samples = %.1f volume octave samples per corner point (the reference port\'s corner phase: %.0f per chunk over '
+                    '25 x 49 points, counting build) x %d distinct corner points of one %d-chunk launch' %
+                    (per_point, oc['per_chunk']['corners']['vol_octave'], points, n)}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -457,12 +580,14 @@ def run_ours(args, rank, world, local_rank):
         return
     stage = {k: sum(t[k] for t in stats) for k in ('biome_ms', 'noise_ms', 'aquifer_ms', 'fill_ms', 'surface_ms', 'kernel_ms')}
     launches = sum(t['launches'] for t in stats) * args.steps   # per step (the stats step) x timed steps
-    # dominant kernel: the column walk with the rule tree, timed by its own CUDA events
     calls = len(stats)
+    clocks = clk.summary()
+    # the column walk with the rule tree, timed by its own CUDA events: its HBM fraction
     per_launch_ms = sum(t['walk_rules_ms'] for t in stats) / calls
     algo_bytes = WALK_BYTES_PER_CHUNK * n
     achieved = algo_bytes / (per_launch_ms / 1000.0) / 1e9
     peak, peak_kind = peaks()
+    roofline = corner_roofline(stats, n, torch.cuda.get_device_properties(dev).multi_processor_count, clocks)
     line = {
         'metric': METRIC, 'value': round(value, 1), 'unit': 'chunks/s', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': round(ms_max / args.steps, 3), 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32+f64+int',
@@ -471,13 +596,13 @@ def run_ours(args, rank, world, local_rank):
                    'seed': SEED, 'chunks_per_step': n * nreg, 'batch_chunks': n, 'l2': 'outputs (2.4 GB per step) larger than L2',
                    'parallelism': 'replicas: each GPU runs the full workload' if world > 1 else 'single GPU'},
         'stage_ms_per_step': {k: round(v, 3) for k, v in stage.items()},
-        'roofline': {'bound': 'hbm', 'kernel': 'surface_walk_rules', 'achieved': round(achieved, 2), 'peak': peak, 'unit': 'GB/s',
-                     'frac': round(achieved / peak, 5), 'traffic': WALK_TRAFFIC_PER_LAUNCH, 'peak_source': peak_kind,
-                     'launch_ms': round(per_launch_ms, 3), 'share_of_step': round(per_launch_ms * calls / stage['kernel_ms'], 3),
-                     'note': 'algorithmic bytes = 417,792 B per chunk (per block the u8 biome and u8 ore bits read and the u16 state '
-                             'written, plus the column air / fluid masks) x 4,096 chunks per launch; traffic = dram read + write bytes of one 4,096-chunk launch (ncu, '
-                             'profiles/walk_rules_traffic.md). The kernel is issue- and latency-bound (integer and FP64 rule '
-                             'arithmetic), so its HBM fraction is small'},
+        'roofline': roofline,
+        'roofline_walk_hbm': {'bound': 'hbm', 'kernel': 'surface_walk_rules', 'achieved': round(achieved, 2), 'peak': peak, 'unit': 'GB/s',
+                              'frac': round(achieved / peak, 5), 'traffic': WALK_TRAFFIC_PER_LAUNCH, 'peak_source': peak_kind,
+                              'launch_ms': round(per_launch_ms, 3), 'share_of_step': round(per_launch_ms * calls / stage['kernel_ms'], 3),
+                              'note': 'algorithmic bytes = 417,792 B per chunk (per block the u8 biome and u8 ore bits read and the u16 state '
+                                      'written, plus the column air / fluid masks) x 4,096 chunks per launch; traffic = dram read + write bytes of '
+                                      'one 4,096-chunk launch (ncu). The kernel is issue- and latency-bound, so its HBM fraction is small'},
         'e2e': {'value': round(e2e_value, 1), 'unit': 'chunks/s', 'h2d_bytes_per_step': int(n * nreg * 8),
                 'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK_U8), 'd2h_gbs': round(e2e_value * BYTES_PER_CHUNK_U8 / 1e9, 2),
                 'pcie_d2h_gbs_measured': pcie, 'pcie_frac': round(e2e_value * BYTES_PER_CHUNK_U8 / 1e9 / pcie, 3) if pcie else None,
@@ -486,7 +611,7 @@ def run_ours(args, rank, world, local_rank):
                     'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK), 'd2h_gbs': round(e2e_u16 * BYTES_PER_CHUNK / 1e9, 2),
                     'api': 'tg_generate (u16 block states and u8 quart biomes to pinned host memory)'},
         'gpu_launches': int(launches),
-        'clocks': clk.summary(),
+        'clocks': clocks,
     }
     if not args.no_serve:
         g.set_stream(0)
@@ -495,6 +620,12 @@ def run_ours(args, rank, world, local_rank):
         g.set_stream(0)
         line['batched'] = batched_bench(g)
         line['biome_stream'] = biome_stream_bench(g)
+    if not args.no_reference_gpu:
+        line['reference_gpu'] = reference_gpu_bench()
+        if line['reference_gpu']:
+            rg = line['reference_gpu']
+            rg['ours_over_reference_kernels'] = round(value / rg['kernel_chunks_per_s'], 3)
+            rg['ours_over_reference_e2e'] = round(e2e_value / rg['e2e_chunks_per_s'], 3)
     if not args.no_cpu_baseline:
         line['cpu_baseline'] = cpu_baseline()
     print(json.dumps(line))
@@ -509,6 +640,7 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-serve', action='store_true', help='skip the served-versus-plain request-stream measurement')
     ap.add_argument('--no-extra', action='store_true', help='skip the batched-seeds and biome-stream measurements')
+    ap.add_argument('--no-reference-gpu', action='store_true', help='skip the reference GPU generator side arm')
     ap.add_argument('--profile-small', action='store_true',
                     help='one untimed step over a 32x32-chunk corner of each region, 1,024-chunk batches (a small case for ncu captures), '
                          'then the first corner again in the u8 form')

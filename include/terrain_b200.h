@@ -56,6 +56,7 @@ typedef struct tg_timing {
     int32_t batches;
     int32_t launches;     /* kernels launched by the call */
     float walk_rules_ms;  /* the column walk with the rule tree (part of surface_ms) */
+    float corner_ms;      /* the channel-corner kernel (part of noise_ms) */
 } tg_timing;
 
 /* Creates a generator for the model compiled into the library. ir_json_path and
@@ -121,6 +122,15 @@ tg_status tg_write_region(struct tg_generator* gen, int64_t seed, int32_t x0, in
 tg_status tg_generate_device(struct tg_generator* gen, const tg_chunk_xz* chunks_dev, int32_t count, uint16_t* blocks_dev, uint8_t* biomes_dev,
                              tg_timing* timing);
 
+/* Final density of every block of count chunks: the f32 value the fill tests (with the
+ * aquifer) before the material rules, in the block layout, count * 16 * 16 * height floats
+ * of host memory. The whole TERRAIN step runs; the fill also writes each density it
+ * evaluates. For parity checks at the density level.
+ * reference: TerrainGenerator::generate's density_out (cuda/include/mccuda_cuda/generator.h:38-39);
+ * the CPU port's ChunkTerrain::density (cpu/include/mccuda/terrain.h:59, filled at
+ * cpu/src/terrain.cpp:787-795) */
+tg_status tg_generate_density(struct tg_generator* gen, const tg_chunk_xz* chunks, int32_t count, float* density_out);
+
 /* Multi-seed batch: each request is its own seed and chunk list; all requests run in
  * shared device batches with positions deduplicated per seed. Output buffers are host
  * memory per request. No counterpart in the reference (single seed per generator). */
@@ -140,15 +150,19 @@ tg_status tg_generate_batch(struct tg_generator* gen, const tg_request* requests
 tg_status tg_biome_lookup(struct tg_generator* gen, const int64_t* seeds, const int32_t* xyz, int32_t n, uint8_t* out);
 
 /* Biome lookups for the seed of tg_set_seed that allocate nothing: for callers that cannot
- * allocate device memory (a tick thread running lookups while batches are in flight, where
- * cudaFree would synchronise the device; a process whose HBM budget is fully reserved).
- * Positions and results pass through one fixed device scratch array of 53,504 bytes, so
- * n <= 4,096 and n <= max_batch_chunks; larger n returns TG_ERR_INVALID_ARGUMENT. xyz
- * (3 x n int32) and out (n u8) are host memory. The first call on a device resolves the
- * scratch address; make it before any stream capture begins. Every call on a device
- * shares the array: calls that overlap on the GPU race (each call waits for its own
- * copies before it returns). Results equal tg_biome_lookup with every seed = the current
- * seed. No counterpart in the reference. */
+ * allocate device memory after start-up (a server that reserves its whole HBM budget when
+ * it creates the generator, so that a lookup cannot fail later on an allocation; a caller
+ * that must not cause the device-wide wait of cudaFree while other libraries' kernels run
+ * on other streams). Positions and results pass through one fixed device scratch array of
+ * 53,504 bytes, so n <= 4,096 and n <= max_batch_chunks; larger n returns
+ * TG_ERR_INVALID_ARGUMENT. xyz (3 x n int32) and out (n u8) are host memory. The call
+ * reuses the generator's batch buffers: it first waits for that generator's earlier work,
+ * so it runs on the generator's own thread, not beside its batches, and a generator owned
+ * by a server refuses it. The first call on a device resolves the scratch address; make
+ * it before any stream capture begins. Every call on a device shares the array: calls that
+ * overlap on the GPU race (each call waits for its own copies before it returns). Results
+ * equal tg_biome_lookup with every seed = the current seed. No counterpart in the
+ * reference. */
 tg_status tg_biome_lookup_noalloc(struct tg_generator* gen, const int32_t* xyz, int32_t n, uint8_t* out);
 
 /* ---- serving: continuous batching ---------------------------------------------------

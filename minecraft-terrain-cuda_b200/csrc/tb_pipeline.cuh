@@ -145,7 +145,7 @@ struct Batch {
     int32_t* aq_skip;                 // n
     // outputs and heights
     uint16_t* blocks;                 // n * kBlocksPerChunk
-    uint16_t* aquifer_copy;           // optional copy after the fill
+    float* density;                   // optional n * kBlocksPerChunk final density per block (block layout)
     int32_t* h0;                      // n * 256, x * 16 + z: heights after the fill
     int32_t* h1;                      // after the eroded-badlands extension
     int32_t* h2;                      // after the frozen-ocean extension (dry run)
@@ -1174,6 +1174,7 @@ TB_HD inline void body_fill(const Batch& B, int it) {
         if (s < 0) s = tbm::kDefaultBlock;
         const size_t bi = ((y - tbm::kMinY) * 16 + lz) * 16 + lx;
         out[bi] = static_cast<uint16_t>(s);
+        if (B.density) B.density[static_cast<size_t>(c) * kBlocksPerChunk + bi] = d;
         if (TB_ORE_MASK) {
             uint32_t om = 0;
             for (int v = 0; v < tbm::kNumOres; ++v)

@@ -388,13 +388,13 @@ __global__ void k_topdown(const uint16_t* blocks, const uint8_t* flags, int n, i
 
 // ---- scratch of the no-allocation biome lookup ---------------------------------------------------
 // tg_biome_lookup_noalloc stages its positions and results in this fixed device array
-// instead of device buffers allocated per call. Callers that cannot allocate device
-// memory use it: a game-server tick thread that runs lookups while the generator's
-// batches are in flight (cudaFree synchronises the whole device, so a per-call
-// allocation would stall those batches and the tick), and a process whose HBM budget is
-// fully reserved for generator and server buffers (an allocation there could fail in the
-// middle of a tick). Layout: [0, 256) header, the u32 count of finished positions at
-// offset 0, which must start at zero and is cleared by every call; then 3 x int32
+// instead of device buffers allocated per call. Callers that cannot allocate device memory
+// after start-up use it: a server that reserves its whole HBM budget when it creates the
+// generator (an allocation in the middle of a tick could fail), and a caller that must not
+// cause the device-wide wait of cudaFree while other libraries' kernels run on other
+// streams. The call still reuses the generator's batch buffers, so it waits for that
+// generator's earlier work first. Layout: [0, 256) header, the u32 count of finished
+// positions at offset 0, which must start at zero and is cleared by every call; then 3 x int32
 // positions; then the u8 biomes. At most 4,096 positions per call: 53,504 bytes.
 // Every call on a device shares this one array, so calls that overlap on the GPU race;
 // each call waits for its own copies before it returns.
@@ -618,7 +618,7 @@ struct Generator {
     cudaStream_t stream = nullptr;      // compute stream (the caller's, when set)
     cudaStream_t own_stream = nullptr;
     cudaStream_t copy_stream = nullptr;
-    cudaEvent_t ev[8] = {};
+    cudaEvent_t ev[10] = {};
     bool use_graphs = true;
     std::atomic<bool> served{false};    // owned by a server's worker thread
     // model
@@ -876,7 +876,9 @@ struct Generator {
         launch(k_number<1, cc_key, 25>, s, 25 * nmax, B);
         launch(k_items<body_cc_resolve, 25>, s, 25 * nmax, B);
         launch(k_dyn<body_corner_col, 1>, s, 16 * nmax, B, cnt_c);
+        mark(8);
         launch(k_dyn<body_corner, kRows, TB_MINB_CORNER>, s, 16 * nmax * kRows, B, cnt_c);
+        mark(9);
         launch(k_items<body_zoom_table, kZoomVerts>, s, kZoomVerts * nmax, B);
         launch(k_items<body_zoom_uniform, kZoomCells>, s, kZoomCells * nmax, B);
         mark(2);
@@ -918,7 +920,19 @@ struct Generator {
         float rules = 0.0f;
         ck(cudaEventElapsedTime(&rules, ev[6], ev[7]), "elapsed");
         t->walk_rules_ms += rules;
+        float corner = 0.0f;
+        ck(cudaEventElapsedTime(&corner, ev[8], ev[9]), "elapsed");
+        t->corner_ms += corner;
         t->batches += 1;
+    }
+
+    // the staged coordinates of o (cx | cz | seed slot | n) into lane W's batch buffers
+    void upload_coords(const Work& W, const OutSlot& o, int n, cudaStream_t s) {
+        const int32_t* h = o.coords.as<int32_t>();
+        ck(cudaMemcpyAsync(W.d_cx.p, h, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_cz.p, h + max_batch, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_cs.p, h + 2 * max_batch, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(W.d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
     }
 
     // Runs one batch whose staged coordinates sit in o.coords into output slot o.
@@ -931,11 +945,7 @@ struct Generator {
         // so each finishes (and its copy starts) as early as possible; smaller ones overlap.
         OutSlot& other = out[&o == &out[0] ? 1 : 0];
         if (lanes > 1 && n >= kOrderedBatch && other.lane != o.lane && other.busy) ck(cudaStreamWaitEvent(s, other.computed, 0), "wait");
-        const int32_t* h = o.coords.as<int32_t>();
-        ck(cudaMemcpyAsync(W.d_cx.p, h, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(W.d_cz.p, h + max_batch, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(W.d_cs.p, h + 2 * max_batch, 4 * n, cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(W.d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
+        upload_coords(W, o, n, s);
         if (want_aquifer && !o.aquifer.p) o.aquifer.alloc(sizeof(uint16_t) * static_cast<size_t>(max_batch) * kBlocksPerChunk);
         const Batch B = batch_view(W, &o);
         uint16_t* aq = want_aquifer ? o.aquifer.as<uint16_t>() : nullptr;
@@ -1223,6 +1233,42 @@ struct Generator {
         if (biomes_dev) ck(cudaMemcpyAsync(biomes_dev, o.biomes.p, static_cast<size_t>(count) * kQuartsPerChunk, cudaMemcpyDeviceToDevice, s), "d2d");
         ck(cudaGetLastError(), "kernel launch");
         ck(cudaStreamSynchronize(s), "sync");
+    }
+
+    // Final density of every block (the value the fill tests with the aquifer), written by
+    // the fill kernel into an extra buffer while the whole TERRAIN step runs as usual. The
+    // chunks go in batches of at most min(max_batch, 1024); out is host memory of
+    // count * kBlocksPerChunk floats in the block layout.
+    DevBuf d_density;
+    void generate_density(const tg_chunk_xz* chunks, int count, float* out_host) {
+        if (current_slot < 0) throw Error(TG_ERR_NO_SEED, "tg_set_seed has not been called");
+        check_chunks(chunks, count);
+        if (count == 0) return;
+        finish();
+        const int piece = std::min(max_batch, 1024);
+        const size_t bytes = sizeof(float) * static_cast<size_t>(piece) * kBlocksPerChunk;
+        if (d_density.bytes < bytes) d_density.alloc(bytes);
+        OutSlot& o = out[0];
+        Work& W = work[0];
+        cudaStream_t s = stream;
+        std::vector<int32_t> cx(piece), cz(piece), cs(piece, current_slot);
+        for (int off = 0; off < count; off += piece) {
+            const int n = std::min(piece, count - off);
+            for (int i = 0; i < n; ++i) {
+                cx[i] = chunks[off + i].x;
+                cz[i] = chunks[off + i].z;
+            }
+            stage(o, n, cx.data(), cz.data(), cs.data());
+            upload_coords(W, o, n, s);
+            Batch B = batch_view(W, &o);
+            B.density = d_density.as<float>();
+            enqueue_batch(W, B, s, max_batch, nullptr, false);
+            ck(cudaGetLastError(), "kernel launch");
+            ck(cudaMemcpyAsync(out_host + static_cast<size_t>(off) * kBlocksPerChunk, d_density.p, sizeof(float) * static_cast<size_t>(n) * kBlocksPerChunk,
+                               cudaMemcpyDeviceToHost, s),
+               "d2h");
+            ck(cudaStreamSynchronize(s), "sync");
+        }
     }
 
     // Biome lookups at independent positions: one thread per position computes the zoomed
@@ -1825,6 +1871,14 @@ tg_status tg_generate_device(tg_generator* gen, const tg_chunk_xz* chunks_dev, i
         tb::g_launches = 0;
         gen->g->generate_device(chunks_dev, count, blocks_dev, biomes_dev, timing);
         if (timing) timing->launches = tb::g_launches;
+    });
+}
+
+tg_status tg_generate_density(tg_generator* gen, const tg_chunk_xz* chunks, int32_t count, float* density_out) {
+    return tb::guarded([&] {
+        usable(gen);
+        if (count < 0 || (count > 0 && (!chunks || !density_out))) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        gen->g->generate_density(chunks, count, density_out);
     });
 }
 

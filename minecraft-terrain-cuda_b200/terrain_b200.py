@@ -29,7 +29,8 @@ class TgConfig(ctypes.Structure):
 
 class TgTiming(ctypes.Structure):
     _fields_ = [(k, ctypes.c_float) for k in ('h2d_ms', 'biome_ms', 'noise_ms', 'aquifer_ms', 'fill_ms', 'surface_ms', 'd2h_ms', 'kernel_ms',
-                                               'wall_ms')] + [('batches', ctypes.c_int32), ('launches', ctypes.c_int32), ('walk_rules_ms', ctypes.c_float)]
+                                               'wall_ms')] + [('batches', ctypes.c_int32), ('launches', ctypes.c_int32), ('walk_rules_ms', ctypes.c_float),
+                                               ('corner_ms', ctypes.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -53,7 +54,8 @@ class TgServerStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_write_region', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_write_region', 'tg_generate_device',
+           'tg_generate_density', 'tg_generate_batch', 'tg_biome_lookup',
            'tg_biome_lookup_noalloc',
            'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
            'tg_alloc_pinned', 'tg_free_pinned', 'tg_model_info', 'tg_last_error_string']
@@ -84,6 +86,7 @@ def load(path=LIB_PATH):
     L.tg_generate_u8.argtypes = [vp, ctypes.POINTER(TgChunk), ctypes.c_int32, vp, vp, vp, ctypes.POINTER(TgTiming)]
     L.tg_write_region.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_char_p, ctypes.c_char_p]
     L.tg_generate_device.argtypes = [vp, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(TgTiming)]
+    L.tg_generate_density.argtypes = [vp, vp, ctypes.c_int32, vp]
     L.tg_generate_batch.argtypes = [vp, ctypes.POINTER(TgRequest), ctypes.c_int32, ctypes.POINTER(TgTiming)]
     L.tg_biome_lookup.argtypes = [vp, vp, vp, ctypes.c_int32, vp]
     L.tg_biome_lookup_noalloc.argtypes = [vp, vp, ctypes.c_int32, vp]
@@ -98,7 +101,8 @@ def load(path=LIB_PATH):
     L.tg_free_pinned.argtypes = [vp]
     L.tg_model_info.argtypes = [ctypes.POINTER(ctypes.c_int32)] * 5
     L.tg_last_error_string.restype = ctypes.c_char_p
-    for f in ('tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_write_region', 'tg_generate_device', 'tg_generate_batch', 'tg_biome_lookup',
+    for f in ('tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_write_region', 'tg_generate_device',
+              'tg_generate_density', 'tg_generate_batch', 'tg_biome_lookup', 'tg_biome_lookup_noalloc',
               'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
               'tg_model_info'):
         getattr(L, f).restype = ctypes.c_int
@@ -197,6 +201,14 @@ class TerrainGenerator:
         self._check(self.L.tg_generate_device(self.h, ctypes.c_void_p(chunks_ptr), count, ctypes.c_void_p(blocks_ptr),
                                               ctypes.c_void_p(biomes_ptr) if biomes_ptr else None, ctypes.byref(t) if timing else None))
         return t.as_dict() if timing else None
+
+    def generate_density(self, chunks):
+        """Final density per block, f32 (n, height, 16, 16) (tg_generate_density)."""
+        a = chunk_array(chunks)
+        n = a.shape[0]
+        out = np.empty((n, self.height, 16, 16), np.float32)
+        self._check(self.L.tg_generate_density(self.h, _ptr(a), n, _ptr(out)))
+        return out
 
     def generate_batch(self, requests, timing=False):
         """requests: list of (seed, chunks). Returns list of (blocks, biomes)."""

@@ -27,10 +27,15 @@ def available():
     return os.path.exists(REF_LIB)
 
 
-def build(ref_root='/root/reference'):
+def reference_root():
+    """Where the reference's sources lie: $TERRAIN_REFERENCE_ROOT, else /root/reference."""
+    return os.environ.get('TERRAIN_REFERENCE_ROOT', '/root/reference')
+
+
+def build(ref_root=None):
     """Compiles oracle/_ref from the reference sources (only where they exist)."""
     import subprocess
-    subprocess.check_call(['make', '-s', '-C', HERE, 'REF=%s' % ref_root, '-j8'])
+    subprocess.check_call(['make', '-s', '-C', HERE, 'REF=%s' % (ref_root or reference_root()), '-j8'])
 
 
 def lib():
@@ -101,8 +106,9 @@ class RefSeed:
         except Exception:
             pass
 
-    def generate(self, chunks, threads=None, aquifer=False):
-        """TERRAIN step for a chunk list: (blocks u16 (n, h, 16, 16), biomes u8 (n, 1536)[, aquifer])."""
+    def generate(self, chunks, threads=None, aquifer=False, density=False):
+        """TERRAIN step for a chunk list: (blocks u16 (n, h, 16, 16), biomes u8 (n, 1536)[, aquifer u16][, density f32]),
+        density being the final density per block (ChunkTerrain::density, cpu/src/terrain.cpp:787-795)."""
         a = np.ascontiguousarray(np.asarray(chunks, np.int32).reshape(-1, 2))
         n = a.shape[0]
         cx = np.ascontiguousarray(a[:, 0])
@@ -111,10 +117,11 @@ class RefSeed:
         blocks = np.empty((n, h, 16, 16), np.uint16)
         biomes = np.empty((n, 16 * (h // 4)), np.uint8)
         aq = np.empty((n, h, 16, 16), np.uint16) if aquifer else None
-        st = self.L.ref_generate(ctypes.c_void_p(self.h), _p(cx), _p(cz), n, threads or os.cpu_count(), _p(blocks), _p(biomes), _p(aq), None)
+        dens = np.empty((n, h, 16, 16), np.float32) if density else None
+        st = self.L.ref_generate(ctypes.c_void_p(self.h), _p(cx), _p(cz), n, threads or os.cpu_count(), _p(blocks), _p(biomes), _p(aq), _p(dens))
         if st != 0:
             raise RuntimeError(self.L.ref_last_error().decode())
-        return (blocks, biomes, aq) if aquifer else (blocks, biomes)
+        return (blocks, biomes) + ((aq,) if aquifer else ()) + ((dens,) if density else ())
 
     def biome_lookup(self, xyz, threads=None):
         xyz = np.ascontiguousarray(np.asarray(xyz, np.int32).reshape(-1, 3))

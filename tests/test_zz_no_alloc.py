@@ -1,7 +1,11 @@
-"""tg_biome_lookup_noalloc, the lookup that allocates nothing, called through the C ABI and
-compared with tg_biome_lookup on the same positions: two calls in a row (the largest
-allowed call, then a smaller one, so stale scratch contents cannot pass), and the size
-limit. Collected last; passes alone in a fresh process and after the other tests."""
+"""tg_biome_lookup_noalloc, the lookup that allocates nothing (for callers that cannot
+allocate device memory after start-up), called through the C ABI: compared with
+tg_biome_lookup on the same positions over two calls in a row (the largest allowed call,
+then a smaller one, so stale scratch contents cannot pass), with the reference port's
+zoomed_biome over cpu_chunk_biomes (cpu/src/biome.cpp:272-289, cpu/src/terrain.cpp:152-176)
+on positions at chunk edges and above and below the world, and the size limit. Integer
+results, zero tolerance. Collected last; passes alone in a fresh process and after the
+other tests."""
 import ctypes
 
 import numpy as np
@@ -53,3 +57,19 @@ def test_noalloc_rejects_sizes_beyond_the_limit(gen):
     ok = positions(np.random.default_rng(3), 64)
     st = L.tg_biome_lookup_noalloc(h, ctypes.c_void_p(ok.ctypes.data), 64, ctypes.c_void_p(out.ctypes.data))
     assert st == 0, L.tg_last_error_string().decode()
+
+
+def test_noalloc_equals_reference_port(gen, ref_model):
+    """Chunk-edge x / z (block 0 and 15 of a chunk, where the zoom reaches the neighbour
+    chunk) and y below and above the world (the quart y is clamped) against the port."""
+    rng = np.random.default_rng(11)
+    n = 1024
+    edge = rng.choice(np.array([0, 1, 14, 15]), (n, 2))
+    cx, cz = rng.integers(-3000, 3000, n), rng.integers(-3000, 3000, n)
+    y = np.concatenate([rng.integers(-200, -64, n // 4), rng.integers(-64, 320, n // 2), rng.integers(320, 500, n - n // 4 - n // 2)])
+    xyz = np.ascontiguousarray(np.stack([cx * 16 + edge[:, 0], y, cz * 16 + edge[:, 1]], 1), np.int32)
+    got = gen.biome_lookup_noalloc(xyz)
+    want = ref_model.seed(SEED).biome_lookup(xyz)
+    assert np.unique(want).size > 1
+    bad = np.nonzero(got != want)[0]
+    assert bad.size == 0, 'positions differing from the reference: %s' % xyz[bad[:10]].tolist()
