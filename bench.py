@@ -49,13 +49,16 @@ WALK_BYTES_PER_CHUNK = 98304 * (1 + 1 + 2) + 2 * 12 * 4 * 256
 # dram__bytes_read.sum + dram__bytes_write.sum of one 4,096-chunk launch of the walk-rules
 # kernel in this workload (538.80 MB + 277.87 MB), from an ncu capture of that launch
 WALK_TRAFFIC_PER_LAUNCH = 816670000
-# Instructions (per thread) one volume-path octave sample needs at least, by pipe, following the
+# Instructions (per thread) one octave sample needs at least, by pipe, following the
 # reference's perlin_volume (cpu/include/mccuda/noise_eval.h:163-178): per axis the coordinate
-# in FP64 (int-to-double, scale multiply, wrap test, offset add, floor, floor back to double,
-# subtract, double-to-float: 8) and its smoothstep (7 FP32); 14 permutation-table loads with
-# their 14 index adds; 8 lattice gradients of two non-zero unit components (2 FP32 and 3
-# integer selects each); the trilinear lerp (7 x 3 FP32); the amplitude accumulate (3 FP32).
-VOL_OCTAVE_INSTR = {'fp64': 24, 'fp32': 21 + 16 + 21 + 3, 'alu': 14 + 24, 'lsu': 14}
+# in FP64 (scale multiply, wrap test, offset add, floor, floor back to double, subtract,
+# double-to-float: 7; the block coordinate's conversion is shared by a stack's layers) and
+# its smoothstep (7 FP32); 7 loads of a paired permutation table (both neighbours of a
+# lattice step in one entry) with an add and a mask each and 8 byte extracts; 8 lattice
+# gradients of two non-zero unit components (a sign flip and an add each in FP32, 3 integer
+# selects); the corner offsets (3 FP32), the trilinear lerp (7 x 3 FP32) and the amplitude
+# accumulate (3 FP32).
+VOL_OCTAVE_INSTR = {'fp64': 21, 'fp32': 21 + 16 + 3 + 21 + 3, 'alu': 14 + 8 + 24, 'lsu': 7}
 OP_COUNTS = os.path.join(REPO, 'minecraft-terrain-cuda_b200', 'model', 'op_counts.json')
 METRIC = 'bit-exact TERRAIN chunks/s on 1 B200, served vs plain; p50/p99 request latency'
 
@@ -247,84 +250,115 @@ def serving_requests(n, rng):
     return seeds, reqs
 
 
-def served_bench(g, n_unique=96, repeats=4, batch_sizes=(512, 768, 1024), loads=(0.5, 0.6, 0.7, 0.75, 0.8), seed=2024, p99_target_ms=20.0):
-    """Plain (one synchronous tg_generate per request, in order) against the continuous-batching
-    server on the same request stream (n_unique view-distance requests, submitted repeats times):
-    saturated throughput of both, then the server's latency under Poisson arrivals at each
-    fraction in `loads` of its saturated throughput, for each device batch size. Reports every
-    point and the highest served throughput whose p99 stays under p99_target_ms. Outputs go to
-    pinned host memory in both forms (repeated requests reuse their request's buffers)."""
+def p99_interval(lat):
+    """(p99, low, high): the 99th percentile of the latencies and its 95 % interval from the
+    order statistics (binomial ranks n * 0.99 -/+ 1.96 sqrt(n * 0.99 * 0.01))."""
+    v = np.sort(np.asarray(lat))
+    n = v.shape[0]
+    if n == 0:
+        return None, None, None
+    sd = 1.96 * np.sqrt(n * 0.99 * 0.01)
+    lo = int(max(0, np.floor(n * 0.99 - sd) - 1))
+    hi = int(min(n - 1, np.ceil(n * 0.99 + sd) - 1))
+    return float(np.quantile(v, 0.99)), float(v[lo]), float(v[hi])
+
+
+def served_bench(g, n_unique=96, batch_chunks=768, loads=(0.6, 0.7, 0.8), seed=2024, p99_target_ms=20.0, seconds=10.0, min_requests=5000):
+    """Plain against served on a stream of view-distance requests: the plain
+    form is one synchronous tg_generate per request, in order; the server runs the same
+    stream in both output forms (u16, and u8 through tg_server_submit_u8). For each form: the
+    saturated throughput (everything submitted at once), then Poisson arrivals at each
+    fraction in `loads` of it, each point lasting at least `seconds` and `min_requests`
+    requests, with p50 and p99 (and the p99's 95 % interval) of submit -> last byte on the
+    host. A point is steady when it served at least 97 % of what was offered; the best
+    steady point under the p99 target is reported. Outputs go to pinned host memory (a
+    request re-submitted reuses its buffers)."""
     import torch
     import terrain_b200
     rng = np.random.default_rng(seed)
     seeds, reqs = serving_requests(n_unique, rng)
     h = g.height
     sizes = [len(c) for _, c in reqs]
-    pool = torch.empty(sum(sizes) * (256 * h + 768), dtype=torch.int16, pin_memory=True).numpy().view(np.uint16)
+    per16 = 256 * h + 768
+    pool = torch.empty(sum(sizes) * per16, dtype=torch.int16, pin_memory=True).numpy().view(np.uint16)
     offs, at = [], 0
     for n in sizes:
         offs.append(at)
-        at += n * (256 * h + 768)
+        at += n * per16
 
-    def bufs(i):
+    def bufs(i, u8):
         n = sizes[i]
-        b = pool[offs[i]:offs[i] + n * 256 * h].reshape(n, h, 16, 16)
-        q = pool[offs[i] + n * 256 * h:offs[i] + n * (256 * h + 768)].view(np.uint8).reshape(n, 1536)
-        return b, q
+        base = pool[offs[i]:offs[i] + n * per16]
+        q = base[n * 256 * h:].view(np.uint8)[:n * 1536].reshape(n, 1536)
+        b = base[:n * 256 * h]
+        return (b.view(np.uint8)[:n * 256 * h].reshape(n, h, 16, 16) if u8 else b.reshape(n, h, 16, 16)), q
 
-    stream = [i % n_unique for i in range(n_unique * repeats)]
-    total = sum(sizes[i] for i in stream)
+    mean_chunks = float(np.mean(sizes))
     for sd in seeds:                      # resident tables for the whole pool
         g.set_seed(sd)
     g.generate(reqs[0][1][:1])
-    t0 = time.perf_counter()
-    for i in stream:
-        b, q = bufs(i)
+    # plain: synchronous calls in order for about `seconds / 2`
+    done, t0 = 0, time.perf_counter()
+    k = 0
+    while time.perf_counter() - t0 < seconds / 2 or k < n_unique:
+        i = k % n_unique
+        b, q = bufs(i, False)
         g.set_seed(reqs[i][0])
         g.generate(reqs[i][1], blocks_out=b, biomes_out=q)
-    plain_cps = total / (time.perf_counter() - t0)
-    out = {'requests': len(stream), 'chunks': total, 'seed_pool': 64, 'plain_chunks_per_s': round(plain_cps, 1), 'p99_target_ms': p99_target_ms,
-           'points': []}
-    best = None
-    for bc in batch_sizes:
-        with terrain_b200.TerrainServer(g, batch_chunks=bc) as srv:
-            for t in [srv.submit(reqs[i][0], reqs[i][1], *bufs(i)) for i in range(4)]:
+        done += sizes[i]
+        k += 1
+    plain_cps = done / (time.perf_counter() - t0)
+    out = {'seed_pool': 64, 'unique_requests': n_unique, 'mean_request_chunks': round(mean_chunks, 1), 'plain_chunks_per_s': round(plain_cps, 1),
+           'plain_requests': k, 'batch_chunks': batch_chunks, 'p99_target_ms': p99_target_ms, 'forms': {}}
+    for form in ('u16', 'u8'):
+        u8 = form == 'u8'
+        res = {'points': []}
+        with terrain_b200.TerrainServer(g, batch_chunks=batch_chunks) as srv:
+            for t in [srv.submit(reqs[i][0], reqs[i][1], *bufs(i, u8), u8=u8) for i in range(4)]:
                 srv.wait(t)
+            # saturated: about seconds / 2 of work submitted at once
+            n_sat = max(n_unique, int(seconds / 2 * 250000 / mean_chunks))
+            stream = [i % n_unique for i in range(n_sat)]
             srv.reset_stats()
             t0 = time.perf_counter()
-            tickets = [srv.submit(reqs[i][0], reqs[i][1], *bufs(i)) for i in stream]
+            tickets = [srv.submit(reqs[i][0], reqs[i][1], *bufs(i, u8), u8=u8) for i in stream]
             for t in tickets:
                 srv.wait(t)
-            sat_cps = total / (time.perf_counter() - t0)
-            st = srv.stats()
-            out['points'].append({'batch_chunks': bc, 'load': 'saturated', 'served_chunks_per_s': round(sat_cps, 1),
-                                  'p50_ms': round(st['p50_ms'], 2), 'p99_ms': round(st['p99_ms'], 2)})
+            sat = sum(sizes[i] for i in stream) / (time.perf_counter() - t0)
+            res['saturated_chunks_per_s'] = round(sat, 1)
+            res['saturated_over_plain'] = round(sat / plain_cps, 3)
             for frac in loads:
-                rate = frac * sat_cps / (total / len(stream))          # requests per second
-                gaps = rng.exponential(1.0 / rate, len(stream))
+                rate = frac * sat / mean_chunks                         # requests per second
+                n_req = int(max(min_requests, rate * seconds))
+                order = rng.integers(0, n_unique, n_req)
+                gaps = rng.exponential(1.0 / rate, n_req)
                 srv.reset_stats()
                 tickets = []
-                due = time.perf_counter()
-                for k, i in enumerate(stream):
-                    due += gaps[k]
+                due = t_start = time.perf_counter()
+                for k2 in range(n_req):
+                    due += gaps[k2]
                     wait = due - time.perf_counter()
                     if wait > 0:
                         time.sleep(wait)
-                    tickets.append(srv.submit(reqs[i][0], reqs[i][1], *bufs(i)))
+                    i = int(order[k2])
+                    tickets.append(srv.submit(reqs[i][0], reqs[i][1], *bufs(i, u8), u8=u8))
                 for t in tickets:
                     srv.wait(t)
+                span = time.perf_counter() - t_start
                 st = srv.stats()
-                pt = {'batch_chunks': bc, 'load': frac, 'offered_chunks_per_s': round(rate * total / len(stream), 1),
-                      'served_chunks_per_s': round(st['chunks_per_s'], 1), 'p50_ms': round(st['p50_ms'], 2), 'p99_ms': round(st['p99_ms'], 2),
-                      'max_ms': round(st['max_ms'], 2)}
-                out['points'].append(pt)
-                if pt['p99_ms'] < p99_target_ms and (best is None or pt['served_chunks_per_s'] > best['served_chunks_per_s']):
-                    best = pt
-    sat = max(p['served_chunks_per_s'] for p in out['points'] if p['load'] == 'saturated')
-    out['served_saturated_chunks_per_s'] = sat
-    out['saturated_over_plain'] = round(sat / plain_cps, 3)
-    if best is not None:
-        out['best_under_target'] = dict(best, served_over_plain=round(best['served_chunks_per_s'] / plain_cps, 3))
+                lat = srv.latencies()
+                p99, lo, hi = p99_interval(lat)
+                offered = sum(sizes[int(i)] for i in order) / (due - t_start)
+                pt = {'load': frac, 'requests': n_req, 'seconds': round(span, 2), 'offered_chunks_per_s': round(offered, 1),
+                      'served_chunks_per_s': round(st['chunks_per_s'], 1), 'p50_ms': round(st['p50_ms'], 2), 'p99_ms': round(p99, 2),
+                      'p99_ci95_ms': [round(lo, 2), round(hi, 2)], 'max_ms': round(st['max_ms'], 2)}
+                pt['steady'] = pt['served_chunks_per_s'] >= 0.97 * pt['offered_chunks_per_s']
+                res['points'].append(pt)
+        steady = [p for p in res['points'] if p['steady'] and p['p99_ms'] < p99_target_ms]
+        if steady:
+            best = max(steady, key=lambda p: p['served_chunks_per_s'])
+            res['best_steady_under_target'] = dict(best, served_over_plain=round(best['served_chunks_per_s'] / plain_cps, 3))
+        out['forms'][form] = res
     return out
 
 
@@ -379,9 +413,45 @@ def batched_bench(g, n_seeds=256, seed=3):
         g._check(g.L.tg_generate_batch(g.h, reqs, n_seeds, None))
         dt = time.perf_counter() - t0
         best = dt if best is None else min(best, dt)
-    return {'seeds': n_seeds, 'chunks': total, 'chunks_per_s': round(total / best, 1), 'ms': round(best * 1000, 2),
-            'form': 'tg_generate_batch, device batches of up to 4,096 chunks mixing seeds, outputs copied to pinned host memory',
-            'lists': 'log-uniform sizes 1..1024; squares, scattered within +/-117,187, and wrap-straddling chunks 6127..6129 / -6128..-6130'}
+    out = {'seeds': n_seeds, 'chunks': total, 'chunks_per_s': round(total / best, 1), 'ms': round(best * 1000, 2),
+           'form': 'tg_generate_batch, device batches of up to 4,096 chunks mixing seeds, outputs copied to pinned host memory',
+           'lists': 'log-uniform sizes 1..1024; squares, scattered within +/-117,187, and wrap-straddling chunks 6127..6129 / -6128..-6130'}
+    out['device_queue'] = batched_device_bench(g, seeds, lists)
+    return out
+
+
+def batched_device_bench(g, seeds, lists, reps=3):
+    """The same 256-seed workload with every list and output in HBM (tg_generate_batch_device):
+    the requests form one device work queue drained by one graph launch (a WHILE loop on the
+    device), against one graph launch per batch from the host; CUDA events on the stream."""
+    import torch
+    chunks = [torch.from_numpy(c).cuda() for c in lists]
+    total = sum(len(c) for c in lists)
+    blocks = torch.empty(total * 98304, dtype=torch.int16, device='cuda')
+    biomes = torch.empty(total * 1536, dtype=torch.uint8, device='cuda')
+    reqs, at = [], 0
+    for sd, c in zip(seeds, chunks):
+        n = c.shape[0]
+        reqs.append((sd, c.data_ptr(), n, blocks.data_ptr() + 2 * 98304 * at, biomes.data_ptr() + 1536 * at))
+        at += n
+    res = {}
+    for name, host_loop in (('device_loop', False), ('host_loop', True)):
+        g.generate_batch_device(reqs, host_loop=host_loop)                     # warm-up: graphs
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            g.generate_batch_device(reqs, host_loop=host_loop)
+            e1.record()
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        res[name] = {'chunks_per_s': round(total / (min(ms) / 1000.0), 1), 'ms': round(min(ms), 2)}
+    res['form'] = ('tg_generate_batch_device: lists and outputs in HBM, one device work queue of (chunk, seed) items, 4,096-chunk '
+                   'batches; device_loop = one graph launch with a WHILE node, host_loop = one graph launch per batch')
+    del blocks, biomes
+    torch.cuda.empty_cache()
+    return res
 
 
 def biome_stream_bench(g, n_seeds=1024, per_seed=16384, seed=5):
@@ -464,37 +534,42 @@ def reference_gpu_bench(steps=3, warmup=2):
 
 def corner_roofline(stats, n, sms, clocks):
     """Issue roofline of the channel-corner kernel, the largest kernel of the step. Its work is
-    counted, not guessed: the reference port's volume-path octave samples per chunk in its
-    corner phase (the interpolated channels' cell corners; oracle/count_ops.py, counting build
-    of the port), 25 corner columns x 49 rows per chunk there, scaled to the distinct corner
-    columns of one 64 x 64-chunk launch (257 x 257, each computed once), times the minimal
-    instruction recipe of one sample (VOL_OCTAVE_INSTR). Peak: 4 warp instructions per clock
-    per SM (32 threads each) at the SM clock sampled during the timed steps; the FP64 pipe (64
-    lanes per SM per clock) is reported beside it."""
+    counted, not guessed: the octave samples the kernel evaluates per corner point, counted
+    on the host twin of the kernel bodies (tests/hostcheck/count_kernels.py: volume, smeared
+    volume and point samples, lazy per-point evaluation), times the distinct corner points of
+    one 64 x 64-chunk launch (257 x 257 columns x 49 rows, each computed once), times the
+    minimal instruction recipe of one sample (VOL_OCTAVE_INSTR). Peak: 4 warp instructions per
+    clock per SM (32 threads each) at the SM clock sampled during the timed steps; the FP64
+    pipe (64 lanes per SM per clock) is reported beside it. The reference port's eager volume
+    path (both branches of every choice node over a whole volume) samples more per point;
+    its count (oracle/count_ops.py) is given beside."""
     try:
         with open(OP_COUNTS) as f:
             oc = json.load(f)
     except OSError:
         return None
-    per_point = oc['per_chunk']['corners']['vol_octave'] / (25 * 49)
+    per_point = sum(oc['kernels']['per_kernel']['corner']['samples_per_unit'].values())
+    port_per_point = (oc['per_chunk']['corners']['vol_octave'] + oc['per_chunk']['corners']['point_octave']) / (25 * 49)
     side = int(round(n ** 0.5))
     points = (side * 4 + 1) ** 2 * 49
     samples = points * per_point
-    instr = samples * sum(VOL_OCTAVE_INSTR.values())
+    per_sample = sum(VOL_OCTAVE_INSTR.values())
+    instr = samples * per_sample
     launch_ms = sum(t['corner_ms'] for t in stats) / len(stats)
     mhz = clocks.get('sm_mhz') or 1965.0
     peak = sms * 4 * 32 * mhz * 1e6 / 1e12                      # T thread-instructions / s
     achieved = instr / (launch_ms / 1000.0) / 1e12
     fp64_peak = sms * 64 * mhz * 1e6 / 1e12
     fp64 = samples * VOL_OCTAVE_INSTR['fp64'] / (launch_ms / 1000.0) / 1e12
-    return {'bound': 'issue', 'kernel': 'corner (k_dyn<body_corner>)', 'achieved': round(achieved, 3), 'peak': round(peak, 3),
+    return {'bound': 'issue', 'kernel': 'corner (k_body<&body_corner>)', 'achieved': round(achieved, 3), 'peak': round(peak, 3),
             'unit': 'T thread-instructions/s', 'frac': round(achieved / peak, 4), 'traffic': None, 'launch_ms': round(launch_ms, 3),
-            'octave_samples_per_launch': int(samples), 'instructions_per_sample': VOL_OCTAVE_INSTR,
+            'octave_samples_per_launch': int(samples), 'samples_per_corner_point': round(per_point, 3),
+            'port_samples_per_corner_point': round(port_per_point, 3), 'instructions_per_sample': VOL_OCTAVE_INSTR,
             'fp64_pipe': {'achieved': round(fp64, 3), 'peak': round(fp64_peak, 3), 'frac': round(fp64 / fp64_peak, 4), 'unit': 'T FP64 ops/s'},
             'peak_source': 'issue rate at the sampled SM clock (%s MHz), %d SMs' % (mhz, sms),
-            'note': 'samples = %.1f volume octave samples per corner point (the reference port\'s corner phase: %.0f per chunk over '
-                    '25 x 49 points, counting build) x %d distinct corner points of one %d-chunk launch' %
-                    (per_point, oc['per_chunk']['corners']['vol_octave'], points, n)}
+            'note': '%.2f octave samples per corner point (counted on the kernel bodies) x %d distinct corner points of one %d-chunk launch '
+                    'x %d instructions per sample; the DRAM traffic is negligible (the kernel reads L2-resident tables)' %
+                    (per_point, points, n, per_sample)}
 
 
 def run_ours(args, rank, world, local_rank):

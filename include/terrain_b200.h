@@ -33,7 +33,8 @@ typedef enum tg_status {
     TG_ERR_NO_SEED = 6,           /* tg_generate before tg_set_seed */
     TG_ERR_DEVICE_TIMEOUT = 7,    /* a bounded device-side wait expired */
     TG_ERR_INTERNAL = 8,
-    TG_ERR_IO = 9                 /* a region file could not be written */
+    TG_ERR_IO = 9,                /* a region file could not be written */
+    TG_ERR_CANCELLED = 10         /* tg_server_wait: the request was cancelled (tg_server_cancel) */
 } tg_status;
 
 /* reference: mcc::cuda::ChunkXZ (cuda/include/mccuda_cuda/generator.h:14-16) */
@@ -108,8 +109,8 @@ tg_status tg_generate_u8(struct tg_generator* gen, const tg_chunk_xz* chunks, in
  *     min_y}, then 8 bytes per block column row-major over the region: u8 top state (highest
  *     non-air block), u8 floor state (first non-fluid block at or below it), u8 fluid depth
  *     (at most 255), u8 0, int16 top y, int16 floor y.
- * region in [1, 2048] (the top-down map of 2,048 is 8.6 GB of host memory); TG_ERR_IO when a
- * file cannot be written.
+ * region in [1, 2048]; the files are written a slab of chunk rows at a time (host memory of at
+ * most 4,096 chunks' outputs); TG_ERR_IO when a file cannot be written.
  * reference: write_dump (bench/bench_main.cpp:170-187) and write_topdown (:134-165); the dump
  * is what the client maps (client/src/main/java/mccuda/client/GpuDump.java:88-104) */
 tg_status tg_write_region(struct tg_generator* gen, int64_t seed, int32_t x0, int32_t z0, int32_t region, const char* dump_dir,
@@ -143,6 +144,25 @@ typedef struct tg_request {
 } tg_request;
 tg_status tg_generate_batch(struct tg_generator* gen, const tg_request* requests, int32_t n, tg_timing* timing);
 
+/* Device-resident multi-seed batch: every request's chunk list and outputs are device
+ * memory (outputs 16-byte aligned). The requests become one device work queue of
+ * (chunk, seed) items; each iteration takes the next batch of at most max_batch_chunks
+ * items, runs the TERRAIN step on it and copies each chunk's outputs to its request. By
+ * default the iterations run as a loop on the device: one CUDA-graph launch (a WHILE
+ * conditional node) drains the whole queue with no host round trip between batches;
+ * TG_BATCH_HOST_LOOP launches one graph per batch from the host instead (same kernels).
+ * Requests with more than 256 distinct seeds go in groups, one launch per group. Returns
+ * when the work is done. No counterpart in the reference (single seed per generator). */
+typedef struct tg_request_device {
+    int64_t seed;
+    const tg_chunk_xz* chunks;   /* device memory, count entries */
+    int32_t count;
+    uint16_t* blocks_out;        /* device memory, count * 16 * 16 * height u16 */
+    uint8_t* biomes_out;         /* device memory, count * 16 * height / 4 u8, or NULL */
+} tg_request_device;
+#define TG_BATCH_HOST_LOOP 1
+tg_status tg_generate_batch_device(struct tg_generator* gen, const tg_request_device* requests, int32_t n, int32_t flags, tg_timing* timing);
+
 /* BiomeManager.getBiome at block positions (xyz triples) for one seed per position,
  * with the chunk's R-tree chain exactly as the TERRAIN step computes it.
  * reference semantics: zoomed_biome over cpu_chunk_biomes (cpu/src/biome.cpp:272-289,
@@ -167,23 +187,27 @@ tg_status tg_biome_lookup_noalloc(struct tg_generator* gen, const int32_t* xyz, 
 
 /* ---- serving: continuous batching ---------------------------------------------------
  * A server owns its generator (which then rejects direct calls until the server is
- * destroyed). A worker thread admits submitted requests while the chunks in flight stay
- * within the HBM-derived limit, cuts device batches across all admitted requests (seeds
- * and request sizes mixed), and copies each batch out on a second stream while the next
- * one computes; per-seed tables stay resident on the device. Results are byte-identical
- * to tg_generate for the same seed and chunks, alone or in any mix.
- * No counterpart in the reference (it has no serving form). */
+ * destroyed). A worker thread admits submitted requests while the chunks in flight, priced
+ * at the HBM a chunk of batch capacity takes (tg_server_stats.device_bytes_per_chunk), stay
+ * within the budget; it cuts device batches across all admitted requests (seeds, request
+ * sizes and output forms mixed), and copies each batch out on a second stream while the
+ * next one computes; per-seed tables stay resident on the device. Results are
+ * byte-identical to tg_generate / tg_generate_u8 for the same seed and chunks, alone or in
+ * any mix. No counterpart in the reference (it has no serving form). */
 typedef struct tg_server_config {
     int32_t batch_chunks;       /* chunks per device batch (<= max_batch_chunks); 0 = max_batch_chunks */
-    int64_t hbm_budget_bytes;   /* output bytes admitted but not yet issued; 0 = 8 batches */
+    int64_t hbm_budget_bytes;   /* device memory of the chunks admitted and not yet issued; 0 = 8 batches */
     int32_t reserved;
 } tg_server_config;
 
 typedef struct tg_server_stats {
     int64_t completed_requests, completed_chunks;
-    double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> last byte on the host */
+    double p50_ms, p99_ms, mean_ms, max_ms;  /* submit -> last byte on the host, completed requests */
     double chunks_per_s;                     /* completed chunks / (first submit -> last completion) */
     int32_t batches, queued_requests, active_requests;
+    int64_t cancelled_requests;
+    double device_bytes_per_chunk;           /* HBM per chunk of batch capacity (admission price) */
+    int64_t max_active_chunks;               /* the budget in chunks */
 } tg_server_stats;
 
 tg_status tg_server_create(struct tg_generator* gen, const tg_server_config* config, struct tg_server** out);
@@ -191,13 +215,48 @@ tg_status tg_server_create(struct tg_generator* gen, const tg_server_config* con
  * are host buffers that must stay valid until the request completes. Non-blocking. */
 tg_status tg_server_submit(struct tg_server* srv, int64_t seed, const tg_chunk_xz* chunks, int32_t count, uint16_t* blocks_out, uint8_t* biomes_out,
                            uint64_t* ticket);
+/* The same in the reference generator's u8 form: terrain_out holds count * 16 * 16 * height
+ * u8 palette indices (the u16 states narrowed on the GPU), half the bytes to copy. */
+tg_status tg_server_submit_u8(struct tg_server* srv, int64_t seed, const tg_chunk_xz* chunks, int32_t count, uint8_t* terrain_out, uint8_t* biomes_out,
+                              uint64_t* ticket);
 /* *done = 1 once the request's outputs are on the host (the ticket is then released);
- * timeout_ms: 0 polls, < 0 waits without limit. */
+ * timeout_ms: 0 polls, < 0 waits without limit. A cancelled request returns
+ * TG_ERR_CANCELLED once its chunks in flight have landed (the ticket is then released). */
 tg_status tg_server_wait(struct tg_server* srv, uint64_t ticket, int32_t timeout_ms, int32_t* done);
+/* Cancels a request: a queued one is dropped at once, an admitted one issues no more chunks
+ * (its outputs hold only the chunks already in flight); *was_pending (may be NULL) = 0 when
+ * it had already completed, whose result stands. Its buffers must stay valid until
+ * tg_server_wait reports it. */
+tg_status tg_server_cancel(struct tg_server* srv, uint64_t ticket, int32_t* was_pending);
 tg_status tg_server_get_stats(struct tg_server* srv, tg_server_stats* stats);
+/* Latencies (ms, submit -> last byte on the host) of the requests completed since the last
+ * reset, in completion order: up to cap values into ms, their total count into *n. */
+tg_status tg_server_latencies(struct tg_server* srv, double* ms, int32_t cap, int32_t* n);
 tg_status tg_server_reset_stats(struct tg_server* srv);
 /* Finishes the work in flight, then stops the worker. */
 tg_status tg_server_destroy(struct tg_server* srv);
+
+/* ---- launch shapes and per-kernel times (the autotuner's interface) -----------------------
+ * The batch pipeline's kernels run in the shapes of a launch table: the autotuned table
+ * compiled into the library (minecraft-terrain-cuda_b200/tuning/launch_table.txt) unless one
+ * is set here. Text format, one line per kernel, '#' starts a comment:
+ *   <kernel> <threads 32..256, multiple of 32> <blocks_per_sm 1..32> <grab 0..64>
+ *   table_load <2..8>
+ * grab 0 runs the kernel as a grid-stride loop; grab g > 0 as a persistent work queue whose
+ * blocks take runs of g * threads items from a device counter. table_load sizes the dedupe
+ * hash tables (capacity >= table_load x the keys a batch can insert). Kernel names, in
+ * pipeline order: nb_insert nb_resolve climate_col climate_quart chain cc_insert cc_resolve
+ * corner_col corner zoom_table zoom_uniform sg_insert sg_resolve surface_level aquifer_cell
+ * aquifer_query aquifer_skip init_heights fill surface1 block_biome walk_rules
+ * surface_frozen gather (the chain kernel has no work-queue form). Results do not depend
+ * on the table. No counterpart in the reference (its launch shapes are constants). */
+tg_status tg_set_launch_table(struct tg_generator* gen, const char* text);   /* NULL: the compiled-in table */
+/* The table in use, as text (needed: its size with the terminating zero). */
+tg_status tg_get_launch_table(struct tg_generator* gen, char* buf, size_t cap, size_t* needed);
+/* Per-kernel device times of timed batches (those of calls given a tg_timing): writes the
+ * milliseconds and launch counts gathered since the previous call (cap entries, pipeline
+ * order), clears them, and enables (enable = 1) or disables the per-kernel events. */
+tg_status tg_kernel_times(struct tg_generator* gen, int32_t enable, float* ms, int32_t* calls, int32_t cap);
 
 /* Pinned host memory for outputs. reference: alloc_pinned / free_pinned
  * (cuda/include/mccuda_cuda/terrain_gpu.h:62-63) */

@@ -1,0 +1,170 @@
+"""Autotuner of the TERRAIN step's launch shapes (runs on the target GPU).
+
+    python minecraft-terrain-cuda_b200/autotune.py [--out tuning/launch_table.txt] [--report autotune.json]
+
+For every tunable kernel of a batch, in order of its share of the step, it tries launch
+shapes -- threads per block {64, 128, 256}, resident-block grid cap {1 .. 16} blocks per SM
+(at most 2,048 threads per SM), and the kernel form: grid-stride loop (grab 0) or persistent
+work queue taking runs of grab * threads items (grab 1, 2, 4) -- with the other kernels held
+at their current best, measuring the kernel's own CUDA-event time (tg_kernel_times) over
+timed 4,096-chunk batches of the ladder workload (a 64x64-chunk region at the origin and
+one at block -1,000,000), and keeps the fastest. Kernels under 2 % of the step try a
+reduced set. Then the dedupe hash-table load (capacity >= 2 or 4 x the keys) is chosen by
+the whole step's time. The table is written for build.py to compile in, with the step time
+of the default and the tuned table, each timed through the graph-launched device-resident
+form (tg_generate_device).
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import terrain_b200  # noqa: E402
+
+SEED = 0x5445525241494E31
+REGIONS = [(0, 0), (-62500, -62500)]
+THREADS = (64, 128, 256)
+BLOCKS_PER_SM = (1, 2, 3, 4, 6, 8, 12, 16)
+GRABS = (0, 1, 2, 4)
+
+
+def parse(text):
+    table, load = {}, 2
+    for line in text.splitlines():
+        line = line.split('#')[0].split()
+        if not line:
+            continue
+        if line[0] == 'table_load':
+            load = int(line[1])
+        else:
+            table[line[0]] = tuple(int(v) for v in line[1:4])
+    return table, load
+
+
+def fmt(table, load, header=''):
+    lines = [header] if header else []
+    lines.append('table_load %d' % load)
+    lines += ['%s %d %d %d' % ((k,) + table[k]) for k in terrain_b200.KERNELS]
+    return '\n'.join(lines) + '\n'
+
+
+class Bench:
+    def __init__(self, batch=4096):
+        import torch
+        self.torch = torch
+        self.g = terrain_b200.TerrainGenerator(max_batch_chunks=batch)
+        self.g.set_seed(SEED)
+        side = int(round(batch ** 0.5))
+        self.n = side * side
+        self.chunks = [torch.from_numpy(np.array([(x0 + x, z0 + z) for z in range(side) for x in range(side)], np.int32)).cuda() for x0, z0 in REGIONS]
+        self.blocks = torch.empty(self.n * 98304, dtype=torch.int16, device='cuda')
+        self.biomes = torch.empty(self.n * 1536, dtype=torch.uint8, device='cuda')
+
+    def kernel_ms(self, table, load, reps=2):
+        """{kernel: ms per batch}: medians over reps timed batches of each region."""
+        g = self.g
+        g.set_launch_table(fmt(table, load))
+        for c in self.chunks:                                     # warm-up (tables, caches)
+            g.generate_device(c.data_ptr(), self.n, self.blocks.data_ptr(), self.biomes.data_ptr(), timing=False)
+        g.kernel_times(enable=True)
+        per = {k: [] for k in terrain_b200.KERNELS}
+        for _ in range(reps):
+            for c in self.chunks:
+                g.generate_device(c.data_ptr(), self.n, self.blocks.data_ptr(), self.biomes.data_ptr(), timing=True)
+                for k, (ms, calls) in g.kernel_times(enable=True).items():
+                    per[k].append(ms / max(calls, 1))
+        g.kernel_times(enable=False)
+        return {k: float(np.median(v)) for k, v in per.items()}
+
+    def step_ms(self, table, load, reps=5):
+        """Device time of the graph-launched steps (all regions), median of reps."""
+        torch = self.torch
+        g = self.g
+        g.set_launch_table(fmt(table, load))
+        for c in self.chunks:
+            g.generate_device(c.data_ptr(), self.n, self.blocks.data_ptr(), self.biomes.data_ptr(), timing=False)
+        out = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for c in self.chunks:
+                g.generate_device(c.data_ptr(), self.n, self.blocks.data_ptr(), self.biomes.data_ptr(), timing=False)
+            e1.record()
+            torch.cuda.synchronize()
+            out.append(e0.elapsed_time(e1))
+        return float(np.median(out))
+
+
+def candidates(kernel, big):
+    if not big:
+        shapes = [(t, b, 0) for t in (128, 256) for b in (4, 8, 16) if t * b <= 2048]
+    else:
+        shapes = [(t, b, gr) for t in THREADS for b in BLOCKS_PER_SM for gr in GRABS if t * b <= 2048]
+    if kernel == 'chain':
+        shapes = [s for s in shapes if s[2] == 0]
+    return shapes
+
+
+def main(argv):
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--out', default=os.path.join(HERE, 'tuning', 'launch_table.txt'))
+    ap.add_argument('--report', default=None)
+    ap.add_argument('--reps', type=int, default=2)
+    args = ap.parse_args(argv)
+    t_start = time.time()
+    b = Bench()
+    default_text = b.g.launch_table()
+    table, load = parse(default_text)
+    base = dict(table)
+    ms0 = b.kernel_ms(table, load, args.reps)
+    total0 = sum(ms0.values())
+    order = sorted(terrain_b200.KERNELS, key=lambda k: -ms0[k])
+    report = {'kernels': {}, 'default_kernel_ms': ms0}
+    for k in order:
+        big = ms0[k] >= 0.02 * total0
+        best, best_ms, tried = table[k], None, []
+        for shape in candidates(k, big):
+            table[k] = shape
+            ms = b.kernel_ms(table, load, args.reps)[k]
+            tried.append((shape, round(ms, 4)))
+            if best_ms is None or ms < best_ms:
+                best, best_ms = shape, ms
+        table[k] = best
+        report['kernels'][k] = {'default': base[k], 'default_ms': round(ms0[k], 4), 'best': best, 'best_ms': round(best_ms, 4),
+                                'tried': len(tried), 'top': sorted(tried, key=lambda x: x[1])[:5]}
+        print('%-15s %s %.4f ms -> %s %.4f ms (%d shapes)' % (k, base[k], ms0[k], best, best_ms, len(tried)), flush=True)
+    loads = {}
+    for ld in (2, 4):
+        loads[ld] = b.step_ms(table, ld)
+    load = min(loads, key=loads.get)
+    step_default = b.step_ms(base, 2, reps=9)
+    step_tuned = b.step_ms(table, load, reps=9)
+    report.update({'table_load_step_ms': loads, 'table_load': load, 'step_ms_default': round(step_default, 3), 'step_ms_tuned': round(step_tuned, 3),
+                   'regions': REGIONS, 'batch_chunks': b.n, 'seconds': round(time.time() - t_start, 1)})
+    keep_tuned = step_tuned < step_default
+    header = ('# Launch shapes of the TERRAIN step\'s kernels, compiled into libterrain_b200.so by build.py.\n'
+              '# Written by autotune.py on a B200; a line per kernel: name threads blocks_per_sm grab\n'
+              '# (grab 0: grid-stride loop; grab g > 0: persistent work queue, g * threads items per take),\n'
+              '# and table_load: dedupe hash tables of at least table_load x the most keys of a batch.\n'
+              '# Two 64x64-chunk ladder regions, 4,096-chunk batches, graph-launched device step:\n'
+              '# default table %.3f ms, tuned %.3f ms per two batches%s.'
+              % (step_default, step_tuned, '' if keep_tuned else ' (tuned slower: default kept)'))
+    text = fmt(table if keep_tuned else base, load if keep_tuned else 2, header)
+    with open(args.out, 'w') as f:
+        f.write(text)
+    report['kept'] = 'tuned' if keep_tuned else 'default'
+    if args.report:
+        with open(args.report, 'w') as f:
+            json.dump(report, f, indent=1)
+    print(json.dumps({k: report[k] for k in ('step_ms_default', 'step_ms_tuned', 'table_load', 'kept', 'seconds')}))
+    b.g.close()
+
+
+if __name__ == '__main__':
+    main(sys.argv[1:])

@@ -31,11 +31,31 @@ def run(cmd):
     subprocess.check_call(cmd)
 
 
+TUNING = os.path.join(HERE, 'tuning', 'launch_table.txt')
+
+
 def generate():
     sys.path.insert(0, os.path.join(HERE, 'codegen'))
     import gen_eval
-    return gen_eval.generate(os.path.join(MODEL, 'overworld_ir.json'), os.path.join(MODEL, 'overworld_terrain.json'),
-                             os.path.join(GEN, 'model_gen.cuh'))
+    r = gen_eval.generate(os.path.join(MODEL, 'overworld_ir.json'), os.path.join(MODEL, 'overworld_terrain.json'),
+                          os.path.join(GEN, 'model_gen.cuh'))
+    write_launch_table()
+    return r
+
+
+def write_launch_table():
+    """_gen/launch_table.h: the committed launch table as a string constant (parsed by the
+    library at tg_create); rewritten only when its contents change."""
+    with open(TUNING) as f:
+        text = f.read()
+    body = '// generated by build.py from tuning/launch_table.txt\n#pragma once\nnamespace tb {\nstatic const char kLaunchTableText[] =\n'
+    body += ''.join('    "%s\\n"\n' % line.replace('\\', '\\\\').replace('"', '\\"') for line in text.splitlines())
+    body += '    "";\n}  // namespace tb\n'
+    out = os.path.join(GEN, 'launch_table.h')
+    if not os.path.exists(out) or open(out).read() != body:
+        os.makedirs(GEN, exist_ok=True)
+        with open(out, 'w') as f:
+            f.write(body)
 
 
 def newer(target, deps):
@@ -46,7 +66,7 @@ def newer(target, deps):
 
 
 def sources():
-    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(GEN, 'model_gen.cuh')]
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(GEN, 'model_gen.cuh'), os.path.join(GEN, 'launch_table.h')]
 
 
 def build_device(force=False, out=None, defines=()):
@@ -70,7 +90,7 @@ def build_host(force=False):
     deps = sources() + [os.path.join(HERE, '..', 'tests', 'hostcheck', 'hostcheck.cpp')]
     if not force and not newer(out, deps):
         return out
-    run(['g++', '-std=c++17', '-O2', '-ffp-contract=off', '-fno-fast-math', '-fPIC', '-shared', '-I', CSRC, '-I', GEN,
+    run(['g++', '-std=c++17', '-O2', '-ffp-contract=off', '-fno-fast-math', '-fPIC', '-shared', '-DTB_COUNT_OPS', '-I', CSRC, '-I', GEN,
          os.path.join(HERE, '..', 'tests', 'hostcheck', 'hostcheck.cpp'), os.path.join(CSRC, 'tb_host.cpp'), '-o', out])
     return out
 

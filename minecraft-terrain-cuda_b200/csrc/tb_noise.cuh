@@ -241,11 +241,24 @@ TB_HD TB_FI float octave_point_smeared(const NoiseTables& T, int32_t oct, double
 #define TB_NOINLINE
 #endif
 
+// Work counting, in the host build of the test suite only (TB_COUNT_OPS): one count per
+// octave sample (volume, smeared volume, point, smeared point) and per simplex sample,
+// into the array the host twin points tb_op_counts at for the stage it runs. The device
+// build never counts.
+#if defined(TB_COUNT_OPS) && !defined(__CUDA_ARCH__)
+extern thread_local long long* tb_op_counts;
+#define TB_COUNT(kind) (++tb_op_counts[kind])
+#else
+#define TB_COUNT(kind) ((void)0)
+#endif
+enum OpKind { kOpVolume, kOpVolumeSmeared, kOpPoint, kOpPointSmeared, kOpSimplex, kOpKinds };
+
 TB_HD TB_NOINLINE inline float stack_volume_rt(const NoiseTables& T, int first, int count, int32_t bx, int32_t by, int32_t bz, double xzs, double yss,
                                                 float amplitude) {
     float acc = 0.0f;
 #pragma unroll 1
     for (int i = first; i < first + count; ++i) {
+        TB_COUNT(kOpVolume);
         const Layer L = T.layer[i];
         const double xs = xzs * L.freq, ys = yss * L.freq;
         const float amp = amplitude * L.amp;
@@ -259,6 +272,7 @@ TB_HD TB_NOINLINE inline float stack_volume_smeared_rt(const NoiseTables& T, int
     float acc = 0.0f;
 #pragma unroll 1
     for (int i = first; i < first + count; ++i) {
+        TB_COUNT(kOpVolumeSmeared);
         const Layer L = T.layer[i];
         const double xs = xzs * L.freq, ys = yss * L.freq;
         const float amp = amplitude * L.amp;
@@ -271,6 +285,7 @@ TB_HD TB_NOINLINE inline float stack_point_rt(const NoiseTables& T, int first, i
     float acc = 0.0f;
 #pragma unroll 1
     for (int i = first; i < first + count; ++i) {
+        TB_COUNT(kOpPoint);
         const Layer L = T.layer[i];
         const double f = L.freq;
         acc = acc + L.amp * octave_point(T, L.oct, x * f, y * f, z * f);
@@ -282,6 +297,7 @@ TB_HD TB_NOINLINE inline float stack_point_smeared_rt(const NoiseTables& T, int 
     float acc = 0.0f;
 #pragma unroll 1
     for (int i = first; i < first + count; ++i) {
+        TB_COUNT(kOpPointSmeared);
         const Layer L = T.layer[i];
         const double f = L.freq;
         acc = acc + L.amp * octave_point_smeared(T, L.oct, x * f, y * f, z * f);
@@ -319,6 +335,7 @@ TB_HD TB_FI double simplex_corner(int g, double x, double y) {
 
 // f2 = (sqrt(3) - 1) / 2, g2 = (3 - sqrt(3)) / 6 as computed in double.
 TB_HD TB_FI float simplex2(const Simplex2& s, double px, double py, double f2, double g2) {
+    TB_COUNT(kOpSimplex);
     const double xin = px + s.ox, yin = py + s.oy;
     const double sk = (xin + yin) * f2;
     const int32_t i = jfloor(xin + sk), j = jfloor(yin + sk);

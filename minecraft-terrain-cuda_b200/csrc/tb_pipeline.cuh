@@ -94,7 +94,13 @@ struct HashTab {
     int32_t* count;
     uint32_t mask;
     int32_t* owner;             // per slot: least inserting item (INT32_MAX-like when free)
+    uint32_t* err;              // sticky error bits of the lane: kErrTableFull, kErrKeyMissing
 };
+// Device-side error bits, read by the host after the work: the tables are sized so that
+// neither can happen (capacity >= 2 x the keys a batch can insert); they turn a broken
+// invariant into an error status instead of a silent wrong index.
+constexpr uint32_t kErrTableFull = 1u;    // an insert's probe sequence met no free slot
+constexpr uint32_t kErrKeyMissing = 2u;   // a resolve did not find its key (index 0 used instead)
 constexpr unsigned long long kEmpty = ~0ull;
 
 // One aquifer grid cell (NoiseBasedAquifer's aquiferLocationCache and aquiferCache entries
@@ -208,6 +214,13 @@ TB_HD TB_FI void min32(int32_t* p, int32_t v) {
     if (v < *p) *p = v;
 #endif
 }
+TB_HD TB_FI void or32(uint32_t* p, uint32_t v) {
+#if defined(__CUDA_ARCH__)
+    atomicOr(p, v);
+#else
+    *p |= v;
+#endif
+}
 TB_HD TB_FI void max32(int32_t* p, int32_t v) {
 #if defined(__CUDA_ARCH__)
     atomicMax(p, v);
@@ -234,6 +247,7 @@ TB_HD inline void ht_insert(const HashTab& t, unsigned long long key, int32_t it
         }
         s = (s + 1) & t.mask;
     }
+    or32(t.err, kErrTableFull);
 }
 
 // The slot holding key (inserted), or the table size when absent.
@@ -269,6 +283,15 @@ TB_HD inline int32_t ht_find(const HashTab& t, unsigned long long key) {
     return -1;
 }
 
+// ht_find for an inserted key; a missing one sets kErrKeyMissing and gives index 0, so
+// that no later access goes out of bounds.
+TB_HD TB_FI int32_t ht_resolve(const HashTab& t, unsigned long long key) {
+    const int32_t v = ht_find(t, key);
+    if (v >= 0) return v;
+    or32(t.err, kErrKeyMissing);
+    return 0;
+}
+
 // Keys: 27-bit offset coordinates (|v| < 2^26), a semantics bit and a 9-bit seed slot.
 constexpr int64_t kKeyBias = 1ll << 26;
 TB_HD TB_FI unsigned long long pack_key(int32_t slot, int32_t a, int32_t b, int32_t sem) {
@@ -291,14 +314,14 @@ TB_HD TB_FI unsigned long long nb_key(const Batch& B, int i) {
     return pack_key(B.cseed[c], B.cx[c] + k % 3 - 1, B.cz[c] + k / 3 - 1, 0);
 }
 TB_HD inline void body_nb_insert(const Batch& B, int i) { ht_insert(B.hb, nb_key(B, i), i); }
-TB_HD inline void body_nb_resolve(const Batch& B, int i) { B.nb9[i] = ht_find(B.hb, nb_key(B, i)); }
+TB_HD inline void body_nb_resolve(const Batch& B, int i) { B.nb9[i] = ht_resolve(B.hb, nb_key(B, i)); }
 // corner columns in quart units (item = chunk * 25 + k * 5 + i)
 TB_HD TB_FI unsigned long long cc_key(const Batch& B, int it) {
     const int c = it / 25, k = (it % 25) / 5, i = it % 5;
     return pack_key(B.cseed[c], B.cx[c] * 4 + i, B.cz[c] * 4 + k, 0);
 }
 TB_HD inline void body_cc_insert(const Batch& B, int it) { ht_insert(B.hc, cc_key(B, it), it); }
-TB_HD inline void body_cc_resolve(const Batch& B, int it) { B.c25[it] = ht_find(B.hc, cc_key(B, it)); }
+TB_HD inline void body_cc_resolve(const Batch& B, int it) { B.c25[it] = ht_resolve(B.hc, cc_key(B, it)); }
 // surface-level quarts: 27 x 19 per chunk; the 11 x 11 window of the aquifer's
 // constructor uses volume semantics (sem 1), the rest the lazy point path (sem 0).
 TB_HD TB_FI unsigned long long sg_key(const Batch& B, int c, int g) {
@@ -309,7 +332,7 @@ TB_HD TB_FI unsigned long long sg_key(const Batch& B, int c, int g) {
 }
 TB_HD TB_FI unsigned long long sg_key_item(const Batch& B, int it) { return sg_key(B, it / kGrid, it % kGrid); }
 TB_HD inline void body_sg_insert(const Batch& B, int it) { ht_insert(B.hs, sg_key_item(B, it), it); }
-TB_HD inline void body_sg_resolve(const Batch& B, int it) { B.g513[it] = ht_find(B.hs, sg_key(B, it / kGrid, it % kGrid)); }
+TB_HD inline void body_sg_resolve(const Batch& B, int it) { B.g513[it] = ht_resolve(B.hs, sg_key(B, it / kGrid, it % kGrid)); }
 
 // ---- biomes -------------------------------------------------------------------------------------
 // chain position p -> quart (qx, qy, qz): vanilla order sections, x, y, z

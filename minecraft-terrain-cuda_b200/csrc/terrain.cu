@@ -40,6 +40,7 @@
 #include <vector>
 
 #include "../../include/terrain_b200.h"
+#include "launch_table.h"   // generated from tuning/launch_table.txt: kLaunchTableText
 #include "tb_pipeline.cuh"
 
 namespace tb {
@@ -79,18 +80,34 @@ double now_ms() { return std::chrono::duration<double, std::milli>(std::chrono::
 #define TB_MINB_QUART 4
 #endif
 
-// item count = chunks in the batch * MUL
+// The per-item bodies of a batch run in one of two kernel forms, chosen per kernel by the
+// launch table (an autotuned, committed table; see launch_shape below). Items number
+// *count * MUL (count: the batch's chunk count or a device-side dedupe count).
+//   k_body    grid-stride loop: thread t takes items t, t + grid, ...
+//   k_body_q  persistent work queue: each block takes runs of grab * blockDim.x consecutive
+//             items from a device counter (one atomicAdd per run) until the items run out,
+//             so blocks that meet cheap items take more of them. Consecutive items stay on
+//             consecutive lanes, as in the stride form.
 template <void (*F)(const Batch&, int), int MUL, int MINB = 1>
-__global__ void __launch_bounds__(256, MINB) k_items(const __grid_constant__ Batch B) {
-    const int n = *B.n_dev * MUL;
+__global__ void __launch_bounds__(256, MINB) k_body(const __grid_constant__ Batch B, const int32_t* count) {
+    const int n = *count * MUL;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) F(B, i);
 }
 
-// item count = *count * MUL (a device-side dedupe count)
 template <void (*F)(const Batch&, int), int MUL, int MINB = 1>
-__global__ void __launch_bounds__(256, MINB) k_dyn(const __grid_constant__ Batch B, const int32_t* count) {
+__global__ void __launch_bounds__(256, MINB) k_body_q(const __grid_constant__ Batch B, const int32_t* count, int32_t* next, int grab) {
     const int n = *count * MUL;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) F(B, i);
+    const int run = grab * static_cast<int>(blockDim.x);
+    __shared__ int32_t base;
+    for (;;) {
+        if (threadIdx.x == 0) base = atomicAdd(next, run);
+        __syncthreads();
+        const int b = base;
+        __syncthreads();   // every thread has read base before thread 0 takes the next run
+        if (b >= n) break;
+        const int end = min(n, b + run);
+        for (int i = b + static_cast<int>(threadIdx.x); i < end; i += blockDim.x) F(B, i);
+    }
 }
 
 // Numbers the keys of one dedupe stage (TAB 0 biome chunks, 1 corner columns, 2 surface
@@ -141,10 +158,7 @@ __global__ void __launch_bounds__(256) k_number(const __grid_constant__ Batch B)
     }
 }
 
-__global__ void k_init_heights(const __grid_constant__ Batch B) {
-    const int n = *B.n_dev * 256;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) B.h0[i] = tbm::kMinY;
-}
+__device__ __forceinline__ void body_init_heights(const Batch& B, int i) { B.h0[i] = tbm::kMinY; }
 
 __global__ void k_split_chunks(const tg_chunk_xz* ch, int n, int32_t slot, int32_t* cx, int32_t* cz, int32_t* cs, int32_t* n_dev) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -386,6 +400,99 @@ __global__ void k_topdown(const uint16_t* blocks, const uint8_t* flags, int n, i
     }
 }
 
+// ---- device work queue of the device-resident multi-seed batch ----------------------------------
+// The whole request list sits in HBM as a queue of (chunk, seed slot, request, index) items.
+// Each iteration of a batch takes the next at most `cap` items (k_queue_take), runs the
+// TERRAIN step on them, copies each chunk's outputs to its request's buffers
+// (k_queue_scatter) and advances the queue (k_queue_advance), which also decides whether
+// another iteration follows: inside one CUDA graph that decision is the condition of a
+// WHILE node, so a whole request list runs from one graph launch.
+struct QueueReq {                    // one request of the list
+    const tg_chunk_xz* chunks;       // device memory
+    uint16_t* blocks;                // device memory, 16-byte aligned
+    uint8_t* biomes;                 // device memory, 16-byte aligned, or null
+    int32_t first, count, slot, pad;
+};
+struct QueueView {
+    const QueueReq* req;
+    int32_t* cx;                     // items: chunk x, z, seed slot, request, index in the request
+    int32_t* cz;
+    int32_t* cs;
+    int32_t* rq;
+    int32_t* ix;
+    int32_t* state;                  // head, total, iterations, iteration limit, items of the batch in flight
+    int32_t n_req;
+};
+
+// The items of every request (one thread per item; the request found by binary search over
+// the requests' first items).
+__global__ void k_queue_fill(QueueView Q) {
+    const int total = Q.state[1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        int lo = 0, hi = Q.n_req - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (Q.req[mid].first <= i) lo = mid;
+            else hi = mid - 1;
+        }
+        const QueueReq& r = Q.req[lo];
+        const int j = i - r.first;
+        Q.cx[i] = r.chunks[j].x;
+        Q.cz[i] = r.chunks[j].z;
+        Q.cs[i] = r.slot;
+        Q.rq[i] = lo;
+        Q.ix[i] = j;
+    }
+}
+
+// The next batch: items [head, head + n), n = min(cap, total - head), into the batch's chunk
+// arrays and its device-side count.
+__global__ void k_queue_take(QueueView Q, int cap, int32_t* cx, int32_t* cz, int32_t* cs, int32_t* n_dev) {
+    const int head = Q.state[0];
+    const int n = max(0, min(cap, Q.state[1] - head));
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        cx[i] = Q.cx[head + i];
+        cz[i] = Q.cz[head + i];
+        cs[i] = Q.cs[head + i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *n_dev = n;
+        Q.state[4] = n;
+    }
+}
+
+// Each chunk of the batch in flight to its request's output buffers, 16 bytes per thread
+// (12,288 of the blocks and 96 of the biomes per chunk).
+constexpr int kScatterBlockVecs = kBlocksPerChunk * 2 / 16, kScatterBiomeVecs = kQuartsPerChunk / 16;
+__global__ void k_queue_scatter(QueueView Q, const uint4* blocks, const uint4* biomes) {
+    const int head = Q.state[0], n = Q.state[4];
+    constexpr int per = kScatterBlockVecs + kScatterBiomeVecs;
+    const long total = static_cast<long>(n) * per;
+    for (long t = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; t < total; t += static_cast<long>(gridDim.x) * blockDim.x) {
+        const int c = static_cast<int>(t / per), k = static_cast<int>(t % per);
+        const QueueReq& r = Q.req[Q.rq[head + c]];
+        const size_t j = static_cast<size_t>(Q.ix[head + c]);
+        if (k < kScatterBlockVecs) {
+            reinterpret_cast<uint4*>(r.blocks)[j * kScatterBlockVecs + k] = blocks[static_cast<size_t>(c) * kScatterBlockVecs + k];
+        } else if (r.biomes) {
+            const int b = k - kScatterBlockVecs;
+            reinterpret_cast<uint4*>(r.biomes)[j * kScatterBiomeVecs + b] = biomes[static_cast<size_t>(c) * kScatterBiomeVecs + b];
+        }
+    }
+}
+
+// Advances the queue past the batch in flight; with a graph loop, sets its condition: another
+// iteration while items remain and the iteration limit (more than the list needs) is not
+// reached. The head grows by at least one item per iteration that has items, so the loop ends.
+__global__ void k_queue_advance(QueueView Q, cudaGraphConditionalHandle h, int looped) {
+    const int head = Q.state[0] + Q.state[4];
+    const int iters = Q.state[2] + 1;
+    Q.state[0] = head;
+    Q.state[2] = iters;
+    Q.state[4] = 0;
+    if (looped) cudaGraphSetConditional(h, (head < Q.state[1] && iters < Q.state[3]) ? 1u : 0u);
+}
+
 // ---- scratch of the no-allocation biome lookup ---------------------------------------------------
 // tg_biome_lookup_noalloc stages its positions and results in this fixed device array
 // instead of device buffers allocated per call. Callers that cannot allocate device memory
@@ -453,6 +560,72 @@ void launch(K kernel, cudaStream_t s, long items_hint, Args... args) {
     ++g_launches;
 }
 
+// ---- launch shapes ------------------------------------------------------------------------------
+// The tunable kernels of a batch, in pipeline order. Their shapes come from a launch table:
+// the committed, autotuned table compiled in (tuning/launch_table.txt) or one set at run
+// time (tg_set_launch_table). A line "kernel threads blocks_per_sm grab" per kernel (grab 0:
+// grid-stride form; grab g > 0: work-queue form taking g * threads items per run), and
+// "table_load f": dedupe hash tables of at least f times the most keys a batch can insert
+// (rounded up to a power of two).
+enum KernelId {
+    K_NB_INSERT, K_NB_RESOLVE, K_CLIMATE_COL, K_CLIMATE_QUART, K_CHAIN, K_CC_INSERT, K_CC_RESOLVE, K_CORNER_COL, K_CORNER, K_ZOOM_TABLE,
+    K_ZOOM_UNIFORM, K_SG_INSERT, K_SG_RESOLVE, K_SURFACE_LEVEL, K_AQ_CELL, K_AQ_QUERY, K_AQ_SKIP, K_INIT_HEIGHTS, K_FILL, K_SURFACE1,
+    K_BLOCK_BIOME, K_WALK, K_FROZEN, K_GATHER, K_COUNT
+};
+const char* const kKernelNames[K_COUNT] = {"nb_insert", "nb_resolve", "climate_col", "climate_quart", "chain", "cc_insert", "cc_resolve",
+                                           "corner_col", "corner", "zoom_table", "zoom_uniform", "sg_insert", "sg_resolve", "surface_level",
+                                           "aquifer_cell", "aquifer_query", "aquifer_skip", "init_heights", "fill", "surface1", "block_biome",
+                                           "walk_rules", "surface_frozen", "gather"};
+
+struct LaunchShape {
+    int threads = 256;        // 32 .. 256, a multiple of 32 (the kernels are built for at most 256)
+    int blocks_per_sm = 8;    // grid = min(blocks for the items, blocks_per_sm * SMs)
+    int grab = 0;             // 0: grid-stride; > 0: work queue, grab * threads items per run
+};
+struct LaunchTable {
+    LaunchShape k[K_COUNT];
+    int table_load = 2;
+};
+
+// Parses a launch table; unknown kernels, bad values and malformed lines are errors.
+LaunchTable parse_launch_table(const std::string& text) {
+    LaunchTable t;
+    std::istringstream in(text);
+    std::string line;
+    int ln = 0;
+    while (std::getline(in, line)) {
+        ++ln;
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line.resize(hash);
+        std::istringstream ls(line);
+        std::string name;
+        if (!(ls >> name)) continue;
+        auto bad = [&](const char* why) { throw Error(TG_ERR_INVALID_ARGUMENT, "launch table line " + std::to_string(ln) + ": " + why); };
+        if (name == "table_load") {
+            if (!(ls >> t.table_load) || t.table_load < 2 || t.table_load > 8) bad("table_load must be 2..8");
+            continue;
+        }
+        int id = -1;
+        for (int i = 0; i < K_COUNT; ++i)
+            if (name == kKernelNames[i]) id = i;
+        if (id < 0) bad("unknown kernel");
+        LaunchShape& k = t.k[id];
+        if (!(ls >> k.threads >> k.blocks_per_sm >> k.grab)) bad("expected: kernel threads blocks_per_sm grab");
+        if (k.threads < 32 || k.threads > 256 || k.threads % 32) bad("threads must be a multiple of 32 in 32..256");
+        if (k.blocks_per_sm < 1 || k.blocks_per_sm > 32) bad("blocks_per_sm must be 1..32");
+        if (k.grab < 0 || k.grab > 64) bad("grab must be 0..64");
+        if (id == K_CHAIN && k.grab) bad("the chain kernel has no work-queue form");
+    }
+    return t;
+}
+
+std::string format_launch_table(const LaunchTable& t) {
+    std::ostringstream o;
+    o << "table_load " << t.table_load << "\n";
+    for (int i = 0; i < K_COUNT; ++i) o << kKernelNames[i] << ' ' << t.k[i].threads << ' ' << t.k[i].blocks_per_sm << ' ' << t.k[i].grab << "\n";
+    return o.str();
+}
+
 uint32_t pow2_at_least(uint64_t v) {
     uint32_t p = 1024;
     while (p < v) p <<= 1;
@@ -503,8 +676,9 @@ struct PinBuf {
 struct TableBufs {
     DevBuf keys, vals, uniq, count, owner;
     uint32_t cap = 0;
-    void alloc(uint64_t max_keys) {
-        cap = pow2_at_least(2 * max_keys);
+    uint32_t* err = nullptr;   // the lane's error word (Work::d_err)
+    void alloc(uint64_t max_keys, int load) {
+        cap = pow2_at_least(static_cast<uint64_t>(load) * max_keys);
         keys.alloc(sizeof(unsigned long long) * cap);
         vals.alloc(sizeof(int32_t) * cap);
         owner.alloc(sizeof(int32_t) * cap);
@@ -512,7 +686,7 @@ struct TableBufs {
         count.alloc(sizeof(int32_t));
     }
     HashTab view() const {
-        return HashTab{keys.as<unsigned long long>(), vals.as<int32_t>(), uniq.as<unsigned long long>(), count.as<int32_t>(), cap - 1, owner.as<int32_t>()};
+        return HashTab{keys.as<unsigned long long>(), vals.as<int32_t>(), uniq.as<unsigned long long>(), count.as<int32_t>(), cap - 1, owner.as<int32_t>(), err};
     }
     // free slots; owners above every item index (0x7F7F7F7F)
     void reset(cudaStream_t s) const {
@@ -549,17 +723,21 @@ struct OutSlot {
 // two output slots run concurrently on two streams.
 struct Work {
     DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_cell,
-        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_zoom_uni, d_bbiome, d_oremask, d_colmask, d_colrec;
+        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_zoom_uni, d_bbiome, d_oremask, d_colmask, d_colrec, d_qnext, d_err;
     TableBufs tb_b, tb_c, tb_s;
-    void alloc(int n) {
+    void alloc(int n, int load) {
         const size_t N = static_cast<size_t>(n);
         d_n.alloc(sizeof(int32_t));
+        d_err.alloc(sizeof(uint32_t));
+        ck(cudaMemset(d_err.p, 0, sizeof(uint32_t)), "memset");
+        tb_b.err = tb_c.err = tb_s.err = d_err.as<uint32_t>();
+        d_qnext.alloc(sizeof(int32_t) * K_COUNT);   // work-queue counters, one per kernel
         d_cx.alloc(4 * N);
         d_cz.alloc(4 * N);
         d_cs.alloc(4 * N);
-        tb_b.alloc(9 * N);
-        tb_c.alloc(25 * N);
-        tb_s.alloc(static_cast<uint64_t>(kGrid) * N);
+        tb_b.alloc(9 * N, load);
+        tb_c.alloc(25 * N, load);
+        tb_s.alloc(static_cast<uint64_t>(kGrid) * N, load);
         const size_t nb = 9 * N, cc = 25 * N, sg = static_cast<size_t>(kGrid) * N;
         d_nb9.alloc(4 * 9 * N);
         d_bcol.alloc(sizeof(float) * nb * 16 * tbm::kClimateCols);
@@ -638,6 +816,14 @@ struct Generator {
     OutSlot out[2];
     int next_out = 0;
     int graph_launches = 0;
+    LaunchTable lt = parse_launch_table(kLaunchTableText);
+    // per-kernel event times of timed batches (tg_kernel_times); prof_now while a timed
+    // batch is being enqueued with prof set
+    bool prof = false, prof_now = false;
+    cudaEvent_t prof_ev[2 * K_COUNT] = {};
+    bool prof_marked[K_COUNT] = {};
+    double prof_ms[K_COUNT] = {};
+    int prof_calls[K_COUNT] = {};
 
     Generator(int dev, int batch, int pipeline_slots) : device(dev), max_batch(batch), lanes(pipeline_slots == 1 ? 1 : 2) {
         ck(cudaSetDevice(device), "cudaSetDevice");
@@ -651,6 +837,7 @@ struct Generator {
         stream = own_stream;
         out[1].lane = lanes == 2 ? 1 : 0;
         for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+        for (auto& e : prof_ev) ck(cudaEventCreate(&e), "cudaEventCreate");
         for (auto& o : out) {
             ck(cudaEventCreateWithFlags(&o.computed, cudaEventDisableTiming), "cudaEventCreate");
             ck(cudaEventCreateWithFlags(&o.drained, cudaEventDisableTiming), "cudaEventCreate");
@@ -663,12 +850,15 @@ struct Generator {
     ~Generator() {
         cudaSetDevice(device);
         cudaDeviceSynchronize();
+        destroy_queue_graphs();
         for (auto& o : out) {
             if (o.graph) cudaGraphExecDestroy(o.graph);
             if (o.computed) cudaEventDestroy(o.computed);
             if (o.drained) cudaEventDestroy(o.drained);
         }
         for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        for (auto& e : prof_ev)
             if (e) cudaEventDestroy(e);
         if (ev_entry) cudaEventDestroy(ev_entry);
         if (lane_stream) cudaStreamDestroy(lane_stream);
@@ -725,12 +915,28 @@ struct Generator {
 
     void alloc_batch(int n) {
         const size_t N = static_cast<size_t>(n);
-        for (int l = 0; l < lanes; ++l) work[l].alloc(n);
+        for (int l = 0; l < lanes; ++l) work[l].alloc(n, lt.table_load);
         for (auto& o : out) {
             o.blocks.alloc(sizeof(uint16_t) * N * kBlocksPerChunk);
             o.biomes.alloc(N * kQuartsPerChunk);
             o.coords.alloc(sizeof(int32_t) * (3 * N + 1));
         }
+    }
+
+    // HBM the batch buffers take per chunk of batch capacity: both lanes' working buffers and
+    // both output slots (u16 blocks and biomes, and their u8 copies once allocated)
+    double device_bytes_per_chunk() const {
+        size_t b = 0;
+        for (int l = 0; l < lanes; ++l) {
+            const Work& W = work[l];
+            for (const DevBuf* d : {&W.d_cx, &W.d_cz, &W.d_cs, &W.d_nb9, &W.d_bcol, &W.d_tgt, &W.d_lstar, &W.d_mdist, &W.d_qbiome, &W.d_c25, &W.d_ccol,
+                                    &W.d_corners, &W.d_g513, &W.d_sfts, &W.d_aq_cell, &W.d_aq_query, &W.d_aq_skip, &W.d_h0, &W.d_h1, &W.d_h2,
+                                    &W.d_zoom, &W.d_zoom_uni, &W.d_bbiome, &W.d_oremask, &W.d_colmask, &W.d_colrec})
+                b += d->bytes;
+            for (const TableBufs* t : {&W.tb_b, &W.tb_c, &W.tb_s}) b += t->keys.bytes + t->vals.bytes + t->uniq.bytes + t->owner.bytes;
+        }
+        for (const OutSlot& o : out) b += o.blocks.bytes + o.biomes.bytes + o.blocks8.bytes;
+        return static_cast<double>(b) / static_cast<double>(max_batch);
     }
 
     // Resident per-seed tables: the slot of a seed, built and uploaded on a miss; slots
@@ -845,20 +1051,48 @@ struct Generator {
         return B;
     }
 
+    // One tunable body kernel in the shape the launch table gives it; items_hint (an upper
+    // bound of the items) sizes the grid, count (device memory) x MUL is the item count.
+    template <void (*F)(const Batch&, int), int MUL, int MINB = 1>
+    void run_body(KernelId id, const Work& W, cudaStream_t s, long items_hint, const Batch& B, const int32_t* count) {
+        const LaunchShape& k = lt.k[id];
+        long blocks = (items_hint + k.threads - 1) / k.threads;
+        blocks = std::max(1L, std::min(blocks, static_cast<long>(g_sm_count) * k.blocks_per_sm));
+        if (prof_now) ck(cudaEventRecord(prof_ev[2 * id], s), "event");
+        if (k.grab > 0)
+            k_body_q<F, MUL, MINB><<<static_cast<unsigned>(blocks), k.threads, 0, s>>>(B, count, W.d_qnext.as<int32_t>() + id, k.grab);
+        else
+            k_body<F, MUL, MINB><<<static_cast<unsigned>(blocks), k.threads, 0, s>>>(B, count);
+        ++g_launches;
+        if (prof_now) {
+            ck(cudaEventRecord(prof_ev[2 * id + 1], s), "event");
+            prof_marked[id] = true;
+        }
+    }
+
     // biome stage (shared by the TERRAIN step and biome lookups); nmax sizes the grids
     void enqueue_biomes(const Work& W, const Batch& B, cudaStream_t s, long nmax) {
+        const int32_t* n_dev = B.n_dev;
         const int32_t* cnt_b = W.tb_b.count.as<int32_t>();
+        ck(cudaMemsetAsync(W.d_qnext.p, 0, sizeof(int32_t) * K_COUNT, s), "memset");   // work-queue counters
         W.tb_b.reset(s);
-        launch(k_items<body_nb_insert, 9>, s, 9 * nmax, B);
+        run_body<body_nb_insert, 9>(K_NB_INSERT, W, s, 9 * nmax, B, n_dev);
         launch(k_number<0, nb_key, 9>, s, 9 * nmax, B);
-        launch(k_items<body_nb_resolve, 9>, s, 9 * nmax, B);
-        launch(k_dyn<body_climate_col, 16>, s, nmax * 16 * 2, B, cnt_b);
-        launch(k_dyn<body_climate_quart, 16 * kRuns, TB_MINB_QUART>, s, nmax * 16 * kRuns * 2, B, cnt_b);
-#if TB_CHAIN_WARP
-        launch(k_chain_warp, s, nmax * 2 * 32, B, cnt_b);
-#else
-        launch(k_dyn<body_chain, 1>, s, nmax * 2, B, cnt_b);
-#endif
+        run_body<body_nb_resolve, 9>(K_NB_RESOLVE, W, s, 9 * nmax, B, n_dev);
+        run_body<body_climate_col, 16>(K_CLIMATE_COL, W, s, nmax * 16 * 2, B, cnt_b);
+        run_body<body_climate_quart, 16 * kRuns, TB_MINB_QUART>(K_CLIMATE_QUART, W, s, nmax * 16 * kRuns * 2, B, cnt_b);
+        {
+            const LaunchShape& k = lt.k[K_CHAIN];
+            long blocks = (nmax * 2 * 32 + k.threads - 1) / k.threads;
+            blocks = std::max(1L, std::min(blocks, static_cast<long>(g_sm_count) * k.blocks_per_sm));
+            if (prof_now) ck(cudaEventRecord(prof_ev[2 * K_CHAIN], s), "event");
+            k_chain_warp<<<static_cast<unsigned>(blocks), k.threads, 0, s>>>(B, cnt_b);
+            ++g_launches;
+            if (prof_now) {
+                ck(cudaEventRecord(prof_ev[2 * K_CHAIN + 1], s), "event");
+                prof_marked[K_CHAIN] = true;
+            }
+        }
     }
 
     // every kernel of one batch; with timed set, events split the stages
@@ -868,43 +1102,74 @@ struct Generator {
         };
         const int32_t* cnt_c = W.tb_c.count.as<int32_t>();
         const int32_t* cnt_s = W.tb_s.count.as<int32_t>();
+        prof_now = timed && prof;
         mark(0);
         enqueue_biomes(W, B, s, nmax);
         mark(1);
+        const int32_t* n_dev = B.n_dev;
         W.tb_c.reset(s);
-        launch(k_items<body_cc_insert, 25>, s, 25 * nmax, B);
+        run_body<body_cc_insert, 25>(K_CC_INSERT, W, s, 25 * nmax, B, n_dev);
         launch(k_number<1, cc_key, 25>, s, 25 * nmax, B);
-        launch(k_items<body_cc_resolve, 25>, s, 25 * nmax, B);
-        launch(k_dyn<body_corner_col, 1>, s, 16 * nmax, B, cnt_c);
+        run_body<body_cc_resolve, 25>(K_CC_RESOLVE, W, s, 25 * nmax, B, n_dev);
+        run_body<body_corner_col, 1>(K_CORNER_COL, W, s, 16 * nmax, B, cnt_c);
         mark(8);
-        launch(k_dyn<body_corner, kRows, TB_MINB_CORNER>, s, 16 * nmax * kRows, B, cnt_c);
+        run_body<body_corner, kRows, TB_MINB_CORNER>(K_CORNER, W, s, 16 * nmax * kRows, B, cnt_c);
         mark(9);
-        launch(k_items<body_zoom_table, kZoomVerts>, s, kZoomVerts * nmax, B);
-        launch(k_items<body_zoom_uniform, kZoomCells>, s, kZoomCells * nmax, B);
+        run_body<body_zoom_table, kZoomVerts>(K_ZOOM_TABLE, W, s, kZoomVerts * nmax, B, n_dev);
+        run_body<body_zoom_uniform, kZoomCells>(K_ZOOM_UNIFORM, W, s, kZoomCells * nmax, B, n_dev);
         mark(2);
         W.tb_s.reset(s);
-        launch(k_items<body_sg_insert, kGrid>, s, kGrid * nmax, B);
+        run_body<body_sg_insert, kGrid>(K_SG_INSERT, W, s, kGrid * nmax, B, n_dev);
         launch(k_number<2, sg_key_item, kGrid>, s, kGrid * nmax, B);
-        launch(k_items<body_sg_resolve, kGrid>, s, kGrid * nmax, B);
-        launch(k_dyn<body_surface_level, 1>, s, 2 * nmax * 100, B, cnt_s);
-        launch(k_items<body_aquifer_cell, kAqCells>, s, kAqCells * nmax, B);
-        launch(k_items<body_aquifer_query, kAqQueries>, s, kAqQueries * nmax, B);
-        launch(k_items<body_aquifer_skip, 1>, s, nmax, B);
+        run_body<body_sg_resolve, kGrid>(K_SG_RESOLVE, W, s, kGrid * nmax, B, n_dev);
+        run_body<body_surface_level, 1>(K_SURFACE_LEVEL, W, s, 2 * nmax * 100, B, cnt_s);
+        run_body<body_aquifer_cell, kAqCells>(K_AQ_CELL, W, s, kAqCells * nmax, B, n_dev);
+        run_body<body_aquifer_query, kAqQueries>(K_AQ_QUERY, W, s, kAqQueries * nmax, B, n_dev);
+        run_body<body_aquifer_skip, 1>(K_AQ_SKIP, W, s, nmax, B, n_dev);
         mark(3);
-        launch(k_init_heights, s, 256 * nmax, B);
-        launch(k_items<body_fill, 256 * kCellsY, TB_MINB_FILL>, s, 256L * kCellsY * nmax, B);
+        run_body<body_init_heights, 256>(K_INIT_HEIGHTS, W, s, 256 * nmax, B, n_dev);
+        run_body<body_fill, 256 * kCellsY, TB_MINB_FILL>(K_FILL, W, s, 256L * kCellsY * nmax, B, n_dev);
         if (aquifer_dev)
             ck(cudaMemcpyAsync(aquifer_dev, B.blocks, sizeof(uint16_t) * static_cast<size_t>(max_batch) * kBlocksPerChunk, cudaMemcpyDeviceToDevice, s),
                "d2d");
         mark(4);
-        launch(k_items<body_surface1, 256>, s, 256 * nmax, B);
-        launch(k_items<body_block_biome, 256>, s, 256L * nmax, B);
+        run_body<body_surface1, 256>(K_SURFACE1, W, s, 256 * nmax, B, n_dev);
+        run_body<body_block_biome, 256>(K_BLOCK_BIOME, W, s, 256L * nmax, B, n_dev);
         mark(6);
-        launch(k_items<body_surface_walk_rules, 256, TB_MINB_WALK>, s, 256 * nmax, B);
+        run_body<body_surface_walk_rules, 256, TB_MINB_WALK>(K_WALK, W, s, 256 * nmax, B, n_dev);
         mark(7);
-        launch(k_items<body_surface_frozen, 256>, s, 256 * nmax, B);
-        launch(k_items<body_gather, kQuartsPerChunk>, s, static_cast<long>(kQuartsPerChunk) * nmax, B);
+        run_body<body_surface_frozen, 256>(K_FROZEN, W, s, 256 * nmax, B, n_dev);
+        run_body<body_gather, kQuartsPerChunk>(K_GATHER, W, s, static_cast<long>(kQuartsPerChunk) * nmax, B, n_dev);
         mark(5);
+        prof_now = false;
+    }
+
+    // per-kernel times of the last timed batch into prof_ms (after its events completed)
+    void collect_kernel_times() {
+        for (int i = 0; i < K_COUNT; ++i)
+            if (prof_marked[i]) {
+                float ms = 0.0f;
+                ck(cudaEventSynchronize(prof_ev[2 * i + 1]), "sync");
+                ck(cudaEventElapsedTime(&ms, prof_ev[2 * i], prof_ev[2 * i + 1]), "elapsed");
+                prof_ms[i] += ms;
+                ++prof_calls[i];
+                prof_marked[i] = false;
+            }
+    }
+
+    // a new launch table: graphs and (for a new table load) the batch buffers are rebuilt
+    void set_launch_table(const LaunchTable& t) {
+        finish();
+        const bool realloc = t.table_load != lt.table_load;
+        lt = t;
+        for (auto& o : out)
+            if (o.graph) {
+                cudaGraphExecDestroy(o.graph);
+                o.graph = nullptr;
+            }
+        destroy_queue_graphs();
+        graph_launches = 0;
+        if (realloc) alloc_batch(max_batch);
     }
 
     void add_stage_times(tg_timing* t) {
@@ -923,6 +1188,7 @@ struct Generator {
         float corner = 0.0f;
         ck(cudaEventElapsedTime(&corner, ev[8], ev[9]), "elapsed");
         t->corner_ms += corner;
+        collect_kernel_times();
         t->batches += 1;
     }
 
@@ -1048,6 +1314,21 @@ struct Generator {
             }
         ck(cudaStreamSynchronize(stream), "sync");
         ck(cudaStreamSynchronize(lane_stream), "sync");
+        check_device_errors();
+    }
+
+    // The lanes' sticky device error words (kErrTableFull, kErrKeyMissing): any bit set is
+    // an internal error of the work that ran (and stays reported until the generator is
+    // destroyed). Called with no work in flight.
+    void check_device_errors() {
+        for (int l = 0; l < lanes; ++l) {
+            uint32_t e = 0;
+            ck(cudaMemcpy(&e, work[l].d_err.p, sizeof e, cudaMemcpyDeviceToHost), "d2h");
+            if (e)
+                throw Error(TG_ERR_INTERNAL, std::string("device error bits ") + std::to_string(e) +
+                                                 ((e & kErrTableFull) ? " (a dedupe hash table was full)" : "") +
+                                                 ((e & kErrKeyMissing) ? " (a dedupe key was missing at resolve)" : ""));
+        }
     }
 
     // lane 1's stream starts after the work already queued on `stream` (the caller's)
@@ -1121,7 +1402,10 @@ struct Generator {
             if (!ft || !fb) throw Error(TG_ERR_IO, std::string("cannot write the region dump in ") + dump_dir);
         }
         const size_t side = static_cast<size_t>(region) * 16;
-        std::vector<uint8_t> rec(topdown_path ? side * side * 8 : 0, 0);
+        // top-down records go to the file a slab at a time (each slab's rows are contiguous in it)
+        std::ofstream ftd;
+        if (topdown_path) ftd = open_topdown_file(topdown_path, region, x0, z0);
+        std::vector<uint8_t> rec(topdown_path ? static_cast<size_t>(rows_per_slab) * 16 * side * 8 : 0, 0);
         std::vector<tg_chunk_xz> chunks(slab_chunks);
         for (int r0 = 0; r0 < region; r0 += rows_per_slab) {
             const int rows = std::min(rows_per_slab, region - r0);
@@ -1134,7 +1418,10 @@ struct Generator {
                 fb.write(bio.as<const char>(), static_cast<std::streamsize>(static_cast<size_t>(n) * kQuartsPerChunk));
                 if (!ft || !fb) throw Error(TG_ERR_IO, std::string("cannot write the region dump in ") + dump_dir);
             }
-            if (topdown_path) topdown_records(blk.as<const uint8_t>(), rows, region, r0, side, rec.data());
+            if (topdown_path) {
+                topdown_records(blk.as<const uint8_t>(), rows, region, side, rec.data());
+                write_topdown_rows(ftd, topdown_path, rec.data(), static_cast<size_t>(rows) * 16 * side * 8);
+            }
         }
         if (dump_dir) {
             ft.close();
@@ -1144,61 +1431,82 @@ struct Generator {
               << ", \"min_y\": " << tbm::kMinY << ", \"chunk_bytes\": " << kBlocksPerChunk << ", \"biome_bytes\": " << kQuartsPerChunk << "}\n";
             if (!m || ft.fail() || fb.fail()) throw Error(TG_ERR_IO, std::string("cannot write the region dump in ") + dump_dir);
         }
-        if (topdown_path) write_topdown_file(topdown_path, region, x0, z0, rec);
+        if (topdown_path) {
+            ftd.close();
+            if (ftd.fail()) throw Error(TG_ERR_IO, std::string("cannot write the top-down map ") + topdown_path);
+        }
     }
 
-    // The top-down map alone: each slab of chunk rows is generated into HBM (pieces of at most
-    // max_batch chunks) and k_topdown reduces it to 8 bytes per block column, so only the
-    // records cross the host link.
+    // The top-down map alone: each slab of chunk rows is generated into HBM in pieces of at
+    // most max_batch chunks, each piece straight into the output slot that k_topdown reads
+    // (stream order keeps the next piece from overwriting it before k_topdown has run), so
+    // only the 8-byte records per block column cross the host link; the slab's records go to
+    // the file once its copy has landed.
     void topdown_on_device(int x0, int z0, int region, const char* path) {
         const int rows_per_slab = std::max(1, std::min(region, 4096 / region));
         const size_t slab_chunks = static_cast<size_t>(rows_per_slab) * region;
         const size_t side = static_cast<size_t>(region) * 16;
         const int piece_max = std::min<int>(max_batch, static_cast<int>(slab_chunks));
-        std::vector<uint8_t> rec(side * side * 8);
+        const size_t slab_bytes = static_cast<size_t>(rows_per_slab) * 16 * side * 8;
         std::vector<tg_chunk_xz> chunks(slab_chunks);
-        DevBuf d_chunks, d_blocks, d_rec;
+        DevBuf d_chunks, d_rec;
+        PinBuf h_rec;
         d_chunks.alloc(sizeof(tg_chunk_xz) * slab_chunks);
-        d_blocks.alloc(sizeof(uint16_t) * static_cast<size_t>(piece_max) * kBlocksPerChunk);
-        d_rec.alloc(static_cast<size_t>(rows_per_slab) * 16 * side * 8);
+        d_rec.alloc(slab_bytes);
+        h_rec.alloc(slab_bytes);
+        std::ofstream f = open_topdown_file(path, region, x0, z0);
+        finish();
+        OutSlot& o = out[0];
+        Work& W = work[0];
+        cudaStream_t s = stream;
         for (int r0 = 0; r0 < region; r0 += rows_per_slab) {
             const int rows = std::min(rows_per_slab, region - r0);
             const int n = rows * region;
             for (int r = 0; r < rows; ++r)
                 for (int i = 0; i < region; ++i) chunks[static_cast<size_t>(r) * region + i] = tg_chunk_xz{x0 + i, z0 + r0 + r};
             check_chunks(chunks.data(), n);
-            ck(cudaMemcpy(d_chunks.p, chunks.data(), sizeof(tg_chunk_xz) * n, cudaMemcpyHostToDevice), "h2d");
+            ck(cudaMemcpyAsync(d_chunks.p, chunks.data(), sizeof(tg_chunk_xz) * n, cudaMemcpyHostToDevice, s), "h2d");
             for (int first = 0; first < n; first += piece_max) {
                 const int cnt = std::min(piece_max, n - first);
-                generate_device(d_chunks.as<tg_chunk_xz>() + first, cnt, d_blocks.as<uint16_t>(), nullptr, nullptr);
-                launch(k_topdown, stream, 256L * cnt, d_blocks.as<const uint16_t>(), model.block_flags, cnt, first, region, d_rec.as<uint2>());
+                launch(k_split_chunks, s, cnt, d_chunks.as<tg_chunk_xz>() + first, cnt, static_cast<int32_t>(current_slot), W.d_cx.as<int32_t>(),
+                       W.d_cz.as<int32_t>(), W.d_cs.as<int32_t>(), W.d_n.as<int32_t>());
+                enqueue_batch(W, batch_view(W, &o), s, max_batch, nullptr, false);
+                launch(k_topdown, s, 256L * cnt, o.blocks.as<const uint16_t>(), model.block_flags, cnt, first, region, d_rec.as<uint2>());
                 ck(cudaGetLastError(), "kernel launch");
             }
             const size_t bytes = static_cast<size_t>(rows) * 16 * side * 8;
-            ck(cudaMemcpyAsync(rec.data() + static_cast<size_t>(r0) * 16 * side * 8, d_rec.p, bytes, cudaMemcpyDeviceToHost, stream), "d2h");
-            ck(cudaStreamSynchronize(stream), "sync");
+            ck(cudaMemcpyAsync(h_rec.p, d_rec.p, bytes, cudaMemcpyDeviceToHost, s), "d2h");
+            ck(cudaStreamSynchronize(s), "sync");
+            write_topdown_rows(f, path, h_rec.as<uint8_t>(), bytes);
         }
-        write_topdown_file(path, region, x0, z0, rec);
+        check_device_errors();
+        f.close();
+        if (f.fail()) throw Error(TG_ERR_IO, std::string("cannot write the top-down map ") + path);
     }
 
-    static void write_topdown_file(const char* path, int region, int x0, int z0, const std::vector<uint8_t>& rec) {
+    static std::ofstream open_topdown_file(const char* path, int region, int x0, int z0) {
         std::ofstream f(path, std::ios::binary);
         const int32_t head[5] = {1, region, x0, z0, tbm::kMinY};
         f.write("MCTD", 4);
         f.write(reinterpret_cast<const char*>(head), sizeof head);
-        f.write(reinterpret_cast<const char*>(rec.data()), static_cast<std::streamsize>(rec.size()));
+        if (!f) throw Error(TG_ERR_IO, std::string("cannot write the top-down map ") + path);
+        return f;
+    }
+
+    static void write_topdown_rows(std::ofstream& f, const char* path, const uint8_t* rec, size_t bytes) {
+        f.write(reinterpret_cast<const char*>(rec), static_cast<std::streamsize>(bytes));
         if (!f) throw Error(TG_ERR_IO, std::string("cannot write the top-down map ") + path);
     }
 
-    // Top-down records of `rows` chunk rows of u8 blocks (row-major, region chunks per row),
-    // the first of them chunk row r0 of the region.
-    static void topdown_records(const uint8_t* blocks, int rows, int region, int r0, size_t side, uint8_t* rec) {
+    // Top-down records of `rows` chunk rows of u8 blocks (row-major, region chunks per row)
+    // into rec: the rows' block rows, side records each.
+    static void topdown_records(const uint8_t* blocks, int rows, int region, size_t side, uint8_t* rec) {
         auto air = [](int st) { return (tbm::kBlockFlags[st] & 1) != 0; };
         auto fluid = [](int st) { return (tbm::kBlockFlags[st] & 8) != 0; };
         for (int r = 0; r < rows; ++r)
             for (int i = 0; i < region; ++i) {
                 const uint8_t* b = blocks + (static_cast<size_t>(r) * region + i) * kBlocksPerChunk;
-                const size_t rx = static_cast<size_t>(i) * 16, rz = static_cast<size_t>(r0 + r) * 16;
+                const size_t rx = static_cast<size_t>(i) * 16, rz = static_cast<size_t>(r) * 16;
                 for (int z = 0; z < 16; ++z)
                     for (int x = 0; x < 16; ++x) {
                         int y = tbm::kHeight - 1;
@@ -1233,6 +1541,7 @@ struct Generator {
         if (biomes_dev) ck(cudaMemcpyAsync(biomes_dev, o.biomes.p, static_cast<size_t>(count) * kQuartsPerChunk, cudaMemcpyDeviceToDevice, s), "d2d");
         ck(cudaGetLastError(), "kernel launch");
         ck(cudaStreamSynchronize(s), "sync");
+        check_device_errors();
     }
 
     // Final density of every block (the value the fill tests with the aquifer), written by
@@ -1269,6 +1578,7 @@ struct Generator {
                "d2h");
             ck(cudaStreamSynchronize(s), "sync");
         }
+        check_device_errors();
     }
 
     // Biome lookups at independent positions: one thread per position computes the zoomed
@@ -1436,6 +1746,177 @@ struct Generator {
             throw Error(TG_ERR_INTERNAL, "no-allocation lookup finished " + std::to_string(finished) + " of " + std::to_string(n) + " positions");
     }
 
+    // ---- device-resident multi-seed batch from a device work queue --------------------------------
+    DevBuf q_req, q_cx, q_cz, q_cs, q_rq, q_ix, q_state;
+    size_t q_item_cap = 0, q_req_cap = 0;
+    PinBuf q_req_host;
+    cudaGraphExec_t q_loop = nullptr, q_iter = nullptr;   // the WHILE-loop graph, one iteration's graph
+    cudaStream_t q_stream = nullptr;
+
+    QueueView queue_view(int n_req) const {
+        return QueueView{q_req.as<QueueReq>(), q_cx.as<int32_t>(), q_cz.as<int32_t>(), q_cs.as<int32_t>(), q_rq.as<int32_t>(), q_ix.as<int32_t>(),
+                         q_state.as<int32_t>(), n_req};
+    }
+
+    // one queue iteration: take, TERRAIN step on lane 0 into out[0], scatter, advance
+    void enqueue_queue_iteration(cudaStream_t s, cudaGraphConditionalHandle h, bool looped) {
+        Work& W = work[0];
+        const QueueView Q = queue_view(0);
+        launch(k_queue_take, s, max_batch, Q, max_batch, W.d_cx.as<int32_t>(), W.d_cz.as<int32_t>(), W.d_cs.as<int32_t>(), W.d_n.as<int32_t>());
+        const Batch B = batch_view(W, &out[0]);
+        enqueue_batch(W, B, s, max_batch, nullptr, false);
+        launch(k_queue_scatter, s, static_cast<long>(max_batch) * (kScatterBlockVecs + kScatterBiomeVecs), Q, out[0].blocks.as<const uint4>(),
+               out[0].biomes.as<const uint4>());
+        k_queue_advance<<<1, 1, 0, s>>>(Q, h, looped ? 1 : 0);
+        ++g_launches;
+    }
+
+    void destroy_queue_graphs() {
+        if (q_loop) cudaGraphExecDestroy(q_loop);
+        if (q_iter) cudaGraphExecDestroy(q_iter);
+        q_loop = q_iter = nullptr;
+    }
+
+    // Builds the graphs of the queue form once per set of queue buffers and stream: a WHILE
+    // node whose body is one iteration (device loop), and one iteration alone (host loop).
+    void build_queue_graphs(cudaStream_t s) {
+        if (q_loop && q_iter && q_stream == s) return;
+        destroy_queue_graphs();
+        const int before = g_launches;
+        cudaGraph_t g;
+        ck(cudaGraphCreate(&g, 0), "graph create");
+        cudaGraphConditionalHandle h;
+        ck(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault), "conditional handle");
+        cudaGraphNodeParams p{};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeWhile;
+        p.conditional.size = 1;
+        cudaGraphNode_t node;
+        ck(cudaGraphAddNode(&node, g, nullptr, 0, &p), "conditional node");
+        cudaGraph_t body = p.conditional.phGraph_out[0];
+        ck(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal), "capture");
+        enqueue_queue_iteration(s, h, true);
+        ck(cudaStreamEndCapture(s, &body), "capture");
+        ck(cudaGraphInstantiate(&q_loop, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+        cudaGraph_t gi;
+        ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
+        enqueue_queue_iteration(s, cudaGraphConditionalHandle{}, false);
+        ck(cudaStreamEndCapture(s, &gi), "capture");
+        ck(cudaGraphInstantiate(&q_iter, gi, 0), "graph instantiate");
+        cudaGraphDestroy(gi);
+        g_launches = before;
+        q_stream = s;
+    }
+
+    // The multi-seed TERRAIN step with every request's chunks and outputs in HBM. The requests
+    // go into a device work queue; with host_loop false one graph launch runs batch after
+    // batch on the device until the queue is empty, with host_loop true the host launches one
+    // graph per batch (the same kernels). Requests whose distinct seeds exceed the resident
+    // slots go in groups, one launch per group.
+    void generate_batch_device(const tg_request_device* req, int n, bool host_loop, tg_timing* t) {
+        for (int r = 0; r < n; ++r) {
+            const tg_request_device& q = req[r];
+            if (q.count < 0 || (q.count > 0 && (!q.chunks || !q.blocks_out))) throw Error(TG_ERR_INVALID_ARGUMENT, "bad request");
+            if ((reinterpret_cast<uintptr_t>(q.blocks_out) | reinterpret_cast<uintptr_t>(q.biomes_out)) & 15u)
+                throw Error(TG_ERR_INVALID_ARGUMENT, "request outputs must be 16-byte aligned");
+        }
+        finish();
+        cudaStream_t s = stream;
+        for (int r0 = 0; r0 < n;) {
+            // a group: consecutive requests with at most kMaxSlots / 2 distinct seeds
+            std::vector<int64_t> seeds;
+            int r1 = r0;
+            for (; r1 < n; ++r1) {
+                if (std::find(seeds.begin(), seeds.end(), req[r1].seed) == seeds.end()) {
+                    if (static_cast<int>(seeds.size()) == kMaxSlots / 2) break;
+                    seeds.push_back(req[r1].seed);
+                }
+            }
+            std::vector<int> keep;
+            std::vector<QueueReq> qr;
+            int64_t total = 0;
+            for (int r = r0; r < r1; ++r) {
+                if (req[r].count == 0) continue;
+                const int slot = seed_slot(req[r].seed, keep);
+                if (std::find(keep.begin(), keep.end(), slot) == keep.end()) keep.push_back(slot);
+                qr.push_back(QueueReq{req[r].chunks, req[r].blocks_out, req[r].biomes_out, static_cast<int32_t>(total), req[r].count, slot, 0});
+                total += req[r].count;
+            }
+            r0 = r1;
+            if (total == 0) continue;
+            if (total > INT32_MAX / 2) throw Error(TG_ERR_INVALID_ARGUMENT, "too many chunks in one batch call");
+            // queue buffers (graphs hold their addresses: rebuilt when they grow)
+            if (static_cast<size_t>(total) > q_item_cap || qr.size() > q_req_cap) {
+                destroy_queue_graphs();
+                q_item_cap = std::max<size_t>(static_cast<size_t>(total), q_item_cap);
+                q_req_cap = std::max<size_t>(qr.size(), q_req_cap);
+                for (DevBuf* b : {&q_cx, &q_cz, &q_cs, &q_rq, &q_ix}) b->alloc(sizeof(int32_t) * q_item_cap);
+                q_req.alloc(sizeof(QueueReq) * q_req_cap);
+                q_req_host.alloc(sizeof(QueueReq) * q_req_cap + 64);
+            }
+            if (!q_state.p) q_state.alloc(sizeof(int32_t) * 8);
+            const int iters = static_cast<int>((total + max_batch - 1) / max_batch);
+            int32_t* hs = reinterpret_cast<int32_t*>(q_req_host.as<uint8_t>() + sizeof(QueueReq) * q_req_cap);
+            hs[0] = 0;
+            hs[1] = static_cast<int32_t>(total);
+            hs[2] = 0;
+            hs[3] = iters + 1;
+            hs[4] = 0;
+            std::memcpy(q_req_host.p, qr.data(), sizeof(QueueReq) * qr.size());
+            ck(cudaMemcpyAsync(q_req.p, q_req_host.p, sizeof(QueueReq) * qr.size(), cudaMemcpyHostToDevice, s), "h2d");
+            ck(cudaMemcpyAsync(q_state.p, hs, sizeof(int32_t) * 5, cudaMemcpyHostToDevice, s), "h2d");
+            launch(k_queue_fill, s, total, queue_view(static_cast<int>(qr.size())));
+            if (t) {
+                // timed: the host loop with stage events between the kernels
+                for (int k = 0; k < iters; ++k) {
+                    Work& W = work[0];
+                    const QueueView Q = queue_view(0);
+                    launch(k_queue_take, s, max_batch, Q, max_batch, W.d_cx.as<int32_t>(), W.d_cz.as<int32_t>(), W.d_cs.as<int32_t>(),
+                           W.d_n.as<int32_t>());
+                    enqueue_batch(W, batch_view(W, &out[0]), s, max_batch, nullptr, true);
+                    add_stage_times(t);
+                    launch(k_queue_scatter, s, static_cast<long>(max_batch) * (kScatterBlockVecs + kScatterBiomeVecs), Q,
+                           out[0].blocks.as<const uint4>(), out[0].biomes.as<const uint4>());
+                    k_queue_advance<<<1, 1, 0, s>>>(Q, cudaGraphConditionalHandle{}, 0);
+                    ++g_launches;
+                }
+            } else {
+                build_queue_graphs(s);
+                if (host_loop) {
+                    for (int k = 0; k < iters; ++k) ck(cudaGraphLaunch(q_iter, s), "graph launch");
+                } else {
+                    ck(cudaGraphLaunch(q_loop, s), "graph launch");
+                }
+                g_launches += iters * (graph_launches_per_batch() + 3);
+            }
+            ck(cudaGetLastError(), "kernel launch");
+            int32_t done[5];
+            ck(cudaMemcpyAsync(done, q_state.p, sizeof done, cudaMemcpyDeviceToHost, s), "d2h");
+            ck(cudaStreamSynchronize(s), "sync");
+            check_device_errors();
+            if (done[0] != total) throw Error(TG_ERR_INTERNAL, "device work queue ended at item " + std::to_string(done[0]) + " of " + std::to_string(total));
+        }
+    }
+
+    // kernels of one batch (as enqueued by enqueue_batch without the aquifer copy)
+    int graph_launches_per_batch() {
+        if (!graph_launches) {
+            const int before = g_launches;
+            g_launches = 0;
+            // count by enqueueing into a throwaway capture
+            cudaGraph_t g;
+            ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "capture");
+            enqueue_batch(work[0], batch_view(work[0], &out[0]), stream, max_batch, nullptr, false);
+            ck(cudaStreamEndCapture(stream, &g), "capture");
+            cudaGraphDestroy(g);
+            graph_launches = g_launches;
+            g_launches = before;
+        }
+        return graph_launches;
+    }
+
     // Multi-seed batch: requests are cut into device batches; a batch mixes seeds.
     void generate_batch(const tg_request* req, int n, tg_timing* t) {
         order_lanes();
@@ -1484,21 +1965,24 @@ struct Generator {
 };
 
 // ---- continuous-batching server ---------------------------------------------------------------------
-// A worker thread owns the generator. Requests (seed, chunk list, host output buffers)
-// queue on submit; the worker admits them into an active set while the chunks in flight
-// stay within the HBM-derived limit, cuts device batches across all active requests
-// (mixing seeds and request sizes), and drains each batch's outputs on the copy stream
-// while the next batch computes. A request completes when its last chunk is copied out.
+// A worker thread owns the generator. Requests (seed, chunk list, host output buffers in the
+// u16 or the u8 form) queue on submit; the worker admits them into an active set while the
+// chunks in flight, priced at the device memory a chunk of batch capacity takes, stay within
+// the HBM budget; it cuts device batches across all active requests (mixing seeds, request
+// sizes and output forms) and drains each batch's outputs on the copy stream while the next
+// batch computes. A request completes when its last chunk is copied out; a cancelled one
+// when its chunks already in flight are (its remaining chunks are never issued).
 struct Server {
     struct Req {
         uint64_t id = 0;
         int64_t seed = 0;
         std::vector<tg_chunk_xz> chunks;
         uint16_t* blocks = nullptr;
+        uint8_t* blocks8 = nullptr;    // u8 form
         uint8_t* biomes = nullptr;
         int issued = 0, finished = 0;
         double t_submit = 0, t_done = 0;
-        bool complete = false;
+        bool complete = false, cancelled = false;
         int slot = -1;
     };
     struct InFlight {
@@ -1509,6 +1993,7 @@ struct Server {
     Generator* g;
     int batch_chunks;
     long max_active_chunks;
+    double device_bytes_per_chunk;
     std::thread worker;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -1524,11 +2009,13 @@ struct Server {
     long chunks_done = 0;
     double t_first = -1, t_last = 0;
     int batches = 0;
+    int64_t cancelled = 0;
 
     Server(Generator* gen, const tg_server_config* cfg) : g(gen) {
         batch_chunks = cfg && cfg->batch_chunks > 0 ? std::min(cfg->batch_chunks, g->max_batch) : g->max_batch;
-        const double per_chunk = static_cast<double>(kBlocksPerChunk) * 2 + kQuartsPerChunk;
-        const long budget_chunks = cfg && cfg->hbm_budget_bytes > 0 ? static_cast<long>(static_cast<double>(cfg->hbm_budget_bytes) / per_chunk) : 8L * g->max_batch;
+        device_bytes_per_chunk = g->device_bytes_per_chunk();
+        const long budget_chunks =
+            cfg && cfg->hbm_budget_bytes > 0 ? static_cast<long>(static_cast<double>(cfg->hbm_budget_bytes) / device_bytes_per_chunk) : 8L * g->max_batch;
         max_active_chunks = std::max<long>(batch_chunks, budget_chunks);
         g->served = true;
         worker = std::thread([this] { run(); });
@@ -1543,12 +2030,13 @@ struct Server {
         g->served = false;
     }
 
-    uint64_t submit(int64_t seed, const tg_chunk_xz* chunks, int count, uint16_t* blocks, uint8_t* biomes) {
+    uint64_t submit(int64_t seed, const tg_chunk_xz* chunks, int count, uint16_t* blocks, uint8_t* blocks8, uint8_t* biomes) {
         g->check_chunks(chunks, count);
         auto r = std::make_unique<Req>();
         r->seed = seed;
         r->chunks.assign(chunks, chunks + count);
         r->blocks = blocks;
+        r->blocks8 = blocks8;
         r->biomes = biomes;
         r->t_submit = now_ms();
         std::lock_guard<std::mutex> l(mu);
@@ -1567,7 +2055,37 @@ struct Server {
         return id;
     }
 
-    // 1 = done (the ticket is released), 0 = pending
+    // A queued request is dropped at once; an active one issues no more chunks and completes
+    // when its chunks in flight are copied out (its outputs then hold only those chunks).
+    // Returns false when the request had already completed (its result stands).
+    bool cancel(uint64_t id) {
+        std::lock_guard<std::mutex> l(mu);
+        auto it = reqs.find(id);
+        if (it == reqs.end()) throw Error(TG_ERR_INVALID_ARGUMENT, "unknown ticket");
+        Req* r = it->second.get();
+        if (r->complete) return false;
+        r->cancelled = true;
+        ++cancelled;
+        auto q = std::find(queue.begin(), queue.end(), r);
+        if (q != queue.end()) {
+            queue.erase(q);
+            r->complete = true;
+            r->t_done = now_ms();
+            cv_done.notify_all();
+        } else if (r->finished == r->issued) {
+            // active with nothing in flight: done now
+            auto a = std::find(active.begin(), active.end(), r);
+            if (a != active.end()) active.erase(a);
+            r->complete = true;
+            r->t_done = now_ms();
+            cv_done.notify_all();
+        }
+        cv_work.notify_one();
+        return true;
+    }
+
+    // 1 = done (the ticket is released), 0 = pending; a cancelled request throws
+    // TG_ERR_CANCELLED once done (and is released).
     int poll(uint64_t id, int wait_ms) {
         std::unique_lock<std::mutex> l(mu);
         auto it = reqs.find(id);
@@ -1578,7 +2096,9 @@ struct Server {
         else if (wait_ms > 0) cv_done.wait_for(l, std::chrono::milliseconds(wait_ms), pred);
         if (failure != TG_OK && !r->complete) throw Error(failure, failure_msg);
         if (!r->complete) return 0;
+        const bool was_cancelled = r->cancelled;
         reqs.erase(it);
+        if (was_cancelled) throw Error(TG_ERR_CANCELLED, "the request was cancelled");
         return 1;
     }
 
@@ -1602,6 +2122,18 @@ struct Server {
         if (t_first >= 0 && t_last > t_first) s->chunks_per_s = static_cast<double>(chunks_done) / ((t_last - t_first) / 1000.0);
         s->queued_requests = static_cast<int32_t>(queue.size());
         s->active_requests = static_cast<int32_t>(active.size());
+        s->cancelled_requests = cancelled;
+        s->device_bytes_per_chunk = device_bytes_per_chunk;
+        s->max_active_chunks = max_active_chunks;
+    }
+
+    // latencies (submit -> last byte on the host) of the requests completed since the last
+    // reset, in completion order
+    int latencies(double* out, int cap) {
+        std::lock_guard<std::mutex> l(mu);
+        const int n = static_cast<int>(std::min<size_t>(lat.size(), static_cast<size_t>(cap)));
+        if (out) std::copy(lat.begin(), lat.begin() + n, out);
+        return static_cast<int>(lat.size());
     }
 
     void reset_stats() {
@@ -1611,22 +2143,26 @@ struct Server {
         t_first = -1;
         t_last = 0;
         batches = 0;
+        cancelled = 0;
     }
 
     void complete_batch(InFlight& f) {
         ck(cudaEventSynchronize(g->out[f.out].drained), "sync");
         g->out[f.out].busy = false;
+        g->check_device_errors();
         const double t = now_ms();
         std::lock_guard<std::mutex> l(mu);
         for (auto& part : f.parts) {
             Req* r = part.first;
             r->finished += part.second;
             chunks_done += part.second;
-            if (r->finished == static_cast<int>(r->chunks.size())) {
+            const bool all = r->finished == static_cast<int>(r->chunks.size());
+            if (all || (r->cancelled && r->finished == r->issued)) {
                 r->complete = true;
                 r->t_done = t;
-                lat.push_back(t - r->t_submit);
-                active.erase(std::find(active.begin(), active.end(), r));
+                if (!r->cancelled) lat.push_back(t - r->t_submit);
+                auto a = std::find(active.begin(), active.end(), r);
+                if (a != active.end()) active.erase(a);
             }
         }
         t_last = t;
@@ -1641,7 +2177,7 @@ struct Server {
             std::vector<int32_t> cx(g->max_batch), cz(g->max_batch), cs(g->max_batch);
             auto unissued = [&] {
                 for (Req* r : active)
-                    if (r->issued < static_cast<int>(r->chunks.size())) return true;
+                    if (!r->cancelled && r->issued < static_cast<int>(r->chunks.size())) return true;
                 return false;
             };
             for (;;) {
@@ -1663,9 +2199,11 @@ struct Server {
                         else cv_work.wait_for(l, std::chrono::microseconds(100), [&] { return stop || !queue.empty(); });
                     }
                     if (stop && flight.empty()) break;
-                    // admission: chunks still to issue across the active set stay within the limit
+                    // admission: chunks still to issue across the active set stay within the
+                    // device-memory budget
                     long pending = 0;
-                    for (Req* r : active) pending += static_cast<long>(r->chunks.size()) - r->issued;
+                    for (Req* r : active)
+                        if (!r->cancelled) pending += static_cast<long>(r->chunks.size()) - r->issued;
                     while (!queue.empty() && (active.empty() || pending + static_cast<long>(queue.front()->chunks.size()) <= max_active_chunks)) {
                         Req* r = queue.front();
                         queue.pop_front();
@@ -1692,21 +2230,28 @@ struct Server {
                 // cut one batch across the active requests, oldest first
                 InFlight f;
                 int n = 0;
+                bool narrow = false;
                 std::vector<Generator::Piece> pieces;
                 {
                     std::lock_guard<std::mutex> l(mu);
                     for (Req* r : active) {
                         if (n == batch_chunks) break;
                         const int left = static_cast<int>(r->chunks.size()) - r->issued;
-                        if (left <= 0 || r->slot < 0) continue;
+                        if (left <= 0 || r->slot < 0 || r->cancelled) continue;
                         const int take = std::min(left, batch_chunks - n);
                         for (int i = 0; i < take; ++i) {
                             cx[n + i] = r->chunks[r->issued + i].x;
                             cz[n + i] = r->chunks[r->issued + i].z;
                             cs[n + i] = r->slot;
                         }
-                        pieces.push_back(Generator::Piece{r->blocks + static_cast<size_t>(r->issued) * kBlocksPerChunk,
-                                                          r->biomes ? r->biomes + static_cast<size_t>(r->issued) * kQuartsPerChunk : nullptr, nullptr, n, take});
+                        const size_t at = static_cast<size_t>(r->issued) * kBlocksPerChunk;
+                        Generator::Piece pc{r->blocks ? r->blocks + at : nullptr, r->biomes ? r->biomes + static_cast<size_t>(r->issued) * kQuartsPerChunk : nullptr,
+                                            nullptr, n, take};
+                        if (r->blocks8) {
+                            pc.blocks8 = r->blocks8 + at;
+                            narrow = true;
+                        }
+                        pieces.push_back(pc);
                         f.parts.push_back({r, take});
                         r->issued += take;
                         n += take;
@@ -1722,7 +2267,7 @@ struct Server {
                         flight.pop_front();
                     }
                     g->stage(o, n, cx.data(), cz.data(), cs.data());
-                    g->run_batch(o, n, nullptr, false);
+                    g->run_batch(o, n, nullptr, false, narrow);
                     g->drain(o, pieces);
                     f.out = oi;
                     flight.push_back(std::move(f));
@@ -1897,6 +2442,21 @@ tg_status tg_generate_batch(tg_generator* gen, const tg_request* requests, int32
     });
 }
 
+tg_status tg_generate_batch_device(tg_generator* gen, const tg_request_device* requests, int32_t n, int32_t flags, tg_timing* timing) {
+    return tb::guarded([&] {
+        usable(gen);
+        if (n < 0 || (n > 0 && !requests) || (flags & ~TG_BATCH_HOST_LOOP)) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        const auto t0 = std::chrono::steady_clock::now();
+        if (timing) std::memset(timing, 0, sizeof *timing);
+        tb::g_launches = 0;
+        gen->g->generate_batch_device(requests, n, (flags & TG_BATCH_HOST_LOOP) != 0, timing);
+        if (timing) {
+            timing->launches = tb::g_launches;
+            timing->wall_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+    });
+}
+
 tg_status tg_biome_lookup(tg_generator* gen, const int64_t* seeds, const int32_t* xyz, int32_t n, uint8_t* out) {
     return tb::guarded([&] {
         usable(gen);
@@ -1921,6 +2481,42 @@ tg_status tg_biome_lookup_noalloc(tg_generator* gen, const int32_t* xyz, int32_t
     });
 }
 
+tg_status tg_set_launch_table(tg_generator* gen, const char* text) {
+    return tb::guarded([&] {
+        usable(gen);
+        gen->g->set_launch_table(tb::parse_launch_table(text ? std::string(text) : std::string(tb::kLaunchTableText)));
+    });
+}
+
+tg_status tg_get_launch_table(tg_generator* gen, char* buf, size_t cap, size_t* needed) {
+    return tb::guarded([&] {
+        if (!gen) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "gen is null");
+        const std::string t = tb::format_launch_table(gen->g->lt);
+        if (needed) *needed = t.size() + 1;
+        if (buf && cap) {
+            const size_t n = std::min(cap - 1, t.size());
+            std::memcpy(buf, t.data(), n);
+            buf[n] = 0;
+        }
+    });
+}
+
+tg_status tg_kernel_times(tg_generator* gen, int32_t enable, float* ms, int32_t* calls, int32_t cap) {
+    return tb::guarded([&] {
+        usable(gen);
+        tb::Generator& g = *gen->g;
+        for (int i = 0; i < std::min<int>(cap, tb::K_COUNT); ++i) {
+            if (ms) ms[i] = static_cast<float>(g.prof_ms[i]);
+            if (calls) calls[i] = g.prof_calls[i];
+        }
+        for (int i = 0; i < tb::K_COUNT; ++i) {
+            g.prof_ms[i] = 0.0;
+            g.prof_calls[i] = 0;
+        }
+        g.prof = enable != 0;
+    });
+}
+
 tg_status tg_server_create(tg_generator* gen, const tg_server_config* config, tg_server** out) {
     return tb::guarded([&] {
         usable(gen);
@@ -1936,14 +2532,44 @@ tg_status tg_server_submit(tg_server* srv, int64_t seed, const tg_chunk_xz* chun
                            uint64_t* ticket) {
     return tb::guarded([&] {
         if (!srv || !ticket || count < 0 || (count > 0 && (!chunks || !blocks_out))) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
-        *ticket = srv->s->submit(seed, chunks, count, blocks_out, biomes_out);
+        *ticket = srv->s->submit(seed, chunks, count, blocks_out, nullptr, biomes_out);
+    });
+}
+
+tg_status tg_server_submit_u8(tg_server* srv, int64_t seed, const tg_chunk_xz* chunks, int32_t count, uint8_t* terrain_out, uint8_t* biomes_out,
+                              uint64_t* ticket) {
+    return tb::guarded([&] {
+        if (!srv || !ticket || count < 0 || (count > 0 && (!chunks || !terrain_out))) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        *ticket = srv->s->submit(seed, chunks, count, nullptr, terrain_out, biomes_out);
+    });
+}
+
+tg_status tg_server_cancel(tg_server* srv, uint64_t ticket, int32_t* was_pending) {
+    return tb::guarded([&] {
+        if (!srv) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        const bool p = srv->s->cancel(ticket);
+        if (was_pending) *was_pending = p ? 1 : 0;
+    });
+}
+
+tg_status tg_server_latencies(tg_server* srv, double* ms, int32_t cap, int32_t* n) {
+    return tb::guarded([&] {
+        if (!srv || cap < 0 || (cap > 0 && !ms)) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        const int k = srv->s->latencies(ms, cap);
+        if (n) *n = k;
     });
 }
 
 tg_status tg_server_wait(tg_server* srv, uint64_t ticket, int32_t timeout_ms, int32_t* done) {
     return tb::guarded([&] {
         if (!srv || !done) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
-        *done = srv->s->poll(ticket, timeout_ms);
+        *done = 0;
+        try {
+            *done = srv->s->poll(ticket, timeout_ms);
+        } catch (const tb::Error& e) {
+            if (e.code == TG_ERR_CANCELLED) *done = 1;
+            throw;
+        }
     });
 }
 

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'lib', 'libterrain_b200.so')
 
 STATUS = {0: 'TG_OK', 1: 'TG_ERR_INVALID_ARGUMENT', 2: 'TG_ERR_MODEL_MISMATCH', 3: 'TG_ERR_CUDA', 4: 'TG_ERR_OUT_OF_MEMORY', 5: 'TG_ERR_RANGE',
-          6: 'TG_ERR_NO_SEED', 7: 'TG_ERR_DEVICE_TIMEOUT', 8: 'TG_ERR_INTERNAL', 9: 'TG_ERR_IO'}
+          6: 'TG_ERR_NO_SEED', 7: 'TG_ERR_DEVICE_TIMEOUT', 8: 'TG_ERR_INTERNAL', 9: 'TG_ERR_IO', 10: 'TG_ERR_CANCELLED'}
 
 
 class TgChunk(ctypes.Structure):
@@ -41,6 +41,14 @@ class TgRequest(ctypes.Structure):
                 ('blocks_out', ctypes.POINTER(ctypes.c_uint16)), ('biomes_out', ctypes.POINTER(ctypes.c_uint8))]
 
 
+class TgRequestDevice(ctypes.Structure):
+    _fields_ = [('seed', ctypes.c_int64), ('chunks', ctypes.c_void_p), ('count', ctypes.c_int32), ('blocks_out', ctypes.c_void_p),
+                ('biomes_out', ctypes.c_void_p)]
+
+
+TG_BATCH_HOST_LOOP = 1
+
+
 class TgServerConfig(ctypes.Structure):
     _fields_ = [('batch_chunks', ctypes.c_int32), ('hbm_budget_bytes', ctypes.c_int64), ('reserved', ctypes.c_int32)]
 
@@ -48,17 +56,24 @@ class TgServerConfig(ctypes.Structure):
 class TgServerStats(ctypes.Structure):
     _fields_ = [('completed_requests', ctypes.c_int64), ('completed_chunks', ctypes.c_int64)] + \
                [(k, ctypes.c_double) for k in ('p50_ms', 'p99_ms', 'mean_ms', 'max_ms', 'chunks_per_s')] + \
-               [(k, ctypes.c_int32) for k in ('batches', 'queued_requests', 'active_requests')]
+               [(k, ctypes.c_int32) for k in ('batches', 'queued_requests', 'active_requests')] + \
+               [('cancelled_requests', ctypes.c_int64), ('device_bytes_per_chunk', ctypes.c_double), ('max_active_chunks', ctypes.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_write_region', 'tg_generate_device',
-           'tg_generate_density', 'tg_generate_batch', 'tg_biome_lookup',
+           'tg_generate_density', 'tg_generate_batch', 'tg_generate_batch_device', 'tg_biome_lookup',
            'tg_biome_lookup_noalloc',
-           'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
+           'tg_server_create', 'tg_server_submit', 'tg_server_submit_u8', 'tg_server_wait', 'tg_server_cancel', 'tg_server_get_stats',
+           'tg_server_latencies', 'tg_server_reset_stats', 'tg_server_destroy', 'tg_set_launch_table', 'tg_get_launch_table', 'tg_kernel_times',
            'tg_alloc_pinned', 'tg_free_pinned', 'tg_model_info', 'tg_last_error_string']
+
+# the tunable kernels of a batch, in pipeline order (tg_kernel_times order)
+KERNELS = ['nb_insert', 'nb_resolve', 'climate_col', 'climate_quart', 'chain', 'cc_insert', 'cc_resolve', 'corner_col', 'corner', 'zoom_table',
+           'zoom_uniform', 'sg_insert', 'sg_resolve', 'surface_level', 'aquifer_cell', 'aquifer_query', 'aquifer_skip', 'init_heights', 'fill',
+           'surface1', 'block_biome', 'walk_rules', 'surface_frozen', 'gather']
 
 
 class TerrainError(RuntimeError):
@@ -88,23 +103,31 @@ def load(path=LIB_PATH):
     L.tg_generate_device.argtypes = [vp, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(TgTiming)]
     L.tg_generate_density.argtypes = [vp, vp, ctypes.c_int32, vp]
     L.tg_generate_batch.argtypes = [vp, ctypes.POINTER(TgRequest), ctypes.c_int32, ctypes.POINTER(TgTiming)]
+    L.tg_generate_batch_device.argtypes = [vp, ctypes.POINTER(TgRequestDevice), ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(TgTiming)]
     L.tg_biome_lookup.argtypes = [vp, vp, vp, ctypes.c_int32, vp]
     L.tg_biome_lookup_noalloc.argtypes = [vp, vp, ctypes.c_int32, vp]
     L.tg_server_create.argtypes = [vp, ctypes.POINTER(TgServerConfig), ctypes.POINTER(vp)]
     L.tg_server_submit.argtypes = [vp, ctypes.c_int64, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.tg_server_submit_u8.argtypes = [vp, ctypes.c_int64, vp, ctypes.c_int32, vp, vp, ctypes.POINTER(ctypes.c_uint64)]
     L.tg_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
+    L.tg_server_cancel.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int32)]
+    L.tg_server_latencies.argtypes = [vp, vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
     L.tg_server_get_stats.argtypes = [vp, ctypes.POINTER(TgServerStats)]
     L.tg_server_reset_stats.argtypes = [vp]
     L.tg_server_destroy.argtypes = [vp]
+    L.tg_set_launch_table.argtypes = [vp, ctypes.c_char_p]
+    L.tg_get_launch_table.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
+    L.tg_kernel_times.argtypes = [vp, ctypes.c_int32, vp, vp, ctypes.c_int32]
     L.tg_alloc_pinned.argtypes = [ctypes.c_size_t]
     L.tg_alloc_pinned.restype = vp
     L.tg_free_pinned.argtypes = [vp]
     L.tg_model_info.argtypes = [ctypes.POINTER(ctypes.c_int32)] * 5
     L.tg_last_error_string.restype = ctypes.c_char_p
     for f in ('tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_generate', 'tg_generate_u8', 'tg_write_region', 'tg_generate_device',
-              'tg_generate_density', 'tg_generate_batch', 'tg_biome_lookup', 'tg_biome_lookup_noalloc',
-              'tg_server_create', 'tg_server_submit', 'tg_server_wait', 'tg_server_get_stats', 'tg_server_reset_stats', 'tg_server_destroy',
-              'tg_model_info'):
+              'tg_generate_density', 'tg_generate_batch', 'tg_generate_batch_device', 'tg_biome_lookup', 'tg_biome_lookup_noalloc',
+              'tg_server_create', 'tg_server_submit', 'tg_server_submit_u8', 'tg_server_wait', 'tg_server_cancel', 'tg_server_get_stats',
+              'tg_server_latencies', 'tg_server_reset_stats', 'tg_server_destroy',
+              'tg_set_launch_table', 'tg_get_launch_table', 'tg_kernel_times', 'tg_model_info'):
         getattr(L, f).restype = ctypes.c_int
     _lib = L
     return L
@@ -210,6 +233,25 @@ class TerrainGenerator:
         self._check(self.L.tg_generate_density(self.h, _ptr(a), n, _ptr(out)))
         return out
 
+    def set_launch_table(self, text=None):
+        """Launch shapes as text (None: the compiled-in, autotuned table)."""
+        self._check(self.L.tg_set_launch_table(self.h, text.encode() if text is not None else None))
+
+    def launch_table(self):
+        need = ctypes.c_size_t()
+        self._check(self.L.tg_get_launch_table(self.h, None, 0, ctypes.byref(need)))
+        buf = ctypes.create_string_buffer(need.value)
+        self._check(self.L.tg_get_launch_table(self.h, buf, need.value, None))
+        return buf.value.decode()
+
+    def kernel_times(self, enable=True):
+        """{kernel: (ms, launches)} gathered from timed batches since the last call; enable
+        switches the per-kernel events on or off from now on."""
+        ms = np.zeros(len(KERNELS), np.float32)
+        calls = np.zeros(len(KERNELS), np.int32)
+        self._check(self.L.tg_kernel_times(self.h, 1 if enable else 0, _ptr(ms), _ptr(calls), len(KERNELS)))
+        return {k: (float(ms[i]), int(calls[i])) for i, k in enumerate(KERNELS)}
+
     def generate_batch(self, requests, timing=False):
         """requests: list of (seed, chunks). Returns list of (blocks, biomes)."""
         outs, keep, reqs = [], [], (TgRequest * max(1, len(requests)))()
@@ -228,6 +270,18 @@ class TerrainGenerator:
         t = TgTiming() if timing else None
         self._check(self.L.tg_generate_batch(self.h, reqs, len(requests), ctypes.byref(t) if timing else None))
         return (outs, t.as_dict()) if timing else outs
+
+    def generate_batch_device(self, requests, host_loop=False, timing=False):
+        """requests: list of (seed, chunks_ptr, count, blocks_ptr, biomes_ptr or 0), device
+        pointers as ints (tg_generate_batch_device). Returns the timing dict with timing=True."""
+        reqs = (TgRequestDevice * max(1, len(requests)))()
+        for i, (seed, cp, n, bp, qp) in enumerate(requests):
+            reqs[i].seed, reqs[i].chunks, reqs[i].count = int(seed), cp, int(n)
+            reqs[i].blocks_out, reqs[i].biomes_out = bp, (qp or None)
+        t = TgTiming() if timing else None
+        self._check(self.L.tg_generate_batch_device(self.h, reqs, len(requests), TG_BATCH_HOST_LOOP if host_loop else 0,
+                                                    ctypes.byref(t) if timing else None))
+        return t.as_dict() if timing else None
 
     def biome_lookup(self, seeds, xyz):
         xyz = np.ascontiguousarray(np.asarray(xyz, np.int32).reshape(-1, 3))
@@ -260,26 +314,44 @@ class TerrainServer:
         gen._check(self.L.tg_server_create(gen.h, ctypes.byref(cfg), ctypes.byref(self.h)))
         self.pending = {}
 
-    def submit(self, seed, chunks, blocks_out=None, biomes_out=None):
+    def submit(self, seed, chunks, blocks_out=None, biomes_out=None, u8=False):
+        """Queues a request; u8=True asks for the u8 palette-index form (tg_server_submit_u8)."""
         a = chunk_array(chunks)
         n = a.shape[0]
         g = self.gen
-        blocks = blocks_out if blocks_out is not None else np.empty((n, g.height, 16, 16), np.uint16)
+        blocks = blocks_out if blocks_out is not None else np.empty((n, g.height, 16, 16), np.uint8 if u8 else np.uint16)
         biomes = biomes_out if biomes_out is not None else np.empty((n, g.qper), np.uint8)
         t = ctypes.c_uint64()
-        g._check(self.L.tg_server_submit(self.h, int(seed), _ptr(a), n, _ptr(blocks), _ptr(biomes), ctypes.byref(t)))
+        f = self.L.tg_server_submit_u8 if u8 else self.L.tg_server_submit
+        g._check(f(self.h, int(seed), _ptr(a), n, _ptr(blocks), _ptr(biomes), ctypes.byref(t)))
         self.pending[t.value] = (a, blocks, biomes)
         return t.value
 
     def poll(self, ticket, timeout_ms=0):
         done = ctypes.c_int32()
-        self.gen._check(self.L.tg_server_wait(self.h, ctypes.c_uint64(ticket), int(timeout_ms), ctypes.byref(done)))
+        st = self.L.tg_server_wait(self.h, ctypes.c_uint64(ticket), int(timeout_ms), ctypes.byref(done))
+        if st == 10:
+            self.pending.pop(ticket, None)
+        self.gen._check(st)
         return bool(done.value)
 
     def wait(self, ticket):
         self.poll(ticket, -1)
         _, blocks, biomes = self.pending.pop(ticket)
         return blocks, biomes
+
+    def cancel(self, ticket):
+        """True when the request was still pending (it will report TG_ERR_CANCELLED)."""
+        p = ctypes.c_int32()
+        self.gen._check(self.L.tg_server_cancel(self.h, ctypes.c_uint64(ticket), ctypes.byref(p)))
+        return bool(p.value)
+
+    def latencies(self):
+        n = ctypes.c_int32()
+        self.gen._check(self.L.tg_server_latencies(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1))
+        self.gen._check(self.L.tg_server_latencies(self.h, _ptr(out), out.shape[0], ctypes.byref(n)))
+        return out[:n.value]
 
     def stats(self):
         st = TgServerStats()

@@ -11,9 +11,15 @@
 
 #include "tb_pipeline.cuh"
 
+namespace tb {
+thread_local long long* tb_op_counts = nullptr;
+}
 using namespace tb;
 
 namespace {
+
+// stage sink when nothing is counted
+long long g_discard[kOpKinds];
 
 struct HostRun {
     ModelHost m;
@@ -64,6 +70,7 @@ struct Table {
     std::vector<unsigned long long> keys, uniq;
     std::vector<int32_t> vals, owner;
     int32_t count = 0;
+    uint32_t err = 0;
     uint32_t cap = 0;
     void init(size_t max_keys) {
         cap = 1024;
@@ -74,7 +81,7 @@ struct Table {
         uniq.assign(max_keys, 0);
         count = 0;
     }
-    HashTab view() { return HashTab{keys.data(), vals.data(), uniq.data(), &count, cap - 1, owner.data()}; }
+    HashTab view() { return HashTab{keys.data(), vals.data(), uniq.data(), &count, cap - 1, owner.data(), &err}; }
 };
 
 template <class F>
@@ -86,9 +93,17 @@ void each(int n, F f) {
 
 extern "C" {
 
-// Full pipeline for n chunks of one seed. blocks: n * 16 * 16 * height u16; biomes: n * 1536 u8
-// (may be null); aquifer: blocks after the fill (may be null).
-int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, uint16_t* blocks, uint8_t* biomes, uint16_t* aquifer) {
+// Stages of the pipeline in the order (and with the names) of the library's tunable kernels.
+enum Stage { S_NB_INSERT, S_NB_RESOLVE, S_CLIMATE_COL, S_CLIMATE_QUART, S_CHAIN, S_CC_INSERT, S_CC_RESOLVE, S_CORNER_COL, S_CORNER, S_ZOOM_TABLE,
+             S_ZOOM_UNIFORM, S_SG_INSERT, S_SG_RESOLVE, S_SURFACE_LEVEL, S_AQ_CELL, S_AQ_QUERY, S_AQ_SKIP, S_INIT_HEIGHTS, S_FILL, S_SURFACE1,
+             S_BLOCK_BIOME, S_WALK, S_FROZEN, S_GATHER, S_COUNT };
+
+// The pipeline for n chunks of one seed, stage by stage; with counts (S_COUNT x kOpKinds),
+// each stage's octave and simplex samples are counted into its row.
+int run_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, uint16_t* blocks, uint8_t* biomes, uint16_t* aquifer, long long* counts,
+                 int32_t* meta) {
+    auto stage = [&](int k) { tb_op_counts = counts ? counts + static_cast<size_t>(k) * kOpKinds : g_discard; };
+    tb_op_counts = g_discard;
     HostRun R(seed);
     std::vector<int32_t> vcx(cx, cx + n), vcz(cz, cz + n), vcs(n, 0);
     Table hb, hc, hs;
@@ -147,36 +162,80 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
     B.oremask = oremask.data();
     B.colmask = colmask.data();
     B.colrec = colrec.data();
+    stage(S_NB_INSERT);
     each(9 * n, [&](int i) { body_nb_insert(B, i); });
     each(9 * n, [&](int i) { ht_number(B.hb, nb_key(B, i), i); });
+    stage(S_NB_RESOLVE);
     each(9 * n, [&](int i) { body_nb_resolve(B, i); });
+    stage(S_CLIMATE_COL);
     each(hb.count * 16, [&](int i) { body_climate_col(B, i); });
+    stage(S_CLIMATE_QUART);
     each(hb.count * 16 * kRuns, [&](int i) { body_climate_quart(B, i); });
+    stage(S_CHAIN);
     each(hb.count, [&](int i) { body_chain(B, i); });
+    stage(S_CC_INSERT);
     each(25 * n, [&](int i) { body_cc_insert(B, i); });
     each(25 * n, [&](int i) { ht_number(B.hc, cc_key(B, i), i); });
+    stage(S_CC_RESOLVE);
     each(25 * n, [&](int i) { body_cc_resolve(B, i); });
+    stage(S_CORNER_COL);
     each(hc.count, [&](int i) { body_corner_col(B, i); });
+    stage(S_CORNER);
     each(hc.count * kRows, [&](int i) { body_corner(B, i); });
+    stage(S_ZOOM_TABLE);
     each(kZoomVerts * n, [&](int i) { body_zoom_table(B, i); });
+    stage(S_ZOOM_UNIFORM);
     each(kZoomCells * n, [&](int i) { body_zoom_uniform(B, i); });
+    stage(S_SG_INSERT);
     each(kGrid * n, [&](int i) { body_sg_insert(B, i); });
     each(kGrid * n, [&](int i) { ht_number(B.hs, sg_key_item(B, i), i); });
+    stage(S_SG_RESOLVE);
     each(kGrid * n, [&](int i) { body_sg_resolve(B, i); });
+    stage(S_SURFACE_LEVEL);
     each(hs.count, [&](int i) { body_surface_level(B, i); });
+    stage(S_AQ_CELL);
     each(kAqCells * n, [&](int i) { body_aquifer_cell(B, i); });
+    stage(S_AQ_QUERY);
     each(kAqQueries * n, [&](int i) { body_aquifer_query(B, i); });
+    stage(S_AQ_SKIP);
     each(n, [&](int i) { body_aquifer_skip(B, i); });
+    stage(S_FILL);
     each(256 * kCellsY * n, [&](int i) { body_fill(B, i); });
     if (aquifer) std::memcpy(aquifer, bl.data(), sizeof(uint16_t) * bl.size());
+    stage(S_SURFACE1);
     each(256 * n, [&](int i) { body_surface1(B, i); });
+    stage(S_BLOCK_BIOME);
     each(256 * n, [&](int i) { body_block_biome(B, i); });
+    stage(S_WALK);
     each(256 * n, [&](int i) { body_surface_walk_rules(B, i); });
+    stage(S_FROZEN);
     each(256 * n, [&](int i) { body_surface_frozen(B, i); });
+    stage(S_GATHER);
     each(kQuartsPerChunk * n, [&](int i) { body_gather(B, i); });
+    tb_op_counts = g_discard;
+    if (meta) {
+        meta[0] = hc.count;
+        meta[1] = hs.count;
+        meta[2] = hb.count;
+    }
     std::memcpy(blocks, bl.data(), sizeof(uint16_t) * bl.size());
     if (biomes) std::memcpy(biomes, bout.data(), bout.size());
     return 0;
+}
+
+// Full pipeline for n chunks of one seed. blocks: n * 16 * 16 * height u16; biomes: n * 1536 u8
+// (may be null); aquifer: blocks after the fill (may be null).
+int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, uint16_t* blocks, uint8_t* biomes, uint16_t* aquifer) {
+    return run_generate(seed, cx, cz, n, blocks, biomes, aquifer, nullptr, nullptr);
+}
+
+// The samples each stage evaluates for n chunks (one batch): counts is S_COUNT x kOpKinds
+// (volume, smeared volume, point, smeared point octave samples; simplex samples), and
+// meta[0..2] the batch's distinct corner columns, surface-level quarts and biome chunks.
+int hc_count_ops(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, long long* counts, int32_t* meta) {
+    std::vector<uint16_t> bl(static_cast<size_t>(n) * kBlocksPerChunk);
+    std::memset(counts, 0, sizeof(long long) * S_COUNT * kOpKinds);
+    return run_generate(seed, cx, cz, n, bl.data(), nullptr, nullptr, counts, meta);
 }
 
 // Point-path root values at positions (root: 0 barrier, 1 floodedness, 2 spread, 3 lava,
@@ -357,5 +416,24 @@ int64_t hc_zoom_seed(int64_t seed) {
     SeedHost s;
     build_seed_host(seed, s);
     return s.zoom_seed;
+}
+}
+
+extern "C" {
+// The dedupe tables' error bits on the host build of the same insert / resolve code: n keys
+// into a table of cap slots (a power of two), then every key resolved; returns the error
+// bits (kErrTableFull when the keys outnumber the slots, kErrKeyMissing for the keys left
+// out) and writes each resolved index (0 for a missing key) to idx.
+uint32_t hc_table_errors(int32_t n, uint32_t cap, int32_t* idx) {
+    std::vector<unsigned long long> keys(cap, kEmpty), uniq(static_cast<size_t>(n));
+    std::vector<int32_t> vals(cap, -1), owner(cap, 0x7F7F7F7F);
+    int32_t count = 0;
+    uint32_t err = 0;
+    const HashTab t{keys.data(), vals.data(), uniq.data(), &count, cap - 1, owner.data(), &err};
+    auto key = [](int i) { return pack_key(0, i, -i, 0); };
+    for (int i = 0; i < n; ++i) ht_insert(t, key(i), i);
+    for (int i = 0; i < n; ++i) ht_number(t, key(i), i);
+    for (int i = 0; i < n; ++i) idx[i] = ht_resolve(t, key(i));
+    return err;
 }
 }

@@ -30,6 +30,9 @@ def lib():
         L.hc_seed_scalars.argtypes = [ctypes.c_int64, vp, vp]
         L.hc_noise_layers.argtypes = [ctypes.c_int64, ctypes.c_int32, vp, vp, vp, vp]
         L.hc_biome_point.argtypes = [ctypes.c_int64, vp, ctypes.c_int32, vp]
+        L.hc_table_errors.argtypes = [ctypes.c_int32, ctypes.c_uint32, vp]
+        L.hc_count_ops.argtypes = [ctypes.c_int64, vp, vp, ctypes.c_int32, vp, vp]
+        L.hc_table_errors.restype = ctypes.c_uint32
         _L = L
     return _L
 
@@ -93,3 +96,29 @@ def noise_layers(seed, key_index):
     perms = np.zeros(128 * 256, np.uint8)
     n = lib().hc_noise_layers(int(seed), key_index, _p(f), _p(amp), _p(offs), _p(perms))
     return f[:n], amp[:n], offs[:3 * n].reshape(-1, 3), perms[:256 * n].reshape(-1, 256)
+
+
+def table_errors(n, cap):
+    """(error bits, resolved indices) of n keys through a cap-slot dedupe table (host build)."""
+    idx = np.zeros(n, np.int32)
+    e = lib().hc_table_errors(n, cap, _p(idx))
+    return int(e), idx
+
+
+STAGES = ['nb_insert', 'nb_resolve', 'climate_col', 'climate_quart', 'chain', 'cc_insert', 'cc_resolve', 'corner_col', 'corner', 'zoom_table',
+          'zoom_uniform', 'sg_insert', 'sg_resolve', 'surface_level', 'aquifer_cell', 'aquifer_query', 'aquifer_skip', 'init_heights', 'fill',
+          'surface1', 'block_biome', 'walk_rules', 'surface_frozen', 'gather']
+OP_KINDS = ['vol_octave', 'vol_octave_smeared', 'point_octave', 'point_octave_smeared', 'simplex']
+
+
+def count_ops(seed, chunks):
+    """Samples per stage of one batch of chunks through the host twin: ({stage: {kind: count}},
+    {'corner_columns', 'surface_quarts', 'biome_chunks'})."""
+    a = np.ascontiguousarray(np.asarray(chunks, np.int32).reshape(-1, 2))
+    cx, cz = np.ascontiguousarray(a[:, 0]), np.ascontiguousarray(a[:, 1])
+    counts = np.zeros((len(STAGES), len(OP_KINDS)), np.int64)
+    meta = np.zeros(4, np.int32)
+    if lib().hc_count_ops(int(seed), _p(cx), _p(cz), a.shape[0], _p(counts), _p(meta)) != 0:
+        raise RuntimeError('hc_count_ops failed')
+    per = {s: {k: int(counts[i, j]) for j, k in enumerate(OP_KINDS)} for i, s in enumerate(STAGES)}
+    return per, {'corner_columns': int(meta[0]), 'surface_quarts': int(meta[1]), 'biome_chunks': int(meta[2])}

@@ -101,3 +101,15 @@ def test_biome_point_lookups(ref_model, seed):
     near = np.stack([rng.integers(-40, 40, 300), rng.integers(-90, 345, 300), rng.integers(-40, 40, 300)], 1)
     xyz = np.ascontiguousarray(np.concatenate([far, near]).astype(np.int32))
     assert (hostcheck.biome_point(seed, xyz) == ref_model.seed(seed).biome_lookup(xyz)).all()
+
+
+def test_dedupe_table_errors_are_reported():
+    """The dedupe tables' invariant checks on the host build of the same code: keys within
+    the capacity number 0..n-1 with no error bit; more keys than slots set the full bit
+    (an insert found no slot) and the missing-key bit (their resolves give index 0, in
+    bounds), which the library turns into TG_ERR_INTERNAL instead of a silent wrong index."""
+    e, idx = hostcheck.table_errors(600, 1024)
+    assert e == 0 and sorted(idx.tolist()) == list(range(600))
+    e, idx = hostcheck.table_errors(1500, 1024)
+    assert e == 3                                   # kErrTableFull | kErrKeyMissing
+    assert idx.min() >= 0 and idx.max() < 1024
