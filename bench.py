@@ -63,6 +63,41 @@ OP_COUNTS = os.path.join(REPO, 'minecraft-terrain-cuda_b200', 'model', 'op_count
 METRIC = 'bit-exact TERRAIN chunks/s on 1 B200, served vs plain; p50/p99 request latency'
 
 
+def json_default(o):
+    """numpy scalars and arrays in the bench line as plain JSON values."""
+    if isinstance(o, np.generic):
+        return o.item()
+    if isinstance(o, np.ndarray):
+        return o.tolist()
+    raise TypeError('not JSON serializable: %r' % type(o))
+
+
+def model_sha256():
+    """SHA-256 of the world model files the library is built from (the workload's definition)."""
+    import hashlib
+    d = os.path.join(REPO, 'minecraft-terrain-cuda_b200', 'model')
+    return {f: hashlib.sha256(open(os.path.join(d, f), 'rb').read()).hexdigest() for f in ('overworld_ir.json', 'overworld_terrain.json')}
+
+
+def samples_per_chunk():
+    """Octave and simplex samples the kernels evaluate per chunk of a large region, counted on
+    the kernel bodies (op_counts.json): the work behind each chunk/s figure of this model."""
+    try:
+        with open(OP_COUNTS) as f:
+            doc = json.load(f)['kernels']
+    except (OSError, KeyError):
+        return None
+    u = doc['units_in_sample']
+    # units per chunk of a 64 x 64 region (distinct corner columns and biome chunks of the square;
+    # distinct surface-level quarts as in the counted sample)
+    per = {'corner': 257 * 257 * 49 / 4096.0, 'corner_col': 257 * 257 / 4096.0, 'climate_col': 66 * 66 / 4096.0, 'climate_quart': 66 * 66 / 4096.0,
+           'surface_level': u['surface_quarts'] / float(u['chunks'])}
+    total = 0.0
+    for name, rec in doc['per_kernel'].items():
+        total += sum(rec['samples_per_unit'].values()) * per.get(name, 1.0)
+    return round(total, 1)
+
+
 def region_chunks(x0, z0, side=SIDE):
     return np.array([(x0 + x, z0 + z) for z in range(side) for x in range(side)], np.int32)
 
@@ -572,6 +607,34 @@ def corner_roofline(stats, n, sms, clocks):
                     (per_point, points, n, per_sample)}
 
 
+def flythrough_bench(g, frames=90, radius=24, width=1280, height=720, speed=15.0):
+    """Live flythrough (tg_viewer_*): a 64 x 64-chunk window, the camera flying along +x at
+    `speed` blocks per frame at 110 blocks up, looking ahead and 12 degrees down; every frame
+    generates the chunks within `radius` that the window lacks (nearest first, at most 512)
+    straight into the window on the device, then ray traces a width x height frame (4 rays
+    per pixel, shadow rays). The first frame fills the window and is left out of the means.
+    Times are CUDA events of the generation and window update, and of the render kernel."""
+    import terrain_b200
+    g.set_seed(SEED)
+    gen_ms, chunks, render_ms = [], [], []
+    with terrain_b200.TerrainViewer(g, window_chunks=64, width=width, height=height) as v:
+        x, z = 8.0, 8.0
+        for f in range(frames + 1):
+            n, ms = v.update(int(np.floor(x / 16)), int(np.floor(z / 16)), radius, cap=512, frame=f)
+            _, _, rms = v.render(terrain_b200.camera(x, 110.0, z, yaw_deg=90.0, pitch_deg=-12.0, fog=radius * 16.0), f, rgb=f == frames)
+            if f > 0:
+                gen_ms.append(ms)
+                chunks.append(n)
+                render_ms.append(rms)
+            x += speed
+    return {'frames': frames, 'frame': '%dx%d' % (width, height), 'radius_chunks': radius, 'speed_blocks_per_frame': speed,
+            'chunks_per_frame': round(float(np.mean(chunks)), 1), 'generate_ms_per_frame': round(float(np.mean(gen_ms)), 3),
+            'render_ms_per_frame': round(float(np.mean(render_ms)), 3), 'render_ms_p99': round(float(np.quantile(render_ms, 0.99)), 3),
+            'frames_per_s_render_and_generate': round(1000.0 / (float(np.mean(gen_ms)) + float(np.mean(render_ms))), 1),
+            'form': 'tg_viewer_update (chunks generated on the device into the voxel window) + tg_viewer_render (2x2 rays per pixel, '
+                    'shadow rays, 4x4-column empty-space skipping)'}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import terrain_b200
@@ -669,6 +732,7 @@ def run_ours(args, rank, world, local_rank):
         'data': 'synthetic world model (project-authored, reference JSON formats); seeded chunk lists',
         'config': {'workload': 'ladder: one seed, three 64x64-chunk regions (origin, -1,000,000 blocks, +1,874,999-block border), 12,288 chunks per step',
                    'seed': SEED, 'chunks_per_step': n * nreg, 'batch_chunks': n, 'l2': 'outputs (2.4 GB per step) larger than L2',
+                   'model_sha256': model_sha256(), 'samples_per_chunk': samples_per_chunk(),
                    'parallelism': 'replicas: each GPU runs the full workload' if world > 1 else 'single GPU'},
         'stage_ms_per_step': {k: round(v, 3) for k, v in stage.items()},
         'roofline': roofline,
@@ -695,6 +759,7 @@ def run_ours(args, rank, world, local_rank):
         g.set_stream(0)
         line['batched'] = batched_bench(g)
         line['biome_stream'] = biome_stream_bench(g)
+        line['flythrough'] = flythrough_bench(g)
     if not args.no_reference_gpu:
         line['reference_gpu'] = reference_gpu_bench()
         if line['reference_gpu']:
@@ -703,7 +768,7 @@ def run_ours(args, rank, world, local_rank):
             rg['ours_over_reference_e2e'] = round(e2e_value / rg['e2e_chunks_per_s'], 3)
     if not args.no_cpu_baseline:
         line['cpu_baseline'] = cpu_baseline()
-    print(json.dumps(line))
+    print(json.dumps(line, default=json_default))
 
 
 def main():

@@ -236,6 +236,56 @@ tg_status tg_server_reset_stats(struct tg_server* srv);
 /* Finishes the work in flight, then stops the worker. */
 tg_status tg_server_destroy(struct tg_server* srv);
 
+/* ---- live flythrough renderer -----------------------------------------------------------
+ * A viewer keeps a toroidal window of window_chunks x window_chunks generated chunks on the
+ * device (u8 palette index per block) and ray traces frames of it. tg_viewer_update
+ * generates the chunks within a radius of the camera's chunk that the window does not hold,
+ * nearest first, with the generator (its seed of tg_set_seed) straight into the window: the
+ * blocks never leave the device. tg_viewer_render traces one width x height frame: 2 x 2
+ * rays per pixel through the voxels (whole 4 x 4-column cells skipped while a ray stays
+ * above their blocks, water seen through), a shadow ray toward the sun, ambient occlusion,
+ * water tint and reflection, distance haze. The generator serves the viewer on the same
+ * host thread (not while a server owns it).
+ * reference: the flythrough renderer viz/fly.cu (k_render :249-310, k_scatter :312-320,
+ * k_cells :322-334, the frame loop :486-560), which copies each chunk to the host and back. */
+typedef struct tg_viewer_config {
+    int32_t window_chunks;   /* window side in chunks, a multiple of 4 in 4..256; 0 = 64 */
+    int32_t width, height;   /* frame size; 0 = 1280 x 720 */
+    int32_t reserved;
+} tg_viewer_config;
+
+typedef struct tg_camera {
+    float x, y, z;                 /* eye position, blocks */
+    float yaw_deg, pitch_deg;      /* yaw 0 looks along +z, 90 along +x; pitch > 0 looks up */
+    float fov_deg;                 /* vertical field of view; 0 = 70 */
+    float sun_x, sun_y, sun_z;     /* direction toward the sun (any length > 0) */
+    float fog;                     /* haze distance in blocks; 0 = the window's reach */
+} tg_camera;
+
+tg_status tg_viewer_create(struct tg_generator* gen, const tg_viewer_config* config, struct tg_viewer** out);
+/* Generates up to cap (0: max_batch_chunks) missing chunks within radius (at most
+ * window_chunks / 2 - 1) of chunk (cx, cz), marking them born at frame; *generated (may
+ * be NULL) receives their number and *ms (may be NULL) the device time of the generation
+ * and window update. */
+tg_status tg_viewer_update(struct tg_viewer* viewer, int32_t cx, int32_t cz, int32_t radius, int32_t cap, int32_t frame, int32_t* generated, float* ms);
+/* Traces one frame. rgb_out (may be NULL): width * height * 3 u8, rows top to bottom;
+ * hits_out (may be NULL): per pixel 4 int32 {palette index or -1, x, y, z} of the first
+ * ray's hit; ms (may be NULL): the render kernel's device time. Chunks generated within 8
+ * frames before frame are tinted green. */
+tg_status tg_viewer_render(struct tg_viewer* viewer, const tg_camera* camera, int32_t frame, uint8_t* rgb_out, int32_t* hits_out, float* ms);
+/* The window state for checks (each may be NULL): voxels (height * (16 * window_chunks)^2
+ * u8, [y][z][x]), cells ((4 * window_chunks)^2 u32: 1 + highest non-air height index per
+ * 4 x 4-column cell), slots (2 * window_chunks^2 int32: chunk x, z held per slot, INT32_MIN
+ * when empty), born (window_chunks^2 int32). */
+tg_status tg_viewer_state(struct tg_viewer* viewer, uint8_t* voxels, uint32_t* cells, int32_t* slots, int32_t* born);
+/* The parameters a frame is traced with, for checks (each may be NULL): the camera record
+ * (18 floats: eye, forward, right, up, tan(fov / 2), aspect, unit sun direction, haze
+ * distance), the linear colours of the palette (64 x 3 floats of top faces, 64 x 3 of
+ * sides), capped texel rows (64 int32), and {window_chunks, air, water, lava, bedrock,
+ * min_y, height}. */
+tg_status tg_viewer_params(struct tg_viewer* viewer, const tg_camera* camera, float* cam_out, float* top, float* side, int32_t* caps, int32_t* ids);
+tg_status tg_viewer_destroy(struct tg_viewer* viewer);
+
 /* ---- launch shapes and per-kernel times (the autotuner's interface) -----------------------
  * The batch pipeline's kernels run in the shapes of a launch table: the autotuned table
  * compiled into the library (minecraft-terrain-cuda_b200/tuning/launch_table.txt) unless one
@@ -248,8 +298,8 @@ tg_status tg_server_destroy(struct tg_server* srv);
  * pipeline order: nb_insert nb_resolve climate_col climate_quart chain cc_insert cc_resolve
  * corner_col corner zoom_table zoom_uniform sg_insert sg_resolve surface_level aquifer_cell
  * aquifer_query aquifer_skip init_heights fill surface1 block_biome walk_rules
- * surface_frozen gather (the chain kernel has no work-queue form). Results do not depend
- * on the table. No counterpart in the reference (its launch shapes are constants). */
+ * surface_frozen gather axis_insert axis_number axis_fill (the chain kernel has no
+ * work-queue form). Results do not depend on the table. No counterpart in the reference (its launch shapes are constants). */
 tg_status tg_set_launch_table(struct tg_generator* gen, const char* text);   /* NULL: the compiled-in table */
 /* The table in use, as text (needed: its size with the terminating zero). */
 tg_status tg_get_launch_table(struct tg_generator* gen, char* buf, size_t cap, size_t* needed);

@@ -305,6 +305,71 @@ TB_HD TB_NOINLINE inline float stack_point_smeared_rt(const NoiseTables& T, int 
     return acc;
 }
 
+// The x or z coordinate record of one octave layer at one coordinate, precomputed per batch
+// (axis_setup of the coordinate, the stack's xz scale times the layer frequency, and the
+// octave's x or z offset): the corner kernel's columns share x and z across their 49 rows
+// and across neighbouring columns, so the tables replace most of an octave's FP64 work by
+// two 16-byte loads.
+struct AxisRec {
+    int32_t f;
+    float r, a;
+    int32_t pad;
+};
+#ifndef TB_AXIS_TABLE
+#define TB_AXIS_TABLE 1
+#endif
+#if TB_AXIS_TABLE
+#define TB_AXIS_SEL(table, plain) (table)
+#else
+#define TB_AXIS_SEL(table, plain) (plain)
+#endif
+
+// stack_volume_rt with the x / z records of layer first + k at ax[k], az[k]
+TB_HD TB_NOINLINE inline float stack_volume_ax_rt(const NoiseTables& T, int first, int count, const AxisRec* ax, const AxisRec* az, int32_t by, double yss,
+                                                   float amplitude) {
+    float acc = 0.0f;
+#pragma unroll 1
+    for (int k = 0; k < count; ++k) {
+        TB_COUNT(kOpVolume);
+        const Layer L = T.layer[first + k];
+        const double ys = yss * L.freq;
+        const float amp = amplitude * L.amp;
+        const AxisRec X = ax[k], Z = az[k];
+        const AxisSetup Y = axis_setup(by, ys, T.off[L.oct].oy);
+        const CellHash c = octave_hash(T, L.oct, X.f, Y.f, Z.f);
+        acc = acc + amp * cell_volume(c, X.r, Z.r, Y.r, X.a, Y.a, Z.a);
+    }
+    return acc;
+}
+
+TB_HD TB_NOINLINE inline float stack_volume_smeared_ax_rt(const NoiseTables& T, int first, int count, const AxisRec* ax, const AxisRec* az, int32_t by,
+                                                           double yss, float amplitude) {
+    float acc = 0.0f;
+#pragma unroll 1
+    for (int k = 0; k < count; ++k) {
+        TB_COUNT(kOpVolumeSmeared);
+        const Layer L = T.layer[first + k];
+        const double ys = yss * L.freq;
+        const float amp = amplitude * L.amp;
+        const AxisRec X = ax[k], Z = az[k];
+        const OctaveOff o = T.off[L.oct];
+        const double oy = static_cast<double>(by) * ys;
+        const double y = nwrap(oy) + o.oy;
+        const int32_t fy = jfloor_finite(y);
+        const double rel = y - static_cast<double>(fy);
+        const float ay = smoothf(static_cast<float>(rel));
+        const CellHash c = octave_hash(T, L.oct, X.f, fy, Z.f);
+        const float fudged = static_cast<float>(rel - smear_fudge(oy, rel, o.smear));
+        acc = acc + amp * cell_volume(c, X.r, Z.r, fudged, X.a, ay, Z.a);
+    }
+    return acc;
+}
+
+template <int FIRST, int COUNT, bool SMEARED>
+TB_HD TB_FI float stack_volume_ax(const NoiseTables& T, const AxisRec* ax, const AxisRec* az, int32_t by, double yss, float amplitude) {
+    return SMEARED ? stack_volume_smeared_ax_rt(T, FIRST, COUNT, ax, az, by, yss, amplitude) : stack_volume_ax_rt(T, FIRST, COUNT, ax, az, by, yss, amplitude);
+}
+
 template <int FIRST, int COUNT, bool SMEARED>
 TB_HD TB_FI float stack_volume(const NoiseTables& T, int32_t bx, int32_t by, int32_t bz, double xzs, double yss, float amplitude) {
     return SMEARED ? stack_volume_smeared_rt(T, FIRST, COUNT, bx, by, bz, xzs, yss, amplitude) : stack_volume_rt(T, FIRST, COUNT, bx, by, bz, xzs, yss, amplitude);

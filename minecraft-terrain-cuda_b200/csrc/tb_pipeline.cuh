@@ -139,6 +139,11 @@ struct Batch {
     int32_t cc_cap;
     int32_t* c25;                     // n * 25 corner-column indices, (k) * 5 + i
     float* ccol;                      // cc_cap * kCornerCols
+    // per-batch axis tables of the corner kernel: the distinct corner x (and z) coordinates
+    // of each seed slot, and per coordinate the x (z) record of every axis-table layer
+    HashTab ha;                       // keys (slot, qx, 0, 0) and (slot, 0, qz, 1)
+    AxisRec* axtab;                   // ha's keys * kAxisLayers
+    int32_t* colax;                   // cc_cap * 2: per corner column its x row and z row of axtab
     float* corners;                   // cc_cap * kRows * kNumChannels
     // surface-level quarts (find_top_surface), volume or point semantics
     HashTab hs;
@@ -817,11 +822,52 @@ TB_HD inline void body_chain(const Batch& B, int b) {
 }
 
 // ---- corner channels ----------------------------------------------------------------------------
+// ---- axis tables of the corner kernel ------------------------------------------------------------
+// item = corner column * 2 + (0: its x, 1: its z)
+TB_HD TB_FI unsigned long long axis_key(const Batch& B, int it) {
+    int32_t slot, qx, qz, sem;
+    unpack_key(B.hc.uniq[it >> 1], slot, qx, qz, sem);
+    return (it & 1) ? pack_key(slot, 0, qz, 1) : pack_key(slot, qx, 0, 0);
+}
+TB_HD inline void body_axis_insert(const Batch& B, int it) { ht_insert(B.ha, axis_key(B, it), it); }
+// numbering in arrival order: the table rows are found by lookup, so their order is free
+TB_HD inline void body_axis_number(const Batch& B, int it) {
+    const unsigned long long key = axis_key(B, it);
+    const uint32_t s = ht_slot(B.ha, key);
+    if (s > B.ha.mask || B.ha.owner[s] != it) return;
+    const int32_t idx = add32(B.ha.count, 1);
+    B.ha.vals[s] = idx;
+    B.ha.uniq[idx] = key;
+}
+// item = row * kAxisLayers + entry: the x (or z) record of one axis-table layer at one
+// coordinate, the arithmetic of axis_setup in the octave it replaces
+TB_HD inline void body_axis_fill(const Batch& B, int it) {
+    if (tbm::kAxisLayers == 0) return;
+    const int row = it / tbm::kAxisLayers, e = it % tbm::kAxisLayers;
+    int32_t slot, qx, qz, sem;
+    unpack_key(B.ha.uniq[row], slot, qx, qz, sem);
+    const NoiseTables& T = B.seeds[slot].nt;
+#if defined(__CUDA_ARCH__)
+    const Layer L = T.layer[tbm::kAxisLayerDev[e]];
+    const double scale = tbm::kAxisScaleDev[e] * L.freq;
+#else
+    const Layer L = T.layer[tbm::kAxisLayer[e]];
+    const double scale = tbm::kAxisScale[e] * L.freq;
+#endif
+    const OctaveOff o = T.off[L.oct];
+    const AxisSetup a = axis_setup((sem ? qz : qx) * 4, scale, sem ? o.oz : o.ox);
+    B.axtab[static_cast<size_t>(row) * tbm::kAxisLayers + e] = AxisRec{a.f, a.r, a.a, 0};
+}
+
 TB_HD inline void body_corner_col(const Batch& B, int u) {
     if (u >= *B.hc.count) return;
     int32_t slot, qx, qz, sem;
     unpack_key(B.hc.uniq[u], slot, qx, qz, sem);
     tbgen::gen_corner_col(B.seeds[slot].nt, qx * 4, qz * 4, B.ccol + static_cast<size_t>(u) * tbm::kCornerCols);
+#if TB_AXIS_TABLE
+    B.colax[2 * u] = ht_resolve(B.ha, pack_key(slot, qx, 0, 0));
+    B.colax[2 * u + 1] = ht_resolve(B.ha, pack_key(slot, 0, qz, 1));
+#endif
 }
 // item = row * count + column: a warp evaluates one corner row over neighbouring
 // columns, where the lazy branches (surface, caves, blended-noise limits) agree most.
@@ -831,7 +877,14 @@ TB_HD inline void body_corner(const Batch& B, int it) {
     if (row >= kRows) return;
     int32_t slot, qx, qz, sem;
     unpack_key(B.hc.uniq[u], slot, qx, qz, sem);
-    tbgen::gen_corner(B.seeds[slot].nt, qx * 4, tbm::kMinY + 8 * row, qz * 4, B.ccol + static_cast<size_t>(u) * tbm::kCornerCols,
+#if TB_AXIS_TABLE
+    const AxisRec* ax = B.axtab + static_cast<size_t>(B.colax[2 * u]) * tbm::kAxisLayers;
+    const AxisRec* az = B.axtab + static_cast<size_t>(B.colax[2 * u + 1]) * tbm::kAxisLayers;
+#else
+    const AxisRec* ax = nullptr;
+    const AxisRec* az = nullptr;
+#endif
+    tbgen::gen_corner(B.seeds[slot].nt, qx * 4, tbm::kMinY + 8 * row, qz * 4, B.ccol + static_cast<size_t>(u) * tbm::kCornerCols, ax, az,
                       B.corners + (static_cast<size_t>(u) * kRows + row) * tbm::kNumChannels);
 }
 

@@ -24,6 +24,7 @@
 #include <atomic>
 #include <chrono>
 #include <climits>
+#include <cmath>
 #include <condition_variable>
 #include <cstdio>
 #include <cstring>
@@ -42,6 +43,7 @@
 #include "../../include/terrain_b200.h"
 #include "launch_table.h"   // generated from tuning/launch_table.txt: kLaunchTableText
 #include "tb_pipeline.cuh"
+#include "tb_viewer.cuh"
 
 namespace tb {
 namespace {
@@ -570,12 +572,12 @@ void launch(K kernel, cudaStream_t s, long items_hint, Args... args) {
 enum KernelId {
     K_NB_INSERT, K_NB_RESOLVE, K_CLIMATE_COL, K_CLIMATE_QUART, K_CHAIN, K_CC_INSERT, K_CC_RESOLVE, K_CORNER_COL, K_CORNER, K_ZOOM_TABLE,
     K_ZOOM_UNIFORM, K_SG_INSERT, K_SG_RESOLVE, K_SURFACE_LEVEL, K_AQ_CELL, K_AQ_QUERY, K_AQ_SKIP, K_INIT_HEIGHTS, K_FILL, K_SURFACE1,
-    K_BLOCK_BIOME, K_WALK, K_FROZEN, K_GATHER, K_COUNT
+    K_BLOCK_BIOME, K_WALK, K_FROZEN, K_GATHER, K_AXIS_INSERT, K_AXIS_NUMBER, K_AXIS_FILL, K_COUNT
 };
 const char* const kKernelNames[K_COUNT] = {"nb_insert", "nb_resolve", "climate_col", "climate_quart", "chain", "cc_insert", "cc_resolve",
                                            "corner_col", "corner", "zoom_table", "zoom_uniform", "sg_insert", "sg_resolve", "surface_level",
                                            "aquifer_cell", "aquifer_query", "aquifer_skip", "init_heights", "fill", "surface1", "block_biome",
-                                           "walk_rules", "surface_frozen", "gather"};
+                                           "walk_rules", "surface_frozen", "gather", "axis_insert", "axis_number", "axis_fill"};
 
 struct LaunchShape {
     int threads = 256;        // 32 .. 256, a multiple of 32 (the kernels are built for at most 256)
@@ -723,14 +725,20 @@ struct OutSlot {
 // two output slots run concurrently on two streams.
 struct Work {
     DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_cell,
-        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_zoom_uni, d_bbiome, d_oremask, d_colmask, d_colrec, d_qnext, d_err;
-    TableBufs tb_b, tb_c, tb_s;
+        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_zoom_uni, d_bbiome, d_oremask, d_colmask, d_colrec, d_qnext, d_err, d_axtab, d_colax;
+    TableBufs tb_b, tb_c, tb_s, tb_a;
     void alloc(int n, int load) {
         const size_t N = static_cast<size_t>(n);
         d_n.alloc(sizeof(int32_t));
         d_err.alloc(sizeof(uint32_t));
         ck(cudaMemset(d_err.p, 0, sizeof(uint32_t)), "memset");
-        tb_b.err = tb_c.err = tb_s.err = d_err.as<uint32_t>();
+        tb_b.err = tb_c.err = tb_s.err = tb_a.err = d_err.as<uint32_t>();
+        if (TB_AXIS_TABLE) {
+            // at most 5 distinct corner x and 5 distinct corner z per chunk
+            tb_a.alloc(10 * N, load);
+            d_axtab.alloc(sizeof(AxisRec) * 10 * N * std::max(1, tbm::kAxisLayers));
+            d_colax.alloc(sizeof(int32_t) * 2 * 25 * N);
+        }
         d_qnext.alloc(sizeof(int32_t) * K_COUNT);   // work-queue counters, one per kernel
         d_cx.alloc(4 * N);
         d_cz.alloc(4 * N);
@@ -931,9 +939,9 @@ struct Generator {
             const Work& W = work[l];
             for (const DevBuf* d : {&W.d_cx, &W.d_cz, &W.d_cs, &W.d_nb9, &W.d_bcol, &W.d_tgt, &W.d_lstar, &W.d_mdist, &W.d_qbiome, &W.d_c25, &W.d_ccol,
                                     &W.d_corners, &W.d_g513, &W.d_sfts, &W.d_aq_cell, &W.d_aq_query, &W.d_aq_skip, &W.d_h0, &W.d_h1, &W.d_h2,
-                                    &W.d_zoom, &W.d_zoom_uni, &W.d_bbiome, &W.d_oremask, &W.d_colmask, &W.d_colrec})
+                                    &W.d_zoom, &W.d_zoom_uni, &W.d_bbiome, &W.d_oremask, &W.d_colmask, &W.d_colrec, &W.d_axtab, &W.d_colax})
                 b += d->bytes;
-            for (const TableBufs* t : {&W.tb_b, &W.tb_c, &W.tb_s}) b += t->keys.bytes + t->vals.bytes + t->uniq.bytes + t->owner.bytes;
+            for (const TableBufs* t : {&W.tb_b, &W.tb_c, &W.tb_s, &W.tb_a}) b += t->keys.bytes + t->vals.bytes + t->uniq.bytes + t->owner.bytes;
         }
         for (const OutSlot& o : out) b += o.blocks.bytes + o.biomes.bytes + o.blocks8.bytes;
         return static_cast<double>(b) / static_cast<double>(max_batch);
@@ -1029,6 +1037,9 @@ struct Generator {
         B.cc_cap = 25 * max_batch;
         B.c25 = W.d_c25.as<int32_t>();
         B.ccol = W.d_ccol.as<float>();
+        B.ha = W.tb_a.view();
+        B.axtab = W.d_axtab.as<AxisRec>();
+        B.colax = W.d_colax.as<int32_t>();
         B.corners = W.d_corners.as<float>();
         B.hs = W.tb_s.view();
         B.sg_cap = kGrid * max_batch;
@@ -1111,6 +1122,13 @@ struct Generator {
         run_body<body_cc_insert, 25>(K_CC_INSERT, W, s, 25 * nmax, B, n_dev);
         launch(k_number<1, cc_key, 25>, s, 25 * nmax, B);
         run_body<body_cc_resolve, 25>(K_CC_RESOLVE, W, s, 25 * nmax, B, n_dev);
+        if (TB_AXIS_TABLE && tbm::kAxisLayers > 0) {
+            const int32_t* cnt_a = W.tb_a.count.as<int32_t>();
+            W.tb_a.reset(s);
+            run_body<body_axis_insert, 2>(K_AXIS_INSERT, W, s, 2 * 16 * nmax, B, cnt_c);
+            run_body<body_axis_number, 2>(K_AXIS_NUMBER, W, s, 2 * 16 * nmax, B, cnt_c);
+            run_body<body_axis_fill, std::max(1, tbm::kAxisLayers)>(K_AXIS_FILL, W, s, 2L * nmax * std::max(1, tbm::kAxisLayers), B, cnt_a);
+        }
         run_body<body_corner_col, 1>(K_CORNER_COL, W, s, 16 * nmax, B, cnt_c);
         mark(8);
         run_body<body_corner, kRows, TB_MINB_CORNER>(K_CORNER, W, s, 16 * nmax * kRows, B, cnt_c);
@@ -2287,6 +2305,210 @@ struct Server {
     }
 };
 
+// ---- live flythrough renderer -----------------------------------------------------------------------
+// Flat block colours by name (sRGB), this renderer's own choice; palette entries match by
+// the name before any state properties. Grass, podzol and mycelium show dirt on their sides
+// under a capped top.
+struct BlockColour {
+    const char* name;
+    uint8_t r, g, b;
+};
+const BlockColour kBlockColours[] = {
+    {"minecraft:stone", 125, 125, 125},          {"minecraft:water", 40, 86, 170},            {"minecraft:lava", 220, 96, 20},
+    {"minecraft:terracotta", 150, 93, 66},       {"minecraft:white_terracotta", 208, 176, 160}, {"minecraft:orange_terracotta", 160, 84, 38},
+    {"minecraft:yellow_terracotta", 185, 131, 36}, {"minecraft:brown_terracotta", 77, 52, 36}, {"minecraft:red_terracotta", 142, 60, 46},
+    {"minecraft:light_gray_terracotta", 134, 106, 97}, {"minecraft:packed_ice", 140, 178, 248}, {"minecraft:snow_block", 240, 245, 248},
+    {"minecraft:bedrock", 58, 58, 58},           {"minecraft:deepslate", 78, 78, 82},         {"minecraft:grass_block", 90, 128, 56},
+    {"minecraft:dirt", 133, 95, 66},             {"minecraft:sand", 218, 206, 160},           {"minecraft:sandstone", 214, 201, 152},
+    {"minecraft:gravel", 130, 126, 125},         {"minecraft:red_sand", 189, 101, 34},        {"minecraft:coarse_dirt", 118, 84, 58},
+    {"minecraft:podzol", 90, 62, 25},            {"minecraft:mycelium", 110, 98, 104},        {"minecraft:calcite", 222, 223, 219},
+    {"minecraft:ice", 146, 182, 252},            {"minecraft:powder_snow", 247, 252, 252},    {"minecraft:mud", 61, 57, 60},
+    {"minecraft:tuff", 107, 108, 101},           {"minecraft:granite", 148, 102, 85},         {"minecraft:copper_ore", 124, 124, 118},
+    {"minecraft:raw_copper_block", 153, 104, 78}, {"minecraft:iron_ore", 136, 129, 122},     {"minecraft:raw_iron_block", 165, 135, 106},
+    {"minecraft:moss_block", 89, 110, 45},       {"minecraft:clay", 160, 166, 179},           {"minecraft:smooth_basalt", 72, 72, 78},
+    {"minecraft:dripstone_block", 134, 107, 92}, {"minecraft:red_sandstone", 180, 97, 32},    {"minecraft:air", 0, 0, 0},
+};
+
+// The linear colour table of the compiled palette (a name missing from kBlockColours is grey).
+ViewColours palette_colours() {
+    static_assert(tbm::kPaletteSize <= kViewPalette, "palette larger than the renderer's colour table");
+    ViewColours c{};
+    auto lin = [](uint8_t v) { return std::pow(static_cast<float>(v) / 255.0f, 2.2f); };
+    auto find = [&](const std::string& n, float* out) {
+        for (const BlockColour& b : kBlockColours)
+            if (n == b.name) {
+                out[0] = lin(b.r);
+                out[1] = lin(b.g);
+                out[2] = lin(b.b);
+                return;
+            }
+        out[0] = out[1] = out[2] = lin(128);
+    };
+    for (int i = 0; i < tbm::kPaletteSize; ++i) {
+        const std::string full = tbm::kPaletteNames[i];
+        const std::string n = full.substr(0, full.find('['));
+        find(n, c.top[i]);
+        find(n, c.side[i]);
+        if (n == "minecraft:grass_block" || n == "minecraft:podzol" || n == "minecraft:mycelium") {
+            find("minecraft:dirt", c.side[i]);
+            c.cap[i] = n == "minecraft:grass_block" ? 3 : 2;
+        }
+    }
+    return c;
+}
+
+struct Viewer {
+    Generator* g;
+    int W, WB, WC, width, height;
+    DevBuf vox, cells, d_slot, d_born, d_coords, d_chunks, d_frame, d_hits, d_colours;
+    PinBuf h_frame;
+    std::vector<int2> slot;
+    std::vector<int32_t> born;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+
+    Viewer(Generator* gen, const tg_viewer_config* cfg) : g(gen) {
+        W = cfg && cfg->window_chunks > 0 ? cfg->window_chunks : 64;
+        width = cfg && cfg->width > 0 ? cfg->width : 1280;
+        height = cfg && cfg->height > 0 ? cfg->height : 720;
+        if (W < 4 || W > 256 || W % 4) throw Error(TG_ERR_INVALID_ARGUMENT, "window_chunks must be a multiple of 4 in 4..256");
+        if (width > 8192 || height > 8192) throw Error(TG_ERR_INVALID_ARGUMENT, "frame larger than 8192 pixels on a side");
+        WB = W * 16;
+        WC = WB / kViewCell;
+        const size_t plane = static_cast<size_t>(WB) * WB;
+        vox.alloc(plane * tbm::kHeight);
+        ck(cudaMemset(vox.p, tbm::kAir, vox.bytes), "memset");
+        cells.alloc(sizeof(uint32_t) * WC * WC);
+        ck(cudaMemset(cells.p, 0, cells.bytes), "memset");
+        slot.assign(static_cast<size_t>(W) * W, make_int2(INT32_MIN, INT32_MIN));
+        born.assign(static_cast<size_t>(W) * W, -1000000);
+        d_slot.alloc(sizeof(int2) * slot.size());
+        d_born.alloc(sizeof(int32_t) * born.size());
+        ck(cudaMemcpy(d_slot.p, slot.data(), d_slot.bytes, cudaMemcpyHostToDevice), "h2d");
+        ck(cudaMemcpy(d_born.p, born.data(), d_born.bytes, cudaMemcpyHostToDevice), "h2d");
+        d_coords.alloc(sizeof(int2) * g->max_batch);
+        d_chunks.alloc(sizeof(tg_chunk_xz) * g->max_batch);
+        d_frame.alloc(static_cast<size_t>(width) * height * 3);
+        d_hits.alloc(sizeof(int4) * static_cast<size_t>(width) * height);
+        const ViewColours col = palette_colours();
+        d_colours.alloc(sizeof col);
+        ck(cudaMemcpy(d_colours.p, &col, sizeof col, cudaMemcpyHostToDevice), "h2d");
+        for (cudaEvent_t* e : {&e0, &e1, &e2}) ck(cudaEventCreate(e), "event");
+    }
+    ~Viewer() {
+        for (cudaEvent_t e : {e0, e1, e2})
+            if (e) cudaEventDestroy(e);
+    }
+
+    ViewWorld world() const {
+        return ViewWorld{vox.as<uint8_t>(), cells.as<uint32_t>(), d_slot.as<int2>(), d_born.as<int32_t>(), W, WB, WC, tbm::kAir, tbm::kWater, tbm::kLava,
+                         tbm::kBedrock >= 0 ? tbm::kBedrock : tbm::kDefaultBlock};
+    }
+    int slot_of(int cx, int cz) const { return ((cz % W + W) % W) * W + ((cx % W + W) % W); }
+
+    // The chunks within radius of chunk (ccx, ccz) that the window does not hold, nearest
+    // first, at most cap (and max_batch) of them, generated on the device straight into the
+    // window (the generator's batch, narrowed to u8 voxels at their slots, then the cells).
+    int update(int ccx, int ccz, int radius, int cap, int frame, float* ms) {
+        if (radius < 0 || 2 * radius + 2 > W) throw Error(TG_ERR_INVALID_ARGUMENT, "radius must be in 0 .. window_chunks / 2 - 1");
+        if (g->current_slot < 0) throw Error(TG_ERR_NO_SEED, "tg_set_seed has not been called");
+        std::vector<std::pair<int, tg_chunk_xz>> need;
+        for (int dz = -radius; dz <= radius; ++dz)
+            for (int dx = -radius; dx <= radius; ++dx) {
+                if (dx * dx + dz * dz > radius * radius) continue;
+                const int cx = ccx + dx, cz = ccz + dz;
+                const int2 s = slot[slot_of(cx, cz)];
+                if (s.x != cx || s.y != cz) need.push_back({dx * dx + dz * dz, tg_chunk_xz{cx, cz}});
+            }
+        std::stable_sort(need.begin(), need.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        const int n = std::min<int>({static_cast<int>(need.size()), cap > 0 ? cap : g->max_batch, g->max_batch});
+        if (ms) *ms = 0.0f;
+        if (n == 0) return 0;
+        std::vector<tg_chunk_xz> list(static_cast<size_t>(n));
+        for (int i = 0; i < n; ++i) list[i] = need[i].second;
+        g->check_chunks(list.data(), n);
+        g->finish();
+        cudaStream_t s = g->stream;
+        Work& Wk = g->work[0];
+        OutSlot& o = g->out[0];
+        ck(cudaEventRecord(e0, s), "event");
+        ck(cudaMemcpyAsync(d_chunks.p, list.data(), sizeof(tg_chunk_xz) * n, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(d_coords.p, list.data(), sizeof(tg_chunk_xz) * n, cudaMemcpyHostToDevice, s), "h2d");
+        launch(k_split_chunks, s, n, d_chunks.as<tg_chunk_xz>(), n, static_cast<int32_t>(g->current_slot), Wk.d_cx.as<int32_t>(), Wk.d_cz.as<int32_t>(),
+               Wk.d_cs.as<int32_t>(), Wk.d_n.as<int32_t>());
+        g->enqueue_batch(Wk, g->batch_view(Wk, &o), s, g->max_batch, nullptr, false);
+        const ViewWorld w = world();
+        launch(k_view_scatter, s, static_cast<long>(n) * tbm::kHeight * 32, w, o.blocks.as<const uint4>(), d_coords.as<const int2>(), n);
+        launch(k_view_cells_clear, s, static_cast<long>(n) * 16, w, d_coords.as<const int2>(), n);
+        launch(k_view_cells, s, static_cast<long>(n) * 256, w, d_coords.as<const int2>(), n);
+        for (int i = 0; i < n; ++i) {
+            const int k = slot_of(list[i].x, list[i].z);
+            slot[k] = make_int2(list[i].x, list[i].z);
+            born[k] = frame;
+        }
+        ck(cudaMemcpyAsync(d_slot.p, slot.data(), d_slot.bytes, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaMemcpyAsync(d_born.p, born.data(), d_born.bytes, cudaMemcpyHostToDevice, s), "h2d");
+        ck(cudaEventRecord(e1, s), "event");
+        ck(cudaGetLastError(), "kernel launch");
+        ck(cudaStreamSynchronize(s), "sync");
+        g->check_device_errors();
+        if (ms) ck(cudaEventElapsedTime(ms, e0, e1), "elapsed");
+        return n;
+    }
+
+    ViewCam camera(const tg_camera& c) const {
+        ViewCam cam{};
+        const double kPi = 3.14159265358979323846;
+        const double yaw = c.yaw_deg * kPi / 180.0, pitch = c.pitch_deg * kPi / 180.0;
+        cam.px = c.x;
+        cam.py = c.y;
+        cam.pz = c.z;
+        cam.fx = static_cast<float>(std::sin(yaw) * std::cos(pitch));
+        cam.fy = static_cast<float>(std::sin(pitch));
+        cam.fz = static_cast<float>(std::cos(yaw) * std::cos(pitch));
+        // right = forward x up, horizontal; up = right x forward
+        const float rn = std::sqrt(cam.fz * cam.fz + cam.fx * cam.fx);
+        cam.rx = -cam.fz / rn;
+        cam.ry = 0.0f;
+        cam.rz = cam.fx / rn;
+        cam.ux = cam.ry * cam.fz - cam.rz * cam.fy;
+        cam.uy = cam.rz * cam.fx - cam.rx * cam.fz;
+        cam.uz = cam.rx * cam.fy - cam.ry * cam.fx;
+        cam.tan_half = static_cast<float>(std::tan((c.fov_deg > 0.0f ? c.fov_deg : 70.0f) * kPi / 360.0));
+        cam.aspect = static_cast<float>(width) / static_cast<float>(height);
+        const float ln = std::sqrt(c.sun_x * c.sun_x + c.sun_y * c.sun_y + c.sun_z * c.sun_z);
+        if (!(ln > 0.0f)) throw Error(TG_ERR_INVALID_ARGUMENT, "sun direction is zero");
+        cam.lx = c.sun_x / ln;
+        cam.ly = c.sun_y / ln;
+        cam.lz = c.sun_z / ln;
+        cam.fog = c.fog > 0.0f ? c.fog : static_cast<float>((W / 2 - 1) * 16);
+        return cam;
+    }
+
+    void render(const tg_camera& c, int frame, uint8_t* rgb, int32_t* hits, float* ms) {
+        const ViewCam cam = camera(c);
+        g->finish();
+        cudaStream_t s = g->stream;
+        const dim3 blk(16, 8), grd((width + 15) / 16, (height + 7) / 8);
+        ck(cudaEventRecord(e1, s), "event");
+        k_view_render<<<grd, blk, 0, s>>>(world(), cam, d_colours.as<ViewColours>(), width, height, frame, d_frame.as<uint8_t>(), hits ? d_hits.as<int4>() : nullptr);
+        ck(cudaEventRecord(e2, s), "event");
+        ck(cudaGetLastError(), "kernel launch");
+        if (rgb) ck(cudaMemcpyAsync(rgb, d_frame.p, static_cast<size_t>(width) * height * 3, cudaMemcpyDeviceToHost, s), "d2h");
+        if (hits) ck(cudaMemcpyAsync(hits, d_hits.p, sizeof(int4) * static_cast<size_t>(width) * height, cudaMemcpyDeviceToHost, s), "d2h");
+        ck(cudaStreamSynchronize(s), "sync");
+        if (ms) ck(cudaEventElapsedTime(ms, e1, e2), "elapsed");
+    }
+
+    // The window's state for checks: voxels [y][z][x], cells, slots (x, z pairs), born frames.
+    void state(uint8_t* v, uint32_t* cl, int32_t* sl, int32_t* bn) {
+        g->finish();
+        if (v) ck(cudaMemcpy(v, vox.p, vox.bytes, cudaMemcpyDeviceToHost), "d2h");
+        if (cl) ck(cudaMemcpy(cl, cells.p, cells.bytes, cudaMemcpyDeviceToHost), "d2h");
+        if (sl) std::memcpy(sl, slot.data(), sizeof(int2) * slot.size());
+        if (bn) std::memcpy(bn, born.data(), sizeof(int32_t) * born.size());
+    }
+};
+
 namespace {
 
 std::string read_file(const char* path) {
@@ -2324,6 +2546,11 @@ struct tg_generator {
 
 struct tg_server {
     std::unique_ptr<tb::Server> s;
+};
+
+struct tg_viewer {
+    std::unique_ptr<tb::Viewer> v;
+    tg_generator* gen;
 };
 
 namespace {
@@ -2479,6 +2706,65 @@ tg_status tg_biome_lookup_noalloc(tg_generator* gen, const int32_t* xyz, int32_t
         if (n < 0 || (n > 0 && (!xyz || !out))) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
         gen->g->biome_lookup_noalloc(xyz, n, out);
     });
+}
+
+tg_status tg_viewer_create(tg_generator* gen, const tg_viewer_config* config, tg_viewer** out) {
+    return tb::guarded([&] {
+        usable(gen);
+        if (!out) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "out is null");
+        *out = nullptr;
+        auto h = std::make_unique<tg_viewer>();
+        h->v = std::make_unique<tb::Viewer>(gen->g.get(), config);
+        h->gen = gen;
+        *out = h.release();
+    });
+}
+
+tg_status tg_viewer_update(tg_viewer* viewer, int32_t cx, int32_t cz, int32_t radius, int32_t cap, int32_t frame, int32_t* generated, float* ms) {
+    return tb::guarded([&] {
+        if (!viewer) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "viewer is null");
+        usable(viewer->gen);
+        const int n = viewer->v->update(cx, cz, radius, cap, frame, ms);
+        if (generated) *generated = n;
+    });
+}
+
+tg_status tg_viewer_render(tg_viewer* viewer, const tg_camera* camera, int32_t frame, uint8_t* rgb_out, int32_t* hits_out, float* ms) {
+    return tb::guarded([&] {
+        if (!viewer || !camera) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        usable(viewer->gen);
+        viewer->v->render(*camera, frame, rgb_out, hits_out, ms);
+    });
+}
+
+tg_status tg_viewer_state(tg_viewer* viewer, uint8_t* voxels, uint32_t* cells, int32_t* slots, int32_t* born) {
+    return tb::guarded([&] {
+        if (!viewer) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "viewer is null");
+        usable(viewer->gen);
+        viewer->v->state(voxels, cells, slots, born);
+    });
+}
+
+tg_status tg_viewer_params(tg_viewer* viewer, const tg_camera* camera, float* cam_out, float* top, float* side, int32_t* caps, int32_t* ids) {
+    return tb::guarded([&] {
+        if (!viewer || !camera) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad argument");
+        const tb::ViewCam c = viewer->v->camera(*camera);
+        static_assert(sizeof(tb::ViewCam) == 18 * sizeof(float), "camera record of 18 floats");
+        if (cam_out) std::memcpy(cam_out, &c, sizeof c);
+        const tb::ViewColours col = tb::palette_colours();
+        if (top) std::memcpy(top, col.top, sizeof col.top);
+        if (side) std::memcpy(side, col.side, sizeof col.side);
+        if (caps) std::memcpy(caps, col.cap, sizeof col.cap);
+        if (ids) {
+            const tb::ViewWorld w = viewer->v->world();
+            const int32_t v[7] = {w.W, w.air, w.water, w.lava, w.bedrock, tbm::kMinY, tbm::kHeight};
+            std::memcpy(ids, v, sizeof v);
+        }
+    });
+}
+
+tg_status tg_viewer_destroy(tg_viewer* viewer) {
+    return tb::guarded([&] { delete viewer; });
 }
 
 tg_status tg_set_launch_table(tg_generator* gen, const char* text) {

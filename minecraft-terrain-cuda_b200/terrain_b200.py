@@ -49,6 +49,14 @@ class TgRequestDevice(ctypes.Structure):
 TG_BATCH_HOST_LOOP = 1
 
 
+class TgViewerConfig(ctypes.Structure):
+    _fields_ = [('window_chunks', ctypes.c_int32), ('width', ctypes.c_int32), ('height', ctypes.c_int32), ('reserved', ctypes.c_int32)]
+
+
+class TgCamera(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_float) for k in ('x', 'y', 'z', 'yaw_deg', 'pitch_deg', 'fov_deg', 'sun_x', 'sun_y', 'sun_z', 'fog')]
+
+
 class TgServerConfig(ctypes.Structure):
     _fields_ = [('batch_chunks', ctypes.c_int32), ('hbm_budget_bytes', ctypes.c_int64), ('reserved', ctypes.c_int32)]
 
@@ -68,12 +76,13 @@ EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_genera
            'tg_biome_lookup_noalloc',
            'tg_server_create', 'tg_server_submit', 'tg_server_submit_u8', 'tg_server_wait', 'tg_server_cancel', 'tg_server_get_stats',
            'tg_server_latencies', 'tg_server_reset_stats', 'tg_server_destroy', 'tg_set_launch_table', 'tg_get_launch_table', 'tg_kernel_times',
+           'tg_viewer_create', 'tg_viewer_update', 'tg_viewer_render', 'tg_viewer_state', 'tg_viewer_params', 'tg_viewer_destroy',
            'tg_alloc_pinned', 'tg_free_pinned', 'tg_model_info', 'tg_last_error_string']
 
 # the tunable kernels of a batch, in pipeline order (tg_kernel_times order)
 KERNELS = ['nb_insert', 'nb_resolve', 'climate_col', 'climate_quart', 'chain', 'cc_insert', 'cc_resolve', 'corner_col', 'corner', 'zoom_table',
            'zoom_uniform', 'sg_insert', 'sg_resolve', 'surface_level', 'aquifer_cell', 'aquifer_query', 'aquifer_skip', 'init_heights', 'fill',
-           'surface1', 'block_biome', 'walk_rules', 'surface_frozen', 'gather']
+           'surface1', 'block_biome', 'walk_rules', 'surface_frozen', 'gather', 'axis_insert', 'axis_number', 'axis_fill']
 
 
 class TerrainError(RuntimeError):
@@ -118,6 +127,13 @@ def load(path=LIB_PATH):
     L.tg_set_launch_table.argtypes = [vp, ctypes.c_char_p]
     L.tg_get_launch_table.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
     L.tg_kernel_times.argtypes = [vp, ctypes.c_int32, vp, vp, ctypes.c_int32]
+    L.tg_viewer_create.argtypes = [vp, ctypes.POINTER(TgViewerConfig), ctypes.POINTER(vp)]
+    L.tg_viewer_update.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
+                                   ctypes.POINTER(ctypes.c_float)]
+    L.tg_viewer_render.argtypes = [vp, ctypes.POINTER(TgCamera), ctypes.c_int32, vp, vp, ctypes.POINTER(ctypes.c_float)]
+    L.tg_viewer_state.argtypes = [vp, vp, vp, vp, vp]
+    L.tg_viewer_params.argtypes = [vp, ctypes.POINTER(TgCamera), vp, vp, vp, vp, vp]
+    L.tg_viewer_destroy.argtypes = [vp]
     L.tg_alloc_pinned.argtypes = [ctypes.c_size_t]
     L.tg_alloc_pinned.restype = vp
     L.tg_free_pinned.argtypes = [vp]
@@ -127,7 +143,8 @@ def load(path=LIB_PATH):
               'tg_generate_density', 'tg_generate_batch', 'tg_generate_batch_device', 'tg_biome_lookup', 'tg_biome_lookup_noalloc',
               'tg_server_create', 'tg_server_submit', 'tg_server_submit_u8', 'tg_server_wait', 'tg_server_cancel', 'tg_server_get_stats',
               'tg_server_latencies', 'tg_server_reset_stats', 'tg_server_destroy',
-              'tg_set_launch_table', 'tg_get_launch_table', 'tg_kernel_times', 'tg_model_info'):
+              'tg_set_launch_table', 'tg_get_launch_table', 'tg_kernel_times', 'tg_model_info',
+              'tg_viewer_create', 'tg_viewer_update', 'tg_viewer_render', 'tg_viewer_state', 'tg_viewer_params', 'tg_viewer_destroy'):
         getattr(L, f).restype = ctypes.c_int
     _lib = L
     return L
@@ -364,6 +381,69 @@ class TerrainServer:
     def close(self):
         if self.h:
             self.L.tg_server_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def camera(x, y, z, yaw_deg=0.0, pitch_deg=-10.0, fov_deg=70.0, sun=(-0.45, 0.62, -0.64), fog=0.0):
+    return TgCamera(x, y, z, yaw_deg, pitch_deg, fov_deg, sun[0], sun[1], sun[2], fog)
+
+
+class TerrainViewer:
+    """Live flythrough renderer over a generator (tg_viewer_*).
+
+        v = TerrainViewer(gen, window_chunks=64, width=1280, height=720)
+        n, ms = v.update(cx, cz, radius=24)             # generate what the window lacks
+        rgb, hits, ms = v.render(camera(x, y, z, yaw, pitch), frame)
+    """
+
+    def __init__(self, gen, window_chunks=64, width=1280, height=720):
+        self.gen = gen
+        self.L = gen.L
+        self.h = ctypes.c_void_p()
+        self.W, self.width, self.height = window_chunks, width, height
+        cfg = TgViewerConfig(window_chunks, width, height, 0)
+        gen._check(self.L.tg_viewer_create(gen.h, ctypes.byref(cfg), ctypes.byref(self.h)))
+
+    def update(self, cx, cz, radius, cap=0, frame=0):
+        n, ms = ctypes.c_int32(), ctypes.c_float()
+        self.gen._check(self.L.tg_viewer_update(self.h, int(cx), int(cz), int(radius), int(cap), int(frame), ctypes.byref(n), ctypes.byref(ms)))
+        return n.value, ms.value
+
+    def render(self, cam, frame=0, hits=False, rgb=True):
+        out = np.empty((self.height, self.width, 3), np.uint8) if rgb else None
+        hit = np.empty((self.height, self.width, 4), np.int32) if hits else None
+        ms = ctypes.c_float()
+        self.gen._check(self.L.tg_viewer_render(self.h, ctypes.byref(cam), int(frame), _ptr(out), _ptr(hit), ctypes.byref(ms)))
+        return out, hit, ms.value
+
+    def state(self):
+        wb = self.W * 16
+        info = model_info()
+        vox = np.empty((info['height'], wb, wb), np.uint8)
+        cells = np.empty((self.W * 4, self.W * 4), np.uint32)
+        slots = np.empty((self.W * self.W, 2), np.int32)
+        born = np.empty(self.W * self.W, np.int32)
+        self.gen._check(self.L.tg_viewer_state(self.h, _ptr(vox), _ptr(cells), _ptr(slots), _ptr(born)))
+        return vox, cells, slots, born
+
+    def params(self, cam):
+        c = np.empty(18, np.float32)
+        top = np.empty((64, 3), np.float32)
+        side = np.empty((64, 3), np.float32)
+        caps = np.empty(64, np.int32)
+        ids = np.empty(7, np.int32)
+        self.gen._check(self.L.tg_viewer_params(self.h, ctypes.byref(cam), _ptr(c), _ptr(top), _ptr(side), _ptr(caps), _ptr(ids)))
+        return c, top, side, caps, ids
+
+    def close(self):
+        if self.h:
+            self.L.tg_viewer_destroy(self.h)
             self.h = ctypes.c_void_p()
 
     def __enter__(self):

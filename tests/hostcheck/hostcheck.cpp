@@ -96,7 +96,7 @@ extern "C" {
 // Stages of the pipeline in the order (and with the names) of the library's tunable kernels.
 enum Stage { S_NB_INSERT, S_NB_RESOLVE, S_CLIMATE_COL, S_CLIMATE_QUART, S_CHAIN, S_CC_INSERT, S_CC_RESOLVE, S_CORNER_COL, S_CORNER, S_ZOOM_TABLE,
              S_ZOOM_UNIFORM, S_SG_INSERT, S_SG_RESOLVE, S_SURFACE_LEVEL, S_AQ_CELL, S_AQ_QUERY, S_AQ_SKIP, S_INIT_HEIGHTS, S_FILL, S_SURFACE1,
-             S_BLOCK_BIOME, S_WALK, S_FROZEN, S_GATHER, S_COUNT };
+             S_BLOCK_BIOME, S_WALK, S_FROZEN, S_GATHER, S_AXIS_INSERT, S_AXIS_NUMBER, S_AXIS_FILL, S_COUNT };
 
 // The pipeline for n chunks of one seed, stage by stage; with counts (S_COUNT x kOpKinds),
 // each stage's octave and simplex samples are counted into its row.
@@ -106,10 +106,11 @@ int run_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, 
     tb_op_counts = g_discard;
     HostRun R(seed);
     std::vector<int32_t> vcx(cx, cx + n), vcz(cz, cz + n), vcs(n, 0);
-    Table hb, hc, hs;
+    Table hb, hc, hs, ha;
     hb.init(9 * static_cast<size_t>(n));
     hc.init(25 * static_cast<size_t>(n));
     hs.init(static_cast<size_t>(kGrid) * n);
+    ha.init(10 * static_cast<size_t>(n));
     const size_t N = n, nb = 9 * N, cc = 25 * N, sg = kGrid * N;
     std::vector<int32_t> nb9(9 * N), c25(25 * N), g513(sg), aq_skip(N);
     std::vector<AqCell> aq_cell(N * kAqCells);
@@ -124,6 +125,8 @@ int run_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, 
     std::vector<uint32_t> colmask(N * 2 * kMaskWords * 256);
     std::vector<uint8_t> zuni(N * kZoomCells);
     std::vector<ColumnRec> colrec(N * 256);
+    std::vector<AxisRec> axtab(10 * N * std::max(1, tbm::kAxisLayers));
+    std::vector<int32_t> colax(2 * 25 * N);
     Batch B{};
     B.M = R.M;
     B.seeds = &R.D;
@@ -143,6 +146,9 @@ int run_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, 
     B.cc_cap = static_cast<int32_t>(cc);
     B.c25 = c25.data();
     B.ccol = ccol.data();
+    B.ha = ha.view();
+    B.axtab = axtab.data();
+    B.colax = colax.data();
     B.corners = corners.data();
     B.hs = hs.view();
     B.sg_cap = static_cast<int32_t>(sg);
@@ -178,6 +184,14 @@ int run_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, 
     each(25 * n, [&](int i) { ht_number(B.hc, cc_key(B, i), i); });
     stage(S_CC_RESOLVE);
     each(25 * n, [&](int i) { body_cc_resolve(B, i); });
+    if (TB_AXIS_TABLE && tbm::kAxisLayers > 0) {
+        stage(S_AXIS_INSERT);
+        each(hc.count * 2, [&](int i) { body_axis_insert(B, i); });
+        stage(S_AXIS_NUMBER);
+        each(hc.count * 2, [&](int i) { body_axis_number(B, i); });
+        stage(S_AXIS_FILL);
+        each(ha.count * tbm::kAxisLayers, [&](int i) { body_axis_fill(B, i); });
+    }
     stage(S_CORNER_COL);
     each(hc.count, [&](int i) { body_corner_col(B, i); });
     stage(S_CORNER);
@@ -274,12 +288,26 @@ int hc_climate(int64_t seed, const int32_t* xyz, int32_t n, float* out) {
 }
 
 // Interpolation-channel inputs (volume path) at cell-corner positions: kNumChannels floats each.
+// The axis-table records of every table layer at one x (or z) block coordinate, as the
+// batch's axis_fill stage writes them.
+void axis_row(const NoiseTables& T, int32_t b, bool z, AxisRec* row) {
+    for (int e = 0; e < tbm::kAxisLayers; ++e) {
+        const Layer L = T.layer[tbm::kAxisLayer[e]];
+        const OctaveOff o = T.off[L.oct];
+        const AxisSetup a = axis_setup(b, tbm::kAxisScale[e] * L.freq, z ? o.oz : o.ox);
+        row[e] = AxisRec{a.f, a.r, a.a, 0};
+    }
+}
+
 int hc_corners(int64_t seed, const int32_t* xyz, int32_t n, float* out) {
     HostRun R(seed);
     float col[tbm::kCornerCols];
+    std::vector<AxisRec> ax(std::max(1, tbm::kAxisLayers)), az(std::max(1, tbm::kAxisLayers));
     for (int i = 0; i < n; ++i) {
         tbgen::gen_corner_col(R.D.nt, xyz[3 * i], xyz[3 * i + 2], col);
-        tbgen::gen_corner(R.D.nt, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], col, out + tbm::kNumChannels * i);
+        axis_row(R.D.nt, xyz[3 * i], false, ax.data());
+        axis_row(R.D.nt, xyz[3 * i + 2], true, az.data());
+        tbgen::gen_corner(R.D.nt, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], col, ax.data(), az.data(), out + tbm::kNumChannels * i);
     }
     return 0;
 }

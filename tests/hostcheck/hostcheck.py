@@ -107,7 +107,7 @@ def table_errors(n, cap):
 
 STAGES = ['nb_insert', 'nb_resolve', 'climate_col', 'climate_quart', 'chain', 'cc_insert', 'cc_resolve', 'corner_col', 'corner', 'zoom_table',
           'zoom_uniform', 'sg_insert', 'sg_resolve', 'surface_level', 'aquifer_cell', 'aquifer_query', 'aquifer_skip', 'init_heights', 'fill',
-          'surface1', 'block_biome', 'walk_rules', 'surface_frozen', 'gather']
+          'surface1', 'block_biome', 'walk_rules', 'surface_frozen', 'gather', 'axis_insert', 'axis_number', 'axis_fill']
 OP_KINDS = ['vol_octave', 'vol_octave_smeared', 'point_octave', 'point_octave_smeared', 'simplex']
 
 
