@@ -2028,6 +2028,7 @@ struct Server {
     double t_first = -1, t_last = 0;
     int batches = 0;
     int64_t cancelled = 0;
+    bool unchecked = false;   // batches completed since the device error word was last read
 
     Server(Generator* gen, const tg_server_config* cfg) : g(gen) {
         batch_chunks = cfg && cfg->batch_chunks > 0 ? std::min(cfg->batch_chunks, g->max_batch) : g->max_batch;
@@ -2167,7 +2168,7 @@ struct Server {
     void complete_batch(InFlight& f) {
         ck(cudaEventSynchronize(g->out[f.out].drained), "sync");
         g->out[f.out].busy = false;
-        g->check_device_errors();
+        unchecked = true;
         const double t = now_ms();
         std::lock_guard<std::mutex> l(mu);
         for (auto& part : f.parts) {
@@ -2206,6 +2207,12 @@ struct Server {
                     ck(q, "event query");
                     complete_batch(flight.front());
                     flight.pop_front();
+                }
+                // The device error word is read once the work in flight is done (a copy
+                // beside the output copies would stall the worker behind them).
+                if (flight.empty() && unchecked) {
+                    g->check_device_errors();
+                    unchecked = false;
                 }
                 std::vector<Req*> admitted;
                 {
