@@ -82,8 +82,8 @@ tg_status tg_set_seed(struct tg_generator* gen, int64_t seed);
  * biomes_out: count * 16 * height / 4 u8 (may be NULL); aquifer_out: the blocks after the
  * aquifer fill and before the material rules (may be NULL); timing may be NULL.
  * Host buffers; pinned ones (tg_alloc_pinned) copy fastest. The chunks go in device
- * batches of at most min(max_batch_chunks, 2048), each batch's copy to the host running
- * while the next one computes.
+ * batches, each batch's copy to the host running while the next one computes; the batch
+ * sizes follow the launch table's host_u16 line (tg_set_launch_table).
  * reference: FullTerrainGenerator::generate (cuda/src/terrain.cu:1392-1417) */
 tg_status tg_generate(struct tg_generator* gen, const tg_chunk_xz* chunks, int32_t count, uint16_t* blocks_out, uint8_t* biomes_out,
                       uint16_t* aquifer_out, tg_timing* timing);
@@ -92,8 +92,8 @@ tg_status tg_generate(struct tg_generator* gen, const tg_chunk_xz* chunks, int32
  * (may be NULL) hold one u8 palette index per block, biomes_out u8 per quart (may be NULL),
  * in the same layouts as tg_generate. Each value is the u16 state of tg_generate narrowed
  * (every state id is below the palette size); half the bytes cross the host link. The
- * narrowing runs on the GPU after each batch; batches hold at most min(max_batch, 4096)
- * chunks, then halving tail batches down to 512.
+ * narrowing runs on the GPU after each batch; the batch sizes follow the launch table's
+ * host_u8 line.
  * reference: FullTerrainGenerator::generate (cuda/include/mccuda_cuda/terrain_gpu.h:41-43,
  * cuda/src/terrain.cu:1392-1417), same argument types and order */
 tg_status tg_generate_u8(struct tg_generator* gen, const tg_chunk_xz* chunks, int32_t count, uint8_t* terrain_out, uint8_t* biomes_out,
@@ -292,6 +292,12 @@ tg_status tg_viewer_destroy(struct tg_viewer* viewer);
  * is set here. Text format, one line per kernel, '#' starts a comment:
  *   <kernel> <threads 32..256, multiple of 32> <blocks_per_sm 1..32> <grab 0..64>
  *   table_load <2..8>
+ *   host_u8 <batch> <tail_min> <tail_pct 0..99> <head_min> <head_pct 0|101..1000>
+ *   host_u16 (the same)
+ * host_u8 / host_u16: the batches of calls with host outputs in that form hold at most
+ * batch chunks (0: max_batch_chunks); at the end of a call they shrink, each tail_pct % of
+ * the one before, down to tail_min chunks; at the start they grow from head_min chunks by
+ * head_pct % each (pct 0: no tail / no head).
  * grab 0 runs the kernel as a grid-stride loop; grab g > 0 as a persistent work queue whose
  * blocks take runs of g * threads items from a device counter. table_load sizes the dedupe
  * hash tables (capacity >= table_load x the keys a batch can insert). Kernel names, in
@@ -303,6 +309,10 @@ tg_status tg_viewer_destroy(struct tg_viewer* viewer);
 tg_status tg_set_launch_table(struct tg_generator* gen, const char* text);   /* NULL: the compiled-in table */
 /* The table in use, as text (needed: its size with the terminating zero). */
 tg_status tg_get_launch_table(struct tg_generator* gen, char* buf, size_t cap, size_t* needed);
+/* The batch sizes a call with host outputs makes under a launch table (NULL: the compiled-in
+ * one): count chunks in the u8 (u8 = 1) or u16 form on a generator of max_batch_chunks.
+ * Writes at most cap sizes, in call order, and their number to n. Host only: needs no GPU. */
+tg_status tg_host_schedule(const char* text, int32_t u8, int32_t count, int32_t max_batch_chunks, int32_t* sizes, int32_t cap, int32_t* n);
 /* Per-kernel device times of timed batches (those of calls given a tg_timing): writes the
  * milliseconds and launch counts gathered since the previous call (cap entries, pipeline
  * order), clears them, and enables (enable = 1) or disables the per-kernel events. */

@@ -370,6 +370,22 @@ TB_HD TB_FI float stack_volume_ax(const NoiseTables& T, const AxisRec* ax, const
     return SMEARED ? stack_volume_smeared_ax_rt(T, FIRST, COUNT, ax, az, by, yss, amplitude) : stack_volume_ax_rt(T, FIRST, COUNT, ax, az, by, yss, amplitude);
 }
 
+// The same stacks with the layer run chosen per thread: threads of a warp that evaluate
+// different stacks of one noise (a blended noise's lower or upper limit) share one call.
+template <bool SMEARED>
+TB_HD TB_FI float stack_volume_ax_dyn(const NoiseTables& T, int first, int count, const AxisRec* ax, const AxisRec* az, int32_t by, double yss,
+                                      float amplitude) {
+    return SMEARED ? stack_volume_smeared_ax_rt(T, first, count, ax, az, by, yss, amplitude) : stack_volume_ax_rt(T, first, count, ax, az, by, yss, amplitude);
+}
+template <bool SMEARED>
+TB_HD TB_FI float stack_volume_dyn(const NoiseTables& T, int first, int count, int32_t bx, int32_t by, int32_t bz, double xzs, double yss, float amplitude) {
+    return SMEARED ? stack_volume_smeared_rt(T, first, count, bx, by, bz, xzs, yss, amplitude) : stack_volume_rt(T, first, count, bx, by, bz, xzs, yss, amplitude);
+}
+template <bool SMEARED>
+TB_HD TB_FI float stack_point_dyn(const NoiseTables& T, int first, int count, double x, double y, double z) {
+    return SMEARED ? stack_point_smeared_rt(T, first, count, x, y, z) : stack_point_rt(T, first, count, x, y, z);
+}
+
 template <int FIRST, int COUNT, bool SMEARED>
 TB_HD TB_FI float stack_volume(const NoiseTables& T, int32_t bx, int32_t by, int32_t bz, double xzs, double yss, float amplitude) {
     return SMEARED ? stack_volume_smeared_rt(T, FIRST, COUNT, bx, by, bz, xzs, yss, amplitude) : stack_volume_rt(T, FIRST, COUNT, bx, by, bz, xzs, yss, amplitude);

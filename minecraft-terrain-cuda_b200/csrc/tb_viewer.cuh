@@ -72,7 +72,7 @@ __device__ __forceinline__ int v_voxel(const ViewWorld& w, int x, int y, int z) 
 // lowest absolute y at or above which the column cell of (x, z) holds only air
 __device__ __forceinline__ int v_cell_top(const ViewWorld& w, int x, int z) {
     if (!v_holds(w, x, z)) return tbm::kMinY;
-    return tbm::kMinY + w.cell_top[vwrap(vfloor_div(z, kViewCell), w.WC) * w.WC + vwrap(vfloor_div(x, kViewCell), w.WC)];
+    return tbm::kMinY + static_cast<int>(w.cell_top[vwrap(vfloor_div(z, kViewCell), w.WC) * w.WC + vwrap(vfloor_div(x, kViewCell), w.WC)]);
 }
 
 struct ViewHit {

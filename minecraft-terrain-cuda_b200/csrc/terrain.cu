@@ -171,6 +171,32 @@ __global__ void k_split_chunks(const tg_chunk_xz* ch, int n, int32_t slot, int32
     if (blockIdx.x == 0 && threadIdx.x == 0) *n_dev = n;
 }
 
+// Fills of a lane's dedupe tables and work-queue counters before a batch, as one launch:
+// each segment is words 32-bit words at p set to value (16-byte stores for the bulk; every
+// segment starts at an allocation's base, so p is 16-byte aligned).
+struct ResetSeg {
+    uint32_t* p;
+    uint32_t words, value;
+};
+struct ResetList {
+    ResetSeg seg[16];
+    int n = 0;
+    void add(void* p, size_t bytes, uint32_t value) {
+        if (n == 16) throw Error(TG_ERR_INTERNAL, "reset list full");
+        seg[n++] = ResetSeg{static_cast<uint32_t*>(p), static_cast<uint32_t>(bytes / 4), value};
+    }
+};
+__global__ void k_reset(const ResetList L) {
+    const uint32_t stride = gridDim.x * blockDim.x, t = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int j = 0; j < L.n; ++j) {
+        const ResetSeg S = L.seg[j];
+        const uint4 v = make_uint4(S.value, S.value, S.value, S.value);
+        const uint32_t n4 = S.words >> 2;
+        for (uint32_t i = t; i < n4; i += stride) reinterpret_cast<uint4*>(S.p)[i] = v;
+        for (uint32_t i = 4 * n4 + t; i < S.words; i += stride) S.p[i] = S.value;
+    }
+}
+
 // The last-result chain of body_chain with one warp per biome chunk. Lane k of a block of
 // 32 quarts p first assumes the chain entered p holding L*(p - 1) (the previous quart's
 // first minimal leaf; for lane 0 the true previous result) and decides whether that leaf is
@@ -568,7 +594,12 @@ void launch(K kernel, cudaStream_t s, long items_hint, Args... args) {
 // time (tg_set_launch_table). A line "kernel threads blocks_per_sm grab" per kernel (grab 0:
 // grid-stride form; grab g > 0: work-queue form taking g * threads items per run), and
 // "table_load f": dedupe hash tables of at least f times the most keys a batch can insert
-// (rounded up to a power of two).
+// (rounded up to a power of two). "host_u8" and "host_u16" set how calls with host outputs
+// of that form cut their chunks into batches (host_schedule): "host_u8 batch tail_min
+// tail_pct head_min head_pct": batches of at most batch chunks (0: max_batch_chunks); the
+// batches at the end of a call shrink, each at most tail_pct % of the one before
+// it, down to tail_min chunks (tail_pct 0: no tail); the batches at the start grow from
+// head_min chunks by head_pct % each (head_pct 0: no head).
 enum KernelId {
     K_NB_INSERT, K_NB_RESOLVE, K_CLIMATE_COL, K_CLIMATE_QUART, K_CHAIN, K_CC_INSERT, K_CC_RESOLVE, K_CORNER_COL, K_CORNER, K_ZOOM_TABLE,
     K_ZOOM_UNIFORM, K_SG_INSERT, K_SG_RESOLVE, K_SURFACE_LEVEL, K_AQ_CELL, K_AQ_QUERY, K_AQ_SKIP, K_INIT_HEIGHTS, K_FILL, K_SURFACE1,
@@ -584,10 +615,53 @@ struct LaunchShape {
     int blocks_per_sm = 8;    // grid = min(blocks for the items, blocks_per_sm * SMs)
     int grab = 0;             // 0: grid-stride; > 0: work queue, grab * threads items per run
 };
+#ifndef TB_HOST_BATCH
+#define TB_HOST_BATCH 2048
+#endif
+#ifndef TB_HOST_BATCH_U8
+#define TB_HOST_BATCH_U8 4096
+#endif
+#ifndef TB_TAIL_MIN
+#define TB_TAIL_MIN 512
+#endif
+struct HostSchedule {
+    int batch, tail_min, tail_pct, head_min, head_pct;
+};
 struct LaunchTable {
     LaunchShape k[K_COUNT];
     int table_load = 2;
+    // host[0]: the u16 output form, host[1]: u8. The u16 form's copies are slower than its
+    // kernels, so smaller batches start them sooner; the u8 form's are faster, the kernels
+    // bound the step and larger batches win.
+    HostSchedule host[2] = {{TB_HOST_BATCH, TB_TAIL_MIN, 50, 0, 0}, {TB_HOST_BATCH_U8, TB_TAIL_MIN, 50, 0, 0}};
 };
+
+// The batch sizes of a call with host outputs: count chunks in batches of at most hb. The
+// copy of the last batch is the one no compute hides, so the batches at the end shrink
+// (tail); the first copy starts only when the first batch is done, so the batches at the
+// start may grow (head). Full batches in between; a part batch goes first (or after the head).
+std::vector<int> host_schedule(int count, int hb, const HostSchedule& t) {
+    std::vector<int> tail, head, mid;
+    long rem = count;
+    if (t.tail_pct > 0 && t.tail_min > 0)
+        for (long b = t.tail_min; rem > 0 && b < hb; b = std::max(b + 1, b * 100 / t.tail_pct)) {
+            const int take = static_cast<int>(std::min(b, rem));
+            tail.push_back(take);
+            rem -= take;
+        }
+    if (t.head_pct > 100 && t.head_min > 0)
+        for (long b = t.head_min; rem > 0 && b < hb; b = b * t.head_pct / 100) {
+            const int take = static_cast<int>(std::min(b, rem));
+            head.push_back(take);
+            rem -= take;
+        }
+    const long part = rem % hb;
+    if (part) mid.push_back(static_cast<int>(part));
+    for (long i = 0; i < rem / hb; ++i) mid.push_back(hb);
+    head.insert(head.end(), mid.begin(), mid.end());
+    head.insert(head.end(), tail.rbegin(), tail.rend());
+    return head;
+}
 
 // Parses a launch table; unknown kernels, bad values and malformed lines are errors.
 LaunchTable parse_launch_table(const std::string& text) {
@@ -607,6 +681,14 @@ LaunchTable parse_launch_table(const std::string& text) {
             if (!(ls >> t.table_load) || t.table_load < 2 || t.table_load > 8) bad("table_load must be 2..8");
             continue;
         }
+        if (name == "host_u8" || name == "host_u16") {
+            HostSchedule& h = t.host[name == "host_u8" ? 1 : 0];
+            if (!(ls >> h.batch >> h.tail_min >> h.tail_pct >> h.head_min >> h.head_pct)) bad("expected: host_u8|host_u16 batch tail_min tail_pct head_min head_pct");
+            if (h.batch < 0 || h.tail_min < 0 || h.head_min < 0) bad("host schedule sizes must be >= 0");
+            if (h.tail_pct < 0 || h.tail_pct >= 100) bad("tail_pct must be 0..99");
+            if (h.head_pct != 0 && (h.head_pct <= 100 || h.head_pct > 1000)) bad("head_pct must be 0 or 101..1000");
+            continue;
+        }
         int id = -1;
         for (int i = 0; i < K_COUNT; ++i)
             if (name == kKernelNames[i]) id = i;
@@ -624,6 +706,10 @@ LaunchTable parse_launch_table(const std::string& text) {
 std::string format_launch_table(const LaunchTable& t) {
     std::ostringstream o;
     o << "table_load " << t.table_load << "\n";
+    for (int f = 1; f >= 0; --f) {
+        const HostSchedule& h = t.host[f];
+        o << (f ? "host_u8 " : "host_u16 ") << h.batch << ' ' << h.tail_min << ' ' << h.tail_pct << ' ' << h.head_min << ' ' << h.head_pct << "\n";
+    }
     for (int i = 0; i < K_COUNT; ++i) o << kKernelNames[i] << ' ' << t.k[i].threads << ' ' << t.k[i].blocks_per_sm << ' ' << t.k[i].grab << "\n";
     return o.str();
 }
@@ -638,17 +724,25 @@ uint32_t pow2_at_least(uint64_t v) {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    bool owned = true;   // false: a view into another buffer
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() {
-        if (p) cudaFree(p);
+        if (p && owned) cudaFree(p);
     }
     void alloc(size_t b) {
-        if (p) cudaFree(p);
+        if (p && owned) cudaFree(p);
         p = nullptr;
+        owned = true;
         bytes = b;
         if (b) ck(cudaMalloc(&p, b), "cudaMalloc");
+    }
+    void view(void* base, size_t b) {
+        if (p && owned) cudaFree(p);
+        p = base;
+        bytes = b;
+        owned = false;
     }
     template <class T>
     T* as() const {
@@ -691,10 +785,10 @@ struct TableBufs {
         return HashTab{keys.as<unsigned long long>(), vals.as<int32_t>(), uniq.as<unsigned long long>(), count.as<int32_t>(), cap - 1, owner.as<int32_t>(), err};
     }
     // free slots; owners above every item index (0x7F7F7F7F)
-    void reset(cudaStream_t s) const {
-        ck(cudaMemsetAsync(keys.p, 0xFF, keys.bytes, s), "memset");
-        ck(cudaMemsetAsync(owner.p, 0x7F, owner.bytes, s), "memset");
-        ck(cudaMemsetAsync(count.p, 0, sizeof(int32_t), s), "memset");
+    void add_reset(ResetList& L) const {
+        L.add(keys.p, keys.bytes, 0xFFFFFFFFu);
+        L.add(owner.p, owner.bytes, 0x7F7F7F7Fu);
+        L.add(count.p, sizeof(int32_t), 0u);
     }
 };
 
@@ -724,12 +818,18 @@ struct OutSlot {
 // per-block biomes). A generator holds one set per lane; two lanes let the batches of the
 // two output slots run concurrently on two streams.
 struct Work {
-    DevBuf d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_cell,
+    DevBuf d_coords, d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_cell,
         d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_zoom_uni, d_bbiome, d_oremask, d_colmask, d_colrec, d_qnext, d_err, d_axtab, d_colax;
     TableBufs tb_b, tb_c, tb_s, tb_a;
     void alloc(int n, int load) {
         const size_t N = static_cast<size_t>(n);
-        d_n.alloc(sizeof(int32_t));
+        // chunk x | chunk z | seed slot | count, the layout of an output slot's staged
+        // coordinates, so that one copy uploads them
+        d_coords.alloc(4 * (3 * N + 1));
+        d_cx.view(d_coords.as<int32_t>(), 4 * N);
+        d_cz.view(d_coords.as<int32_t>() + N, 4 * N);
+        d_cs.view(d_coords.as<int32_t>() + 2 * N, 4 * N);
+        d_n.view(d_coords.as<int32_t>() + 3 * N, 4);
         d_err.alloc(sizeof(uint32_t));
         ck(cudaMemset(d_err.p, 0, sizeof(uint32_t)), "memset");
         tb_b.err = tb_c.err = tb_s.err = tb_a.err = d_err.as<uint32_t>();
@@ -740,9 +840,6 @@ struct Work {
             d_colax.alloc(sizeof(int32_t) * 2 * 25 * N);
         }
         d_qnext.alloc(sizeof(int32_t) * K_COUNT);   // work-queue counters, one per kernel
-        d_cx.alloc(4 * N);
-        d_cz.alloc(4 * N);
-        d_cs.alloc(4 * N);
         tb_b.alloc(9 * N, load);
         tb_c.alloc(25 * N, load);
         tb_s.alloc(static_cast<uint64_t>(kGrid) * N, load);
@@ -777,24 +874,6 @@ struct Work {
 
 // ---- the generator ----------------------------------------------------------------------------------
 struct Generator {
-#ifndef TB_TAIL_MIN
-#define TB_TAIL_MIN 512
-#endif
-    static constexpr int kTailMin = TB_TAIL_MIN;   // smallest batch the tail split of generate() makes (0: no split)
-#ifndef TB_HOST_BATCH
-#define TB_HOST_BATCH 2048
-#endif
-    // Batches of generate() (outputs to host memory) hold at most this many chunks: once the
-    // kernels outrun the device-to-host link, smaller batches start the copies sooner while
-    // still keeping the GPU busy.
-    static constexpr int kHostBatch = TB_HOST_BATCH;
-#ifndef TB_HOST_BATCH_U8
-#define TB_HOST_BATCH_U8 4096
-#endif
-    // The same for the u8 output form (0: max_batch). Its copies take half as long and the
-    // link no longer limits the step, so larger batches, on which the kernels run faster,
-    // win (4,096: 301k chunks/s end to end against 282k at 2,048, 12,288 chunks).
-    static constexpr int kHostBatchU8 = TB_HOST_BATCH_U8;
 #ifndef TB_ORDERED_BATCH
 #define TB_ORDERED_BATCH 2048
 #endif
@@ -1081,12 +1160,29 @@ struct Generator {
         }
     }
 
-    // biome stage (shared by the TERRAIN step and biome lookups); nmax sizes the grids
-    void enqueue_biomes(const Work& W, const Batch& B, cudaStream_t s, long nmax) {
+    // One launch that clears the lane's work-queue counters and dedupe tables for a batch:
+    // the biome stage's table, and with all those of the whole step. (Separate memsets, six
+    // to a batch, each waited behind the copies of the other output slot on the copy engines.)
+    void reset_lane(const Work& W, cudaStream_t s, bool all) {
+        ResetList L;
+        L.add(W.d_qnext.p, W.d_qnext.bytes, 0u);
+        W.tb_b.add_reset(L);
+        if (all) {
+            W.tb_c.add_reset(L);
+            W.tb_s.add_reset(L);
+            if (TB_AXIS_TABLE && tbm::kAxisLayers > 0) W.tb_a.add_reset(L);
+        }
+        size_t words = 0;
+        for (int i = 0; i < L.n; ++i) words += L.seg[i].words;
+        launch(k_reset, s, static_cast<long>(words / 4), L);
+    }
+
+    // biome stage (shared by the TERRAIN step and biome lookups); nmax sizes the grids;
+    // reset: clear the counters and the table first (else reset_lane ran before)
+    void enqueue_biomes(const Work& W, const Batch& B, cudaStream_t s, long nmax, bool reset = true) {
         const int32_t* n_dev = B.n_dev;
         const int32_t* cnt_b = W.tb_b.count.as<int32_t>();
-        ck(cudaMemsetAsync(W.d_qnext.p, 0, sizeof(int32_t) * K_COUNT, s), "memset");   // work-queue counters
-        W.tb_b.reset(s);
+        if (reset) reset_lane(W, s, false);
         run_body<body_nb_insert, 9>(K_NB_INSERT, W, s, 9 * nmax, B, n_dev);
         launch(k_number<0, nb_key, 9>, s, 9 * nmax, B);
         run_body<body_nb_resolve, 9>(K_NB_RESOLVE, W, s, 9 * nmax, B, n_dev);
@@ -1106,25 +1202,25 @@ struct Generator {
         }
     }
 
-    // every kernel of one batch; with timed set, events split the stages
-    void enqueue_batch(const Work& W, const Batch& B, cudaStream_t s, long nmax, uint16_t* aquifer_dev, bool timed) {
+    // every kernel of one batch; with timed set, events split the stages; reset: clear the
+    // lane's counters and tables first (else the caller ran reset_lane before)
+    void enqueue_batch(const Work& W, const Batch& B, cudaStream_t s, long nmax, uint16_t* aquifer_dev, bool timed, bool reset = true) {
         auto mark = [&](int i) {
             if (timed) ck(cudaEventRecord(ev[i], s), "event");
         };
         const int32_t* cnt_c = W.tb_c.count.as<int32_t>();
         const int32_t* cnt_s = W.tb_s.count.as<int32_t>();
         prof_now = timed && prof;
+        if (reset) reset_lane(W, s, true);
         mark(0);
-        enqueue_biomes(W, B, s, nmax);
+        enqueue_biomes(W, B, s, nmax, false);
         mark(1);
         const int32_t* n_dev = B.n_dev;
-        W.tb_c.reset(s);
         run_body<body_cc_insert, 25>(K_CC_INSERT, W, s, 25 * nmax, B, n_dev);
         launch(k_number<1, cc_key, 25>, s, 25 * nmax, B);
         run_body<body_cc_resolve, 25>(K_CC_RESOLVE, W, s, 25 * nmax, B, n_dev);
         if (TB_AXIS_TABLE && tbm::kAxisLayers > 0) {
             const int32_t* cnt_a = W.tb_a.count.as<int32_t>();
-            W.tb_a.reset(s);
             run_body<body_axis_insert, 2>(K_AXIS_INSERT, W, s, 2 * 16 * nmax, B, cnt_c);
             run_body<body_axis_number, 2>(K_AXIS_NUMBER, W, s, 2 * 16 * nmax, B, cnt_c);
             run_body<body_axis_fill, std::max(1, tbm::kAxisLayers)>(K_AXIS_FILL, W, s, 2L * nmax * std::max(1, tbm::kAxisLayers), B, cnt_a);
@@ -1136,7 +1232,6 @@ struct Generator {
         run_body<body_zoom_table, kZoomVerts>(K_ZOOM_TABLE, W, s, kZoomVerts * nmax, B, n_dev);
         run_body<body_zoom_uniform, kZoomCells>(K_ZOOM_UNIFORM, W, s, kZoomCells * nmax, B, n_dev);
         mark(2);
-        W.tb_s.reset(s);
         run_body<body_sg_insert, kGrid>(K_SG_INSERT, W, s, kGrid * nmax, B, n_dev);
         launch(k_number<2, sg_key_item, kGrid>, s, kGrid * nmax, B);
         run_body<body_sg_resolve, kGrid>(K_SG_RESOLVE, W, s, kGrid * nmax, B, n_dev);
@@ -1211,12 +1306,10 @@ struct Generator {
     }
 
     // the staged coordinates of o (cx | cz | seed slot | n) into lane W's batch buffers
+    // (one copy: the lane's coordinate buffer has the staging layout)
     void upload_coords(const Work& W, const OutSlot& o, int n, cudaStream_t s) {
-        const int32_t* h = o.coords.as<int32_t>();
-        ck(cudaMemcpyAsync(W.d_cx.p, h, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(W.d_cz.p, h + max_batch, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(W.d_cs.p, h + 2 * max_batch, 4 * static_cast<size_t>(n), cudaMemcpyHostToDevice, s), "h2d");
-        ck(cudaMemcpyAsync(W.d_n.p, h + 3 * max_batch, 4, cudaMemcpyHostToDevice, s), "h2d");
+        (void)n;
+        ck(cudaMemcpyAsync(W.d_coords.p, o.coords.p, 4 * (3 * static_cast<size_t>(max_batch) + 1), cudaMemcpyHostToDevice, s), "h2d");
     }
 
     // Runs one batch whose staged coordinates sit in o.coords into output slot o.
@@ -1225,16 +1318,18 @@ struct Generator {
         Work& W = work[o.lane];
         cudaStream_t s = o.lane ? lane_stream : stream;
         if (o.busy) ck(cudaStreamWaitEvent(s, o.drained, 0), "wait");   // the slot's previous outputs are copied out
+        // the lane's own buffers: ready while the other lane's batch still runs
+        upload_coords(W, o, n, s);
+        reset_lane(W, s, true);
         // A batch that fills the GPU alone runs after the previous one rather than beside it,
         // so each finishes (and its copy starts) as early as possible; smaller ones overlap.
         OutSlot& other = out[&o == &out[0] ? 1 : 0];
         if (lanes > 1 && n >= kOrderedBatch && other.lane != o.lane && other.busy) ck(cudaStreamWaitEvent(s, other.computed, 0), "wait");
-        upload_coords(W, o, n, s);
         if (want_aquifer && !o.aquifer.p) o.aquifer.alloc(sizeof(uint16_t) * static_cast<size_t>(max_batch) * kBlocksPerChunk);
         const Batch B = batch_view(W, &o);
         uint16_t* aq = want_aquifer ? o.aquifer.as<uint16_t>() : nullptr;
         if (t) {
-            enqueue_batch(W, B, s, max_batch, aq, true);
+            enqueue_batch(W, B, s, max_batch, aq, true, false);
             add_stage_times(t);
         } else if (use_graphs) {
             if (!o.graph || o.graph_aquifer != want_aquifer || o.graph_stream != s) {
@@ -1243,7 +1338,7 @@ struct Generator {
                 cudaGraph_t g;
                 ck(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "capture");
                 const int before = g_launches;
-                enqueue_batch(W, B, s, max_batch, aq, false);
+                enqueue_batch(W, B, s, max_batch, aq, false, false);
                 ck(cudaStreamEndCapture(s, &g), "capture");
                 ck(cudaGraphInstantiate(&o.graph, g, 0), "graph instantiate");
                 cudaGraphDestroy(g);
@@ -1255,7 +1350,7 @@ struct Generator {
             ck(cudaGraphLaunch(o.graph, s), "graph launch");
             g_launches += graph_launches;
         } else {
-            enqueue_batch(W, B, s, max_batch, aq, false);
+            enqueue_batch(W, B, s, max_batch, aq, false, false);
         }
         if (narrow) {
             const size_t cap = static_cast<size_t>(max_batch) * kBlocksPerChunk;
@@ -1364,13 +1459,10 @@ struct Generator {
         order_lanes();
         check_chunks(chunks, count);
         std::vector<int32_t> cx(max_batch), cz(max_batch), cs(max_batch, current_slot);
-        const int hcap = blocks8 ? kHostBatchU8 : kHostBatch;
-        const int hb = hcap > 0 ? std::min(max_batch, hcap) : max_batch;
-        for (int off = 0; off < count;) {
-            // The copy of the last batch is the one no compute hides: within the last two
-            // batches' worth, halve the batches (down to kTailMin chunks) so that it is short.
-            const int rem = count - off;
-            const int n = (kTailMin == 0 || rem > 2 * hb) ? std::min(hb, rem) : std::min(hb, std::max((rem + 1) / 2, std::min(rem, kTailMin)));
+        const HostSchedule& hs = lt.host[blocks8 ? 1 : 0];
+        const int hb = hs.batch > 0 ? std::min(max_batch, hs.batch) : max_batch;
+        int off = 0;
+        for (const int n : host_schedule(count, hb, hs)) {
             for (int i = 0; i < n; ++i) {
                 cx[i] = chunks[off + i].x;
                 cz[i] = chunks[off + i].z;
@@ -2791,6 +2883,18 @@ tg_status tg_get_launch_table(tg_generator* gen, char* buf, size_t cap, size_t* 
             std::memcpy(buf, t.data(), n);
             buf[n] = 0;
         }
+    });
+}
+
+tg_status tg_host_schedule(const char* text, int32_t u8, int32_t count, int32_t max_batch_chunks, int32_t* sizes, int32_t cap, int32_t* n) {
+    return tb::guarded([&] {
+        if (count < 0 || max_batch_chunks <= 0 || cap < 0 || (cap > 0 && !sizes)) throw tb::Error(TG_ERR_INVALID_ARGUMENT, "bad count, max_batch_chunks or buffer");
+        const tb::LaunchTable t = tb::parse_launch_table(text ? std::string(text) : std::string(tb::kLaunchTableText));
+        const tb::HostSchedule& hs = t.host[u8 ? 1 : 0];
+        const int hb = hs.batch > 0 ? std::min(max_batch_chunks, hs.batch) : max_batch_chunks;
+        const std::vector<int> v = tb::host_schedule(count, hb, hs);
+        if (n) *n = static_cast<int32_t>(v.size());
+        for (size_t i = 0; i < v.size() && static_cast<int32_t>(i) < cap; ++i) sizes[i] = v[i];
     });
 }
 

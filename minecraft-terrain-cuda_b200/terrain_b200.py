@@ -76,7 +76,7 @@ EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_genera
            'tg_biome_lookup_noalloc',
            'tg_server_create', 'tg_server_submit', 'tg_server_submit_u8', 'tg_server_wait', 'tg_server_cancel', 'tg_server_get_stats',
            'tg_server_latencies', 'tg_server_reset_stats', 'tg_server_destroy', 'tg_set_launch_table', 'tg_get_launch_table', 'tg_kernel_times',
-           'tg_viewer_create', 'tg_viewer_update', 'tg_viewer_render', 'tg_viewer_state', 'tg_viewer_params', 'tg_viewer_destroy',
+           'tg_host_schedule', 'tg_viewer_create', 'tg_viewer_update', 'tg_viewer_render', 'tg_viewer_state', 'tg_viewer_params', 'tg_viewer_destroy',
            'tg_alloc_pinned', 'tg_free_pinned', 'tg_model_info', 'tg_last_error_string']
 
 # the tunable kernels of a batch, in pipeline order (tg_kernel_times order)
@@ -127,6 +127,7 @@ def load(path=LIB_PATH):
     L.tg_set_launch_table.argtypes = [vp, ctypes.c_char_p]
     L.tg_get_launch_table.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]
     L.tg_kernel_times.argtypes = [vp, ctypes.c_int32, vp, vp, ctypes.c_int32]
+    L.tg_host_schedule.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]
     L.tg_viewer_create.argtypes = [vp, ctypes.POINTER(TgViewerConfig), ctypes.POINTER(vp)]
     L.tg_viewer_update.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32),
                                    ctypes.POINTER(ctypes.c_float)]
@@ -143,7 +144,7 @@ def load(path=LIB_PATH):
               'tg_generate_density', 'tg_generate_batch', 'tg_generate_batch_device', 'tg_biome_lookup', 'tg_biome_lookup_noalloc',
               'tg_server_create', 'tg_server_submit', 'tg_server_submit_u8', 'tg_server_wait', 'tg_server_cancel', 'tg_server_get_stats',
               'tg_server_latencies', 'tg_server_reset_stats', 'tg_server_destroy',
-              'tg_set_launch_table', 'tg_get_launch_table', 'tg_kernel_times', 'tg_model_info',
+              'tg_set_launch_table', 'tg_get_launch_table', 'tg_kernel_times', 'tg_host_schedule', 'tg_model_info',
               'tg_viewer_create', 'tg_viewer_update', 'tg_viewer_render', 'tg_viewer_state', 'tg_viewer_params', 'tg_viewer_destroy'):
         getattr(L, f).restype = ctypes.c_int
     _lib = L
@@ -155,6 +156,20 @@ def model_info():
     v = [ctypes.c_int32() for _ in range(5)]
     L.tg_model_info(*[ctypes.byref(x) for x in v])
     return dict(zip(('min_y', 'height', 'sea_level', 'palette_size', 'biome_count'), [x.value for x in v]))
+
+
+def host_schedule(count, max_batch_chunks, u8=True, table=None):
+    """The batch sizes of a call with host outputs (tg_generate_u8 when u8, else tg_generate)
+    over count chunks on a generator of max_batch_chunks, under a launch table (text; None:
+    the compiled-in one). Host only."""
+    L = load()
+    n = ctypes.c_int32()
+    st = L.tg_host_schedule(table.encode() if table is not None else None, 1 if u8 else 0, count, max_batch_chunks, None, 0, ctypes.byref(n))
+    if st != 0:
+        raise TerrainError(st, L.tg_last_error_string().decode())
+    out = np.zeros(n.value, np.int32)
+    L.tg_host_schedule(table.encode() if table is not None else None, 1 if u8 else 0, count, max_batch_chunks, _ptr(out), n.value, ctypes.byref(n))
+    return out.tolist()
 
 
 def _ptr(a):

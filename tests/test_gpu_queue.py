@@ -106,6 +106,15 @@ def test_launch_tables_change_no_output(ref_model):
             assert all(times[k][1] >= 1 for k in names) and times['corner'][0] > 0
             b, q = g.generate(chunks)                       # graphs of the new shapes
             assert (b == base[0]).all() and (q == base[1]).all()
+        # host-output batch schedules: tails, heads and small batches cut the same chunks
+        base8 = g.generate_u8(chunks)
+        for text in ['host_u8 16 4 50 4 200\nhost_u16 24 8 75 0 0\n', 'host_u8 0 0 0 0 0\nhost_u16 7 0 0 3 300\n']:
+            g.set_launch_table(text)
+            assert len(terrain_b200.host_schedule(len(chunks), 64, u8=False, table=text)) > 2
+            b, q = g.generate(chunks)
+            assert (b == base[0]).all() and (q == base[1]).all()
+            b8, q8 = g.generate_u8(chunks)
+            assert (b8 == base8[0]).all() and (q8 == base8[1]).all()
         g.set_launch_table(None)
         assert g.launch_table() == default
         with pytest.raises(terrain_b200.TerrainError):
