@@ -240,9 +240,10 @@ def main(argv):
               '# table_load: dedupe hash tables of at least table_load x the most keys of a batch;\n'
               '# host_u8 / host_u16: batch tail_min tail_pct head_min head_pct of calls with host outputs.\n'
               '# Two 64x64-chunk ladder regions, 4,096-chunk batches, graph-launched device step:\n'
-              '# the table in use before %.3f ms, tuned %.3f ms per two batches%s.\n'
+              '# %s.\n'
               '# Three ladder regions in one call to pinned host memory: u8 %.3f -> %.3f ms, u16 %.3f -> %.3f ms.'
-              % (step_default, step_tuned, '' if keep_tuned else ' (tuned slower: the previous shapes kept)',
+              % (('%.3f ms per two batches (kernel shapes not re-tuned in this run)' % step_default) if args.schedule_only else
+                 ('the table in use before %.3f ms, tuned %.3f ms per two batches%s' % (step_default, step_tuned, '' if keep_tuned else ' (tuned slower: the previous shapes kept)')),
                  hs['host_u8']['before_ms'], hs['host_u8']['chosen_ms'], hs['host_u16']['before_ms'], hs['host_u16']['chosen_ms']))
     text = fmt(table, load, sched, header)
     with open(args.out, 'w') as f:
