@@ -1683,6 +1683,7 @@ TB_HD TB_NOINLINE inline int ore_vein_hit(const Batch& B, int c, int lx, int lz,
 }
 
 // Block context handed to the generated rule tree (MaterialSystem's per-block state).
+static_assert(tbgen::kRuleNoise2d <= 32, "2-D threshold noise memo slots fit one 32-bit mask");
 struct RuleCtx {
     Column* col;
     const Batch* B;
@@ -1693,14 +1694,24 @@ struct RuleCtx {
     double secondary;
     int min_surf;
     float prelim;
+    // column values the rules read, each evaluated at its first use and kept for the
+    // column's other blocks: the 2-D threshold noises (by memo slot) and the clay-band offset
+    double n2d[tbgen::kRuleNoise2d > 0 ? tbgen::kRuleNoise2d : 1];
+    uint32_t n2d_set;
+    int band_off;
+    bool band_set;
     // block
     int y, stone_above, stone_below, water_height;
     int biome_v;        // zoomed biome of the block
     uint32_t ore_bits;  // its ore-vein density tests
 
     TB_HD TB_FI int biome() const { return biome_v; }
-    TB_HD TB_FI double noise2d(int k, int first, int count) const {
-        return static_cast<double>(stack_point_rt(col->S->nt, first, count, col->bx, 0.0, col->bz));
+    TB_HD TB_FI double noise2d(int slot, int first, int count) {
+        if (!((n2d_set >> slot) & 1u)) {
+            n2d[slot] = static_cast<double>(stack_point_rt(col->S->nt, first, count, col->bx, 0.0, col->bz));
+            n2d_set |= 1u << slot;
+        }
+        return n2d[slot];
     }
     TB_HD TB_FI double noise3d(int k, int first, int count) const {
         return static_cast<double>(stack_point_rt(col->S->nt, first, count, col->bx, y, col->bz));
@@ -1729,9 +1740,12 @@ struct RuleCtx {
         const double t = (secondary - -1.0) / (1.0 - -1.0);
         return d2i(0.0 + t * (static_cast<double>(range) - 0.0));
     }
-    TB_HD TB_FI int band() const {
-        const int off = jround(static_cast<float>(col->noise<tbm::kNoise_clay_bands_offset>(col->bx, 0.0, col->bz)) * 4.0f);
-        return col->S->clay[(y + off + 192) % 192];
+    TB_HD TB_FI int band() {
+        if (!band_set) {
+            band_off = jround(static_cast<float>(col->noise<tbm::kNoise_clay_bands_offset>(col->bx, 0.0, col->bz)) * 4.0f);
+            band_set = true;
+        }
+        return col->S->clay[(y + band_off + 192) % 192];
     }
     // OreVeinRule: the density inline (its guards usually end it after a y test), the rest
     // out of line

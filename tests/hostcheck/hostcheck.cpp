@@ -12,7 +12,8 @@
 #include "tb_pipeline.cuh"
 
 namespace tb {
-thread_local long long* tb_op_counts = nullptr;
+long long tb_count_sink[kOpKinds];   // counts of calls made outside a counted stage
+thread_local long long* tb_op_counts = tb_count_sink;
 }
 using namespace tb;
 
