@@ -38,10 +38,12 @@ GRABS = (0, 1, 2, 4)
 
 
 SCHED_KEYS = ('host_u8', 'host_u16')
+OTHER_KEYS = ('walk_defer',)   # carried through unchanged
 
 
 def parse(text):
-    """(kernel shapes, table load, schedule lines {host_u8 / host_u16: (batch, tail_min, tail_pct, head_min, head_pct)})"""
+    """(kernel shapes, table load, other lines {host_u8 / host_u16: (batch, tail_min, tail_pct, head_min, head_pct),
+    walk_defer: (blocks per chunk,)})"""
     table, load, sched = {}, 2, {}
     for line in text.splitlines():
         line = line.split('#')[0].split()
@@ -49,7 +51,7 @@ def parse(text):
             continue
         if line[0] == 'table_load':
             load = int(line[1])
-        elif line[0] in SCHED_KEYS:
+        elif line[0] in SCHED_KEYS or line[0] in OTHER_KEYS:
             sched[line[0]] = tuple(int(v) for v in line[1:6])
         else:
             table[line[0]] = tuple(int(v) for v in line[1:4])
@@ -59,7 +61,7 @@ def parse(text):
 def fmt(table, load, sched=None, header=''):
     lines = [header] if header else []
     lines.append('table_load %d' % load)
-    lines += ['%s %d %d %d %d %d' % ((k,) + tuple(sched[k])) for k in SCHED_KEYS if sched and k in sched]
+    lines += ['%s %s' % (k, ' '.join('%d' % v for v in sched[k])) for k in SCHED_KEYS + OTHER_KEYS if sched and k in sched]
     lines += ['%s %d %d %d' % ((k,) + table[k]) for k in terrain_b200.KERNELS]
     return '\n'.join(lines) + '\n'
 

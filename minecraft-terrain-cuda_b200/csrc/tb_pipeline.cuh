@@ -169,6 +169,9 @@ struct Batch {
                                       // (c * 2 * kMaskWords + w) * 256 + column; words below
                                       // kMaskWords hold air, the rest fluid; bit k = y kMinY + 32 w + k
     struct ColumnRec* colrec;         // n * 256 per-column surface context
+    struct DeferRec* defer;           // blocks the walk leaves to the deferred pass (nullptr: none)
+    int32_t* defer_count;             // blocks appended (may pass defer_cap; the rest stay in the walk)
+    int32_t defer_cap;
 };
 
 // Per-column context of the material rules (MaterialSystem column state).
@@ -177,6 +180,19 @@ struct ColumnRec {
     int32_t surface_depth, min_surface, grad_x, grad_z;
     int32_t surface_biome, start_h;
 };
+// A block whose rule evaluation reaches a per-block noise or an ore vein past its density
+// bit: the walk's inputs to the rules, for the deferred pass (body_walk_deferred).
+struct DeferRec {
+    int32_t column;                   // chunk * 256 + x * 16 + z
+    int16_t y, stone_above, stone_below, water_height;   // water_height kNoWater for none
+    uint8_t biome, ore_bits;
+    uint16_t pad;
+};
+constexpr int16_t kNoWater = INT16_MIN;
+#ifndef TB_DEFER_ORE
+#define TB_DEFER_ORE 0   // also defer blocks that reach an ore vein past its density bit
+#endif
+
 // Per block, bit k: whether ore vein k's density test passes (its density is not <= 0),
 // decided by the fill from the channel values it already holds, so that the rule tree
 // interpolates channels only inside veins.
@@ -1713,7 +1729,16 @@ struct RuleCtx {
         }
         return n2d[slot];
     }
-    TB_HD TB_FI double noise3d(int k, int first, int count) const {
+    // The walk leaves a block whose rules need a per-block noise or an ore vein past its
+    // density bit (rare, costly, and in different iterations of each thread's walk) to the
+    // deferred pass, where the threads of a warp evaluate such blocks side by side: with
+    // defer set these set deferred and give NaN / nothing, and the walk discards the state.
+    bool defer, deferred;
+    TB_HD TB_FI double noise3d(int k, int first, int count) {
+        if (defer) {
+            deferred = true;
+            return bitsd(0x7FF8000000000000ull);   // a quiet NaN: its tests come out false
+        }
         return static_cast<double>(stack_point_rt(col->S->nt, first, count, col->bx, y, col->bz));
     }
     TB_HD TB_FI bool vgradient(int k, int true_at, int false_at) const {
@@ -1749,8 +1774,12 @@ struct RuleCtx {
     }
     // OreVeinRule: the density inline (its guards usually end it after a y test), the rest
     // out of line
-    TB_HD TB_FI int ore_vein(int k, int ore, int raw, int filler, float chance) const {
+    TB_HD TB_FI int ore_vein(int k, int ore, int raw, int filler, float chance) {
         if (TB_ORE_MASK && !((ore_bits >> k) & 1)) return -1;
+        if (TB_DEFER_ORE && defer) {
+            deferred = true;
+            return -1;
+        }
         const LazyChannels ch{B, c, col->lx, col->lz, y, 0u, {}};
         const float density = tbgen::gen_ore_density(k, col->S->nt, col->bx, y, col->bz, ch);
         if (density <= 0.0f) return -1;
@@ -1842,6 +1871,7 @@ TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
     R.min_surf = r.min_surface;
     R.sec_set = true;
     R.secondary = r.secondary;
+    R.defer = B.defer != nullptr;
     // The walk reads the column's air and fluid bits, which stay true while it runs (the rules
     // never make air or fluid). All lanes of a warp walk the same height: above its own
     // height a column holds air, which leaves the walk state as it starts.
@@ -1912,10 +1942,54 @@ TB_HD inline void body_surface_walk_rules(const Batch& B, int it) {
             R.water_height = water_height;
             R.biome_v = static_cast<int>((bq >> (8 * (r & 3))) & 255u);
             R.ore_bits = (oq >> (8 * (r & 3))) & 255u;
-            const int state = tbgen::apply_rules(R);
+            R.deferred = false;
+            int state = tbgen::apply_rules(R);
+            if (R.deferred) {
+                const int32_t slot = add32(B.defer_count, 1);
+                if (slot < B.defer_cap) {
+                    B.defer[slot] = DeferRec{ci, static_cast<int16_t>(y), static_cast<int16_t>(stone_above), static_cast<int16_t>(R.stone_below),
+                                             water_height == INT_MIN ? kNoWater : static_cast<int16_t>(water_height), static_cast<uint8_t>(R.biome_v),
+                                             static_cast<uint8_t>(R.ore_bits), 0};
+                    continue;
+                }
+                // the list is full: the block's rules run here after all
+                R.defer = false;
+                state = tbgen::apply_rules(R);
+                R.defer = true;
+            }
             if (state >= 0) C.blocks[C.idx(y)] = static_cast<uint16_t>(state);
         }
     }
+}
+
+// deferred pass (item = index into the walk's deferred list): the material rules of a block
+// the walk left, from the inputs it recorded and its column's context (ColumnRec)
+TB_HD inline void body_walk_deferred(const Batch& B, int it) {
+    if (it >= B.defer_cap) return;
+    const DeferRec d = B.defer[it];
+    const int c = d.column >> 8, ci = d.column & 255, lx = ci >> 4, lz = ci & 15;
+    Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
+             B.h1[d.column]};
+    const ColumnRec& r = B.colrec[d.column];
+    RuleCtx R{};
+    R.col = &C;
+    R.B = &B;
+    R.c = c;
+    R.surface_depth = r.surface_depth;
+    R.grad_x = r.grad_x;
+    R.grad_z = r.grad_z;
+    R.min_set = true;
+    R.min_surf = r.min_surface;
+    R.sec_set = true;
+    R.secondary = r.secondary;
+    R.y = d.y;
+    R.stone_above = d.stone_above;
+    R.stone_below = d.stone_below;
+    R.water_height = d.water_height == kNoWater ? INT_MIN : d.water_height;
+    R.biome_v = d.biome;
+    R.ore_bits = d.ore_bits;
+    const int state = tbgen::apply_rules(R);
+    if (state >= 0) C.blocks[C.idx(d.y)] = static_cast<uint16_t>(state);
 }
 
 // pass 2c (item = chunk * 256 + z * 16 + x): the frozen-ocean extension after the rules

@@ -603,12 +603,13 @@ void launch(K kernel, cudaStream_t s, long items_hint, Args... args) {
 enum KernelId {
     K_NB_INSERT, K_NB_RESOLVE, K_CLIMATE_COL, K_CLIMATE_QUART, K_CHAIN, K_CC_INSERT, K_CC_RESOLVE, K_CORNER_COL, K_CORNER, K_ZOOM_TABLE,
     K_ZOOM_UNIFORM, K_SG_INSERT, K_SG_RESOLVE, K_SURFACE_LEVEL, K_AQ_CELL, K_AQ_QUERY, K_AQ_SKIP, K_INIT_HEIGHTS, K_FILL, K_SURFACE1,
-    K_BLOCK_BIOME, K_WALK, K_FROZEN, K_GATHER, K_AXIS_INSERT, K_AXIS_NUMBER, K_AXIS_FILL, K_COUNT
+    K_BLOCK_BIOME, K_WALK, K_FROZEN, K_GATHER, K_AXIS_INSERT, K_AXIS_NUMBER, K_AXIS_FILL, K_WALK_DEFER, K_COUNT
 };
 const char* const kKernelNames[K_COUNT] = {"nb_insert", "nb_resolve", "climate_col", "climate_quart", "chain", "cc_insert", "cc_resolve",
                                            "corner_col", "corner", "zoom_table", "zoom_uniform", "sg_insert", "sg_resolve", "surface_level",
                                            "aquifer_cell", "aquifer_query", "aquifer_skip", "init_heights", "fill", "surface1", "block_biome",
-                                           "walk_rules", "surface_frozen", "gather", "axis_insert", "axis_number", "axis_fill"};
+                                           "walk_rules", "surface_frozen", "gather", "axis_insert", "axis_number", "axis_fill",
+                                           "walk_deferred"};
 
 struct LaunchShape {
     int threads = 256;        // 32 .. 256, a multiple of 32 (the kernels are built for at most 256)
@@ -617,6 +618,9 @@ struct LaunchShape {
 };
 #ifndef TB_HOST_BATCH
 #define TB_HOST_BATCH 2048
+#endif
+#ifndef TB_DEFER_PER_CHUNK
+#define TB_DEFER_PER_CHUNK 8192
 #endif
 #ifndef TB_HOST_BATCH_U8
 #define TB_HOST_BATCH_U8 4096
@@ -630,6 +634,9 @@ struct HostSchedule {
 struct LaunchTable {
     LaunchShape k[K_COUNT];
     int table_load = 2;
+    // "walk_defer n": the column walk's deferred list holds n blocks per chunk of batch
+    // capacity (0: no deferred pass, every block's rules run in the walk)
+    int defer_per_chunk = TB_DEFER_PER_CHUNK;
     // host[0]: the u16 output form, host[1]: u8. The u16 form's copies are slower than its
     // kernels, so smaller batches start them sooner; the u8 form's are faster, the kernels
     // bound the step and larger batches win.
@@ -681,6 +688,10 @@ LaunchTable parse_launch_table(const std::string& text) {
             if (!(ls >> t.table_load) || t.table_load < 2 || t.table_load > 8) bad("table_load must be 2..8");
             continue;
         }
+        if (name == "walk_defer") {
+            if (!(ls >> t.defer_per_chunk) || t.defer_per_chunk < 0 || t.defer_per_chunk > 65536) bad("walk_defer must be 0..65536");
+            continue;
+        }
         if (name == "host_u8" || name == "host_u16") {
             HostSchedule& h = t.host[name == "host_u8" ? 1 : 0];
             if (!(ls >> h.batch >> h.tail_min >> h.tail_pct >> h.head_min >> h.head_pct)) bad("expected: host_u8|host_u16 batch tail_min tail_pct head_min head_pct");
@@ -706,6 +717,7 @@ LaunchTable parse_launch_table(const std::string& text) {
 std::string format_launch_table(const LaunchTable& t) {
     std::ostringstream o;
     o << "table_load " << t.table_load << "\n";
+    o << "walk_defer " << t.defer_per_chunk << "\n";
     for (int f = 1; f >= 0; --f) {
         const HostSchedule& h = t.host[f];
         o << (f ? "host_u8 " : "host_u16 ") << h.batch << ' ' << h.tail_min << ' ' << h.tail_pct << ' ' << h.head_min << ' ' << h.head_pct << "\n";
@@ -819,9 +831,11 @@ struct OutSlot {
 // two output slots run concurrently on two streams.
 struct Work {
     DevBuf d_coords, d_n, d_cx, d_cz, d_cs, d_nb9, d_bcol, d_tgt, d_lstar, d_mdist, d_qbiome, d_c25, d_ccol, d_corners, d_g513, d_sfts, d_aq_cell,
-        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_zoom_uni, d_bbiome, d_oremask, d_colmask, d_colrec, d_qnext, d_err, d_axtab, d_colax;
+        d_aq_query, d_aq_skip, d_h0, d_h1, d_h2, d_zoom, d_zoom_uni, d_bbiome, d_oremask, d_colmask, d_colrec, d_qnext, d_err, d_axtab, d_colax,
+        d_defer, d_defer_count;
     TableBufs tb_b, tb_c, tb_s, tb_a;
-    void alloc(int n, int load) {
+    int32_t defer_cap = 0;
+    void alloc(int n, int load, int defer_per_chunk) {
         const size_t N = static_cast<size_t>(n);
         // chunk x | chunk z | seed slot | count, the layout of an output slot's staged
         // coordinates, so that one copy uploads them
@@ -867,6 +881,9 @@ struct Work {
         if (TB_ORE_MASK) d_oremask.alloc(N * kBlocksPerChunk);
         d_colmask.alloc(sizeof(uint32_t) * N * 2 * kMaskWords * 256);
         d_colrec.alloc(sizeof(ColumnRec) * N * 256);
+        defer_cap = static_cast<int32_t>(std::min<size_t>(static_cast<size_t>(defer_per_chunk) * N, INT32_MAX / 2));
+        d_defer.alloc(sizeof(DeferRec) * static_cast<size_t>(defer_cap));
+        d_defer_count.alloc(sizeof(int32_t));
     }
 };
 
@@ -1002,7 +1019,7 @@ struct Generator {
 
     void alloc_batch(int n) {
         const size_t N = static_cast<size_t>(n);
-        for (int l = 0; l < lanes; ++l) work[l].alloc(n, lt.table_load);
+        for (int l = 0; l < lanes; ++l) work[l].alloc(n, lt.table_load, lt.defer_per_chunk);
         for (auto& o : out) {
             o.blocks.alloc(sizeof(uint16_t) * N * kBlocksPerChunk);
             o.biomes.alloc(N * kQuartsPerChunk);
@@ -1018,7 +1035,8 @@ struct Generator {
             const Work& W = work[l];
             for (const DevBuf* d : {&W.d_cx, &W.d_cz, &W.d_cs, &W.d_nb9, &W.d_bcol, &W.d_tgt, &W.d_lstar, &W.d_mdist, &W.d_qbiome, &W.d_c25, &W.d_ccol,
                                     &W.d_corners, &W.d_g513, &W.d_sfts, &W.d_aq_cell, &W.d_aq_query, &W.d_aq_skip, &W.d_h0, &W.d_h1, &W.d_h2,
-                                    &W.d_zoom, &W.d_zoom_uni, &W.d_bbiome, &W.d_oremask, &W.d_colmask, &W.d_colrec, &W.d_axtab, &W.d_colax})
+                                    &W.d_zoom, &W.d_zoom_uni, &W.d_bbiome, &W.d_oremask, &W.d_colmask, &W.d_colrec, &W.d_axtab, &W.d_colax,
+                                    &W.d_defer})
                 b += d->bytes;
             for (const TableBufs* t : {&W.tb_b, &W.tb_c, &W.tb_s, &W.tb_a}) b += t->keys.bytes + t->vals.bytes + t->uniq.bytes + t->owner.bytes;
         }
@@ -1138,6 +1156,9 @@ struct Generator {
         B.oremask = W.d_oremask.as<uint8_t>();
         B.colmask = W.d_colmask.as<uint32_t>();
         B.colrec = W.d_colrec.as<ColumnRec>();
+        B.defer = W.defer_cap > 0 ? W.d_defer.as<DeferRec>() : nullptr;
+        B.defer_count = W.d_defer_count.as<int32_t>();
+        B.defer_cap = W.defer_cap;
         return B;
     }
 
@@ -1168,6 +1189,7 @@ struct Generator {
         L.add(W.d_qnext.p, W.d_qnext.bytes, 0u);
         W.tb_b.add_reset(L);
         if (all) {
+            L.add(W.d_defer_count.p, W.d_defer_count.bytes, 0u);
             W.tb_c.add_reset(L);
             W.tb_s.add_reset(L);
             if (TB_AXIS_TABLE && tbm::kAxisLayers > 0) W.tb_a.add_reset(L);
@@ -1250,6 +1272,7 @@ struct Generator {
         run_body<body_block_biome, 256>(K_BLOCK_BIOME, W, s, 256L * nmax, B, n_dev);
         mark(6);
         run_body<body_surface_walk_rules, 256, TB_MINB_WALK>(K_WALK, W, s, 256 * nmax, B, n_dev);
+        if (W.defer_cap > 0) run_body<body_walk_deferred, 1>(K_WALK_DEFER, W, s, W.defer_cap, B, W.d_defer_count.as<int32_t>());
         mark(7);
         run_body<body_surface_frozen, 256>(K_FROZEN, W, s, 256 * nmax, B, n_dev);
         run_body<body_gather, kQuartsPerChunk>(K_GATHER, W, s, static_cast<long>(kQuartsPerChunk) * nmax, B, n_dev);
@@ -1273,7 +1296,7 @@ struct Generator {
     // a new launch table: graphs and (for a new table load) the batch buffers are rebuilt
     void set_launch_table(const LaunchTable& t) {
         finish();
-        const bool realloc = t.table_load != lt.table_load;
+        const bool realloc = t.table_load != lt.table_load || t.defer_per_chunk != lt.defer_per_chunk;
         lt = t;
         for (auto& o : out)
             if (o.graph) {

@@ -82,7 +82,7 @@ EXPORTS = ['tg_create', 'tg_destroy', 'tg_set_stream', 'tg_set_seed', 'tg_genera
 # the tunable kernels of a batch, in pipeline order (tg_kernel_times order)
 KERNELS = ['nb_insert', 'nb_resolve', 'climate_col', 'climate_quart', 'chain', 'cc_insert', 'cc_resolve', 'corner_col', 'corner', 'zoom_table',
            'zoom_uniform', 'sg_insert', 'sg_resolve', 'surface_level', 'aquifer_cell', 'aquifer_query', 'aquifer_skip', 'init_heights', 'fill',
-           'surface1', 'block_biome', 'walk_rules', 'surface_frozen', 'gather', 'axis_insert', 'axis_number', 'axis_fill']
+           'surface1', 'block_biome', 'walk_rules', 'surface_frozen', 'gather', 'axis_insert', 'axis_number', 'axis_fill', 'walk_deferred']
 
 
 class TerrainError(RuntimeError):

@@ -33,7 +33,7 @@ def main(argv):
     args = ap.parse_args(argv)
     side = args.side
     total = {s: {k: 0 for k in hostcheck.OP_KINDS} for s in hostcheck.STAGES}
-    meta_t = {'corner_columns': 0, 'surface_quarts': 0, 'biome_chunks': 0}
+    meta_t = {'corner_columns': 0, 'surface_quarts': 0, 'biome_chunks': 0, 'deferred_blocks': 0}
     for _, x0, z0 in bench.REGIONS:
         per, meta = hostcheck.count_ops(bench.SEED, bench.region_chunks(x0, z0, side))
         for s in per:
@@ -57,7 +57,7 @@ def main(argv):
                               'per work unit of the kernel', 'sample': '%dx%d chunks at the corner of each ladder region, one batch per region' % (side, side),
                       'seed': bench.SEED, 'per_kernel': kernels,
                       'units_in_sample': {'chunks': n, 'corner_columns': meta_t['corner_columns'], 'surface_quarts': meta_t['surface_quarts'],
-                                          'biome_chunks': meta_t['biome_chunks']}}
+                                          'biome_chunks': meta_t['biome_chunks'], 'walk_deferred_blocks': meta_t['deferred_blocks']}}
     with open(OUT, 'w') as f:
         json.dump(doc, f, indent=1, sort_keys=True)
         f.write('\n')

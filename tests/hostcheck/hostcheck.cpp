@@ -97,7 +97,10 @@ extern "C" {
 // Stages of the pipeline in the order (and with the names) of the library's tunable kernels.
 enum Stage { S_NB_INSERT, S_NB_RESOLVE, S_CLIMATE_COL, S_CLIMATE_QUART, S_CHAIN, S_CC_INSERT, S_CC_RESOLVE, S_CORNER_COL, S_CORNER, S_ZOOM_TABLE,
              S_ZOOM_UNIFORM, S_SG_INSERT, S_SG_RESOLVE, S_SURFACE_LEVEL, S_AQ_CELL, S_AQ_QUERY, S_AQ_SKIP, S_INIT_HEIGHTS, S_FILL, S_SURFACE1,
-             S_BLOCK_BIOME, S_WALK, S_FROZEN, S_GATHER, S_AXIS_INSERT, S_AXIS_NUMBER, S_AXIS_FILL, S_COUNT };
+             S_BLOCK_BIOME, S_WALK, S_FROZEN, S_GATHER, S_AXIS_INSERT, S_AXIS_NUMBER, S_AXIS_FILL, S_WALK_DEFER, S_COUNT };
+
+// blocks per chunk the host twin's deferred list holds (hc_set_defer; the library's default)
+int g_defer_per_chunk = 8192;
 
 // The pipeline for n chunks of one seed, stage by stage; with counts (S_COUNT x kOpKinds),
 // each stage's octave and simplex samples are counted into its row.
@@ -169,6 +172,11 @@ int run_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, 
     B.oremask = oremask.data();
     B.colmask = colmask.data();
     B.colrec = colrec.data();
+    int32_t defer_count = 0;
+    std::vector<DeferRec> defer(static_cast<size_t>(g_defer_per_chunk) * N);
+    B.defer = g_defer_per_chunk > 0 ? defer.data() : nullptr;
+    B.defer_count = &defer_count;
+    B.defer_cap = static_cast<int32_t>(defer.size());
     stage(S_NB_INSERT);
     each(9 * n, [&](int i) { body_nb_insert(B, i); });
     each(9 * n, [&](int i) { ht_number(B.hb, nb_key(B, i), i); });
@@ -223,6 +231,9 @@ int run_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, 
     each(256 * n, [&](int i) { body_block_biome(B, i); });
     stage(S_WALK);
     each(256 * n, [&](int i) { body_surface_walk_rules(B, i); });
+    stage(S_WALK_DEFER);
+    if (B.defer) each(std::min(defer_count, B.defer_cap), [&](int i) { body_walk_deferred(B, i); });
+    if (meta) meta[3] = defer_count;
     stage(S_FROZEN);
     each(256 * n, [&](int i) { body_surface_frozen(B, i); });
     stage(S_GATHER);
@@ -246,7 +257,12 @@ int hc_generate(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, u
 
 // The samples each stage evaluates for n chunks (one batch): counts is S_COUNT x kOpKinds
 // (volume, smeared volume, point, smeared point octave samples; simplex samples), and
-// meta[0..2] the batch's distinct corner columns, surface-level quarts and biome chunks.
+// meta[0..2] the batch's distinct corner columns, surface-level quarts and biome chunks,
+// meta[3] the blocks the column walk left to the deferred pass.
+// Blocks per chunk of the deferred list in the following calls (0: the walk keeps every
+// block), so that the tests can run the walk with a full list.
+void hc_set_defer(int32_t per_chunk) { g_defer_per_chunk = per_chunk; }
+
 int hc_count_ops(int64_t seed, const int32_t* cx, const int32_t* cz, int32_t n, long long* counts, int32_t* meta) {
     std::vector<uint16_t> bl(static_cast<size_t>(n) * kBlocksPerChunk);
     std::memset(counts, 0, sizeof(long long) * S_COUNT * kOpKinds);

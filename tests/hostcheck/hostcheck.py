@@ -32,6 +32,7 @@ def lib():
         L.hc_biome_point.argtypes = [ctypes.c_int64, vp, ctypes.c_int32, vp]
         L.hc_table_errors.argtypes = [ctypes.c_int32, ctypes.c_uint32, vp]
         L.hc_count_ops.argtypes = [ctypes.c_int64, vp, vp, ctypes.c_int32, vp, vp]
+        L.hc_set_defer.argtypes = [ctypes.c_int32]
         L.hc_table_errors.restype = ctypes.c_uint32
         _L = L
     return _L
@@ -107,7 +108,7 @@ def table_errors(n, cap):
 
 STAGES = ['nb_insert', 'nb_resolve', 'climate_col', 'climate_quart', 'chain', 'cc_insert', 'cc_resolve', 'corner_col', 'corner', 'zoom_table',
           'zoom_uniform', 'sg_insert', 'sg_resolve', 'surface_level', 'aquifer_cell', 'aquifer_query', 'aquifer_skip', 'init_heights', 'fill',
-          'surface1', 'block_biome', 'walk_rules', 'surface_frozen', 'gather', 'axis_insert', 'axis_number', 'axis_fill']
+          'surface1', 'block_biome', 'walk_rules', 'surface_frozen', 'gather', 'axis_insert', 'axis_number', 'axis_fill', 'walk_deferred']
 OP_KINDS = ['vol_octave', 'vol_octave_smeared', 'point_octave', 'point_octave_smeared', 'simplex']
 
 
@@ -121,4 +122,9 @@ def count_ops(seed, chunks):
     if lib().hc_count_ops(int(seed), _p(cx), _p(cz), a.shape[0], _p(counts), _p(meta)) != 0:
         raise RuntimeError('hc_count_ops failed')
     per = {s: {k: int(counts[i, j]) for j, k in enumerate(OP_KINDS)} for i, s in enumerate(STAGES)}
-    return per, {'corner_columns': int(meta[0]), 'surface_quarts': int(meta[1]), 'biome_chunks': int(meta[2])}
+    return per, {'corner_columns': int(meta[0]), 'surface_quarts': int(meta[1]), 'biome_chunks': int(meta[2]), 'deferred_blocks': int(meta[3])}
+
+
+def set_defer(per_chunk):
+    """Blocks per chunk the twin's deferred list holds from now on (0: the walk keeps all)."""
+    lib().hc_set_defer(int(per_chunk))

@@ -86,8 +86,10 @@ def test_device_queue_rejects_unaligned_outputs(small_gen):
 
 
 def test_launch_tables_change_no_output(ref_model):
-    """Work-queue forms, other block sizes and grids, and a larger hash-table load: the same
-    blocks and biomes as the compiled-in table; per-kernel times are gathered."""
+    """Work-queue forms, other block sizes and grids, a larger hash-table load, host-output
+    schedules and deferred-list sizes of the column walk (none; one block per chunk, so
+    that it fills): the same blocks and biomes as the compiled-in table; per-kernel times
+    are gathered."""
     g = terrain_b200.TerrainGenerator(max_batch_chunks=64)
     try:
         g.set_seed(4242)
@@ -108,9 +110,11 @@ def test_launch_tables_change_no_output(ref_model):
             assert (b == base[0]).all() and (q == base[1]).all()
         # host-output batch schedules: tails, heads and small batches cut the same chunks
         base8 = g.generate_u8(chunks)
-        for text in ['host_u8 16 4 50 4 200\nhost_u16 24 8 75 0 0\n', 'host_u8 0 0 0 0 0\nhost_u16 7 0 0 3 300\n']:
+        for text in ['host_u8 16 4 50 4 200\nhost_u16 24 8 75 0 0\n', 'host_u8 0 0 0 0 0\nhost_u16 7 0 0 3 300\nwalk_defer 1\n',
+                     'walk_defer 0\n']:
             g.set_launch_table(text)
-            assert len(terrain_b200.host_schedule(len(chunks), 64, u8=False, table=text)) > 2
+            if 'host_u16' in text:
+                assert len(terrain_b200.host_schedule(len(chunks), 64, u8=False, table=text)) > 2
             b, q = g.generate(chunks)
             assert (b == base[0]).all() and (q == base[1]).all()
             b8, q8 = g.generate_u8(chunks)

@@ -90,6 +90,24 @@ def test_random_chunks(ref_model):
         assert (aq == raq).all() and (b == rb).all() and (q == rq).all(), seed
 
 
+@pytest.mark.parametrize('per_chunk', [0, 1, 64])
+def test_walk_deferred_list_sizes(ref_model, per_chunk):
+    """The column walk leaves blocks whose rules need a per-block noise or an ore vein past
+    its bit to a deferred pass; with no list, or one that fills after a few blocks (the
+    rest run in the walk), the blocks are the same."""
+    seed = 4172144997902289642
+    chunks = CHUNKS[:6] + [(-62500, -62500), (-62499, -62500)]
+    try:
+        hostcheck.set_defer(per_chunk)
+        b, q = hostcheck.generate(seed, chunks)
+    finally:
+        hostcheck.set_defer(8192)
+    rb, rq = ref_model.seed(seed).generate(chunks)
+    assert (b == rb).all() and (q == rq).all()
+    per, meta = hostcheck.count_ops(seed, chunks)
+    assert meta['deferred_blocks'] > 100 * len(chunks)
+
+
 @pytest.mark.parametrize('seed', [123456789, -4172144997902289642])
 def test_biome_point_lookups(ref_model, seed):
     """The single-position lookup path (zoom corner, the quart's minimum and tie test, the
