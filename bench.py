@@ -47,8 +47,8 @@ BYTES_PER_CHUNK_U8 = 98304 + 1536
 # block read, its u16 state written, and the column air / fluid masks (2 x 12 words x 256 columns)
 WALK_BYTES_PER_CHUNK = 98304 * (1 + 1 + 2) + 2 * 12 * 4 * 256
 # dram__bytes_read.sum + dram__bytes_write.sum of one 4,096-chunk launch of the walk-rules
-# kernel in this workload (538.80 MB + 277.87 MB), from an ncu capture of that launch
-WALK_TRAFFIC_PER_LAUNCH = 816670000
+# kernel in this workload (515.35 MB + 288.65 MB), from a one-pass ncu capture of that launch
+WALK_TRAFFIC_PER_LAUNCH = 803998464
 # Instructions (per thread) one octave sample needs at least, by pipe, following the
 # reference's perlin_volume (cpu/include/mccuda/noise_eval.h:163-178): per axis the coordinate
 # in FP64 (scale multiply, wrap test, offset add, floor, floor back to double, subtract,
@@ -112,15 +112,52 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples during the timed region."""
+    """SM clock and clock-event reasons of the GPU sampled during the timed region: NVML
+    queries (read only) every 5 ms on a thread, from before the region starts to its end;
+    nvidia-smi at 100 ms when NVML cannot be loaded. dev is the CUDA device ordinal; the
+    NVML handle is found by its PCI address."""
 
-    def __init__(self, index):
-        self.index = index
+    REASONS = (('hw_slowdown', 0x8), ('hw_thermal_slowdown', 0x40), ('sw_thermal_slowdown', 0x20), ('sw_power_cap', 0x4))
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.samples = []          # (sm MHz, reason bits)
+        self.max_mhz = None
+        self.stop = threading.Event()
         self.proc = None
         self.lines = []
+        self.t = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.dev)
+        try:
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId('%08x:%02x:%02x.0' % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id))
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _poll(self, nv, h):
+        while not self.stop.is_set():
+            try:
+                self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except Exception:
+                pass
+            self.stop.wait(0.005)
 
     def __enter__(self):
-        cmd = ['nvidia-smi', '-i', str(self.index), '--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.t.start()
+            while not self.samples and self.t.is_alive():   # the first sample precedes the region
+                time.sleep(0.001)
+            return self
+        except Exception:
+            self.t = None
+        cmd = ['nvidia-smi', '-i', str(self.dev), '--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
                'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
                'clocks_event_reasons.sw_power_cap', '--format=csv,noheader,nounits', '-lms', '100']
         try:
@@ -136,15 +173,23 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        elif self.t:
+            self.t.join(timeout=1)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
+        sm, mx, reasons = [], self.max_mhz, set()
+        for mhz, bits in self.samples:
+            sm.append(float(mhz))
+            for name, bit in self.REASONS:
+                if bits & bit:
+                    reasons.add(name)
         for l in self.lines:
             f = [x.strip() for x in l.split(',')]
             if len(f) < 8:
@@ -154,11 +199,11 @@ class ClockSampler:
                 mx = float(f[1])
             except ValueError:
                 continue
-            names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
-            for n, v in zip(names, f[4:8]):
+            for (n, _), v in zip(self.REASONS, f[4:8]):
                 if v.lower() == 'active':
                     reasons.add(n)
-        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm)}
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': mx, 'reasons': sorted(reasons), 'samples': len(sm),
+                'source': 'nvml 5 ms' if self.samples else 'nvidia-smi 100 ms'}
 
 
 def host_cores():
@@ -736,12 +781,13 @@ def run_ours(args, rank, world, local_rank):
                    'parallelism': 'replicas: each GPU runs the full workload' if world > 1 else 'single GPU'},
         'stage_ms_per_step': {k: round(v, 3) for k, v in stage.items()},
         'roofline': roofline,
-        'roofline_walk_hbm': {'bound': 'hbm', 'kernel': 'surface_walk_rules', 'achieved': round(achieved, 2), 'peak': peak, 'unit': 'GB/s',
+        'roofline_walk_hbm': {'bound': 'hbm', 'kernel': 'surface_walk_rules and its deferred pass (walk_deferred)', 'achieved': round(achieved, 2), 'peak': peak, 'unit': 'GB/s',
                               'frac': round(achieved / peak, 5), 'traffic': WALK_TRAFFIC_PER_LAUNCH, 'peak_source': peak_kind,
                               'launch_ms': round(per_launch_ms, 3), 'share_of_step': round(per_launch_ms * calls / stage['kernel_ms'], 3),
                               'note': 'algorithmic bytes = 417,792 B per chunk (per block the u8 biome and u8 ore bits read and the u16 state '
-                                      'written, plus the column air / fluid masks) x 4,096 chunks per launch; traffic = dram read + write bytes of '
-                                      'one 4,096-chunk launch (ncu). The kernel is issue- and latency-bound, so its HBM fraction is small'},
+                                      'written, plus the column air / fluid masks) x 4,096 chunks per launch, over the time of the walk and its deferred '
+                                      'pass; traffic = dram read + write bytes of one 4,096-chunk walk launch (ncu; the deferred pass moves 16 B per '
+                                      'deferred block, about 3 MB). The kernels are issue- and latency-bound, so their HBM fraction is small'},
         'e2e': {'value': round(e2e_value, 1), 'unit': 'chunks/s', 'h2d_bytes_per_step': int(n * nreg * 8),
                 'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK_U8), 'd2h_gbs': round(e2e_value * BYTES_PER_CHUNK_U8 / 1e9, 2),
                 'pcie_d2h_gbs_measured': pcie, 'pcie_frac': round(e2e_value * BYTES_PER_CHUNK_U8 / 1e9 / pcie, 3) if pcie else None,

@@ -56,7 +56,7 @@ typedef struct tg_timing {
     float h2d_ms, biome_ms, noise_ms, aquifer_ms, fill_ms, surface_ms, d2h_ms, kernel_ms, wall_ms;
     int32_t batches;
     int32_t launches;     /* kernels launched by the call */
-    float walk_rules_ms;  /* the column walk with the rule tree (part of surface_ms) */
+    float walk_rules_ms;  /* the column walk with the rule tree and its deferred pass (part of surface_ms) */
     float corner_ms;      /* the channel-corner kernel (part of noise_ms) */
 } tg_timing;
 

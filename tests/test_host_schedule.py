@@ -1,5 +1,6 @@
 """Host logic: the batch schedule of calls with host outputs (tg_host_schedule, the launch
-table's host_u8 / host_u16 lines). No GPU: the schedule and the table parser run on the host."""
+table's host_u8 / host_u16 lines), and the launch-table parser's errors. No GPU: both run on
+the host."""
 import numpy as np
 import pytest
 
@@ -64,7 +65,8 @@ def test_random_counts_and_tables():
 
 
 @pytest.mark.parametrize('bad', ['host_u8 4096 512 100 0 0', 'host_u8 4096 512 50 512 100', 'host_u16 -1 0 0 0 0',
-                                 'host_u8 4096 512', 'host_u16 2048 512 50 0 1001'])
+                                 'host_u8 4096 512', 'host_u16 2048 512 50 0 1001', 'walk_defer -1', 'walk_defer 70000',
+                                 'table_load 9', 'corner 300 8 0', 'no_such_kernel 128 8 0'])
 def test_bad_lines_are_errors(bad):
     with pytest.raises(terrain_b200.TerrainError) as e:
         terrain_b200.host_schedule(100, 4096, table=bad + '\n')
