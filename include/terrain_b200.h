@@ -118,8 +118,10 @@ tg_status tg_write_region(struct tg_generator* gen, int64_t seed, int32_t x0, in
 
 /* Device-resident form: chunks, blocks_out and biomes_out (may be NULL) are device
  * pointers; count <= max_batch_chunks; runs on the generator's stream and returns
- * when the work is done. No counterpart in the reference (its buffers are host-side);
- * used to measure the kernels with inputs already in HBM. */
+ * when the work is done. The kernels write blocks_out and biomes_out in place when both
+ * are 16-byte aligned (else through the generator's buffers and a device copy). No
+ * counterpart in the reference (its buffers are host-side); used to measure the kernels
+ * with inputs already in HBM. */
 tg_status tg_generate_device(struct tg_generator* gen, const tg_chunk_xz* chunks_dev, int32_t count, uint16_t* blocks_dev, uint8_t* biomes_dev,
                              tg_timing* timing);
 

@@ -1667,11 +1667,21 @@ struct Generator {
         cudaStream_t s = stream;
         launch(k_split_chunks, s, count, chunks_dev, count, static_cast<int32_t>(current_slot), W.d_cx.as<int32_t>(), W.d_cz.as<int32_t>(),
                W.d_cs.as<int32_t>(), W.d_n.as<int32_t>());
-        const Batch B = batch_view(W, &o);
+        // The kernels write the caller's buffers directly when they are 16-byte aligned (the
+        // pipeline reads and writes them only within the count chunks); otherwise the
+        // output slot's buffers and a device-to-device copy.
+        const bool direct = reinterpret_cast<uintptr_t>(blocks_dev) % 16 == 0 && reinterpret_cast<uintptr_t>(biomes_dev) % 16 == 0;
+        Batch B = batch_view(W, &o);
+        if (direct) {
+            B.blocks = blocks_dev;
+            if (biomes_dev) B.biomes_out = biomes_dev;
+        }
         enqueue_batch(W, B, s, max_batch, nullptr, t != nullptr);
         if (t) add_stage_times(t);
-        ck(cudaMemcpyAsync(blocks_dev, o.blocks.p, sizeof(uint16_t) * count * kBlocksPerChunk, cudaMemcpyDeviceToDevice, s), "d2d");
-        if (biomes_dev) ck(cudaMemcpyAsync(biomes_dev, o.biomes.p, static_cast<size_t>(count) * kQuartsPerChunk, cudaMemcpyDeviceToDevice, s), "d2d");
+        if (!direct) {
+            ck(cudaMemcpyAsync(blocks_dev, o.blocks.p, sizeof(uint16_t) * count * kBlocksPerChunk, cudaMemcpyDeviceToDevice, s), "d2d");
+            if (biomes_dev) ck(cudaMemcpyAsync(biomes_dev, o.biomes.p, static_cast<size_t>(count) * kQuartsPerChunk, cudaMemcpyDeviceToDevice, s), "d2d");
+        }
         ck(cudaGetLastError(), "kernel launch");
         ck(cudaStreamSynchronize(s), "sync");
         check_device_errors();

@@ -47,10 +47,11 @@ def test_batch_larger_than_one_device_batch(ref_model):
 
 
 def test_host_batches_equal_whole_device_batches(ref_model):
-    """tg_generate cuts host-output work into batches of at most 2,048 chunks (then halving
-    tail batches, down to 512); on a generator of capacity 4,096 its result for 5,100 chunks
-    equals the device-resident form run on whole 4,096-chunk batches, and its last chunks
-    equal the reference."""
+    """tg_generate cuts host-output work into the batches of the launch table's host_u16
+    schedule; on a generator of capacity 4,096 its result for 5,100 chunks equals the
+    device-resident form run on whole 4,096-chunk batches (written in place into aligned
+    buffers; through the generator's buffers and a copy into unaligned ones, and with no
+    biome buffer), and its last chunks equal the reference."""
     import torch
     g = terrain_b200.TerrainGenerator(max_batch_chunks=4096)
     try:
@@ -66,6 +67,20 @@ def test_host_batches_equal_whole_device_batches(ref_model):
             torch.cuda.synchronize()
             assert (dev_b[:n].cpu().numpy().view(np.uint16) == b[off:off + n]).all(), off
             assert (dev_q[:n].cpu().numpy() == q[off:off + n]).all(), off
+        # unaligned outputs (2 and 1 bytes past a 16-byte boundary), then no biome buffer
+        n = 70
+        part = torch.from_numpy(np.ascontiguousarray(chunks[:n])).cuda()
+        flat_b = torch.zeros(n * g.height * 256 + 16, dtype=torch.int16, device='cuda')
+        flat_q = torch.zeros(n * g.qper + 16, dtype=torch.uint8, device='cuda')
+        g.generate_device(part.data_ptr(), n, flat_b.data_ptr() + 2, flat_q.data_ptr() + 1, timing=False)
+        torch.cuda.synchronize()
+        got_b = flat_b[1:1 + n * g.height * 256].cpu().numpy().view(np.uint16).reshape(b[:n].shape)
+        assert (got_b == b[:n]).all() and (flat_q[1:1 + n * g.qper].cpu().numpy().reshape(q[:n].shape) == q[:n]).all()
+        assert int(flat_b[0]) == 0 and int(flat_q[0]) == 0
+        dev_b.zero_()
+        g.generate_device(part.data_ptr(), n, dev_b.data_ptr(), None, timing=False)
+        torch.cuda.synchronize()
+        assert (dev_b[:n].cpu().numpy().view(np.uint16) == b[:n]).all()
         tail = [tuple(int(v) for v in c) for c in chunks[-6:]]
         rb, rq = ref_model.seed(777).generate(tail)
         assert (b[-6:] == rb).all() and (q[-6:] == rq).all()
