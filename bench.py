@@ -344,7 +344,8 @@ def p99_interval(lat):
 
 
 def served_bench(g, n_unique=96, batch_chunks=768, loads=(0.6, 0.7, 0.8), seed=2024, p99_target_ms=20.0, seconds=10.0, min_requests=5000):
-    """Plain against served on a stream of view-distance requests: the plain
+    """Plain against served on a stream of view-distance requests (squares and rings of radius
+    2-12 around centres within +/-117,187 chunks, seeds from a resident pool): the plain
     form is one synchronous tg_generate per request, in order; the server runs the same
     stream in both output forms (u16, and u8 through tg_server_submit_u8). For each form: the
     saturated throughput (everything submitted at once), then Poisson arrivals at each

@@ -82,7 +82,7 @@ def fold_chunk_list(ref_seed, ir_path=IR_PATH):
 
 
 # Reference corpus positions (Corpus.java:185-234): origin, near / far / world border,
-# the wrap chunks, BASELINE's +/-117,187 reading, eroded-badlands and frozen-ocean chunks
+# the wrap chunks, chunks at +/-117,187 (the world border read as a chunk coordinate), eroded-badlands and frozen-ocean chunks
 # of the model, and chunks past the BlockPos wrap of the aquifer cell locations.
 CORPUS = [(0, 0), (1, 0), (0, 1), (-1, -1), (6250, -6250), (-625000, 625000), (1874999, -1874999), (-1874999, 1874999), (6128, -6129),
           (-6129, 6128), (117187, -117187), (-4000, -3360), (-4000, -1440), (-4000, 1600), (2097148, -2097149), (3000000, -5000000),
