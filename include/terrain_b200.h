@@ -296,6 +296,9 @@ tg_status tg_viewer_destroy(struct tg_viewer* viewer);
  *   table_load <2..8>
  *   host_u8 <batch> <tail_min> <tail_pct 0..99> <head_min> <head_pct 0|101..1000>
  *   host_u16 (the same)
+ *   walk_defer <0..65536>       blocks per chunk of batch capacity in the column walk's
+ *                               deferred list (blocks whose material rules need a per-block
+ *                               noise; 0: no deferred pass)
  * host_u8 / host_u16: the batches of calls with host outputs in that form hold at most
  * batch chunks (0: max_batch_chunks); at the end of a call they shrink, each tail_pct % of
  * the one before, down to tail_min chunks; at the start they grow from head_min chunks by
@@ -306,7 +309,7 @@ tg_status tg_viewer_destroy(struct tg_viewer* viewer);
  * pipeline order: nb_insert nb_resolve climate_col climate_quart chain cc_insert cc_resolve
  * corner_col corner zoom_table zoom_uniform sg_insert sg_resolve surface_level aquifer_cell
  * aquifer_query aquifer_skip init_heights fill surface1 block_biome walk_rules
- * surface_frozen gather axis_insert axis_number axis_fill (the chain kernel has no
+ * surface_frozen gather axis_insert axis_number axis_fill walk_deferred (the chain kernel has no
  * work-queue form). Results do not depend on the table. No counterpart in the reference (its launch shapes are constants). */
 tg_status tg_set_launch_table(struct tg_generator* gen, const char* text);   /* NULL: the compiled-in table */
 /* The table in use, as text (needed: its size with the terminating zero). */
