@@ -7,16 +7,17 @@ TERRAIN step over all 12,288 chunks: biomes, density with caves, aquifers, ore v
 material rules, u16 block states and u8 quart biomes out.
 
   value      chunks/s with the chunk lists already in HBM and the outputs left in HBM
-             (tg_generate_device), device time from CUDA events on the launching stream
+             (tg_generate_device, the step's 12,288 chunks as one batch), device time from
+             CUDA events on the launching stream
   e2e        chunks/s through tg_generate_u8 -- the reference generator's own call and output
              type (u8 palette index per block) -- with host buffers: the chunk list is copied
              in and every block and biome byte copied out to pinned memory inside the step;
              e2e_u16 is the same through tg_generate (u16 block states, the CPU port's type)
-  roofline   the largest kernel, the channel corners, against the issue rate: its work
-             counted in the reference port (octave samples of the corner phase, per distinct
-             corner point) times a minimal instruction recipe per sample, over its CUDA-event
-             launch time; roofline_walk_hbm gives the column walk's HBM fraction (417,792 B
-             per chunk over its launch time, against the measured HBM copy peak)
+  roofline   the channel-corner kernel against the issue rate: its work counted on the host
+             twin of the kernel bodies (octave samples per distinct corner point) times a
+             minimal instruction recipe per sample, over its CUDA-event launch time;
+             roofline_walk_hbm gives the column walk's HBM fraction (417,792 B per chunk over
+             its launch time, against the measured HBM copy peak)
   reference_gpu  the reference's own GPU generator built for sm_100a on the same step and
              model (baseline/): end to end and kernels only, with our ratios
   cpu_baseline  the reference's own C++ port (oracle/_ref) on this host's cores: a 16x16
@@ -613,12 +614,12 @@ def reference_gpu_bench(steps=3, warmup=2):
     return out
 
 
-def corner_roofline(stats, n, sms, clocks):
+def corner_roofline(stats, n, regions, sms, clocks):
     """Issue roofline of the channel-corner kernel, the largest kernel of the step. Its work is
     counted, not guessed: the octave samples the kernel evaluates per corner point, counted
     on the host twin of the kernel bodies (tests/hostcheck/count_kernels.py: volume, smeared
     volume and point samples, lazy per-point evaluation), times the distinct corner points of
-    one 64 x 64-chunk launch (257 x 257 columns x 49 rows, each computed once), times the
+    one launch (257 x 257 columns x 49 rows, each computed once, per 64 x 64-chunk region), times the
     minimal instruction recipe of one sample (VOL_OCTAVE_INSTR). Peak: 4 warp instructions per
     clock per SM (32 threads each) at the SM clock sampled during the timed steps; the FP64
     pipe (64 lanes per SM per clock) is reported beside it. The reference port's eager volume
@@ -632,7 +633,7 @@ def corner_roofline(stats, n, sms, clocks):
     per_point = sum(oc['kernels']['per_kernel']['corner']['samples_per_unit'].values())
     port_per_point = (oc['per_chunk']['corners']['vol_octave'] + oc['per_chunk']['corners']['point_octave']) / (25 * 49)
     side = int(round(n ** 0.5))
-    points = (side * 4 + 1) ** 2 * 49
+    points = (side * 4 + 1) ** 2 * 49 * regions
     samples = points * per_point
     per_sample = sum(VOL_OCTAVE_INSTR.values())
     instr = samples * per_sample
@@ -650,7 +651,7 @@ def corner_roofline(stats, n, sms, clocks):
             'peak_source': 'issue rate at the sampled SM clock (%s MHz), %d SMs' % (mhz, sms),
             'note': '%.2f octave samples per corner point (counted on the kernel bodies) x %d distinct corner points of one %d-chunk launch '
                     'x %d instructions per sample; the DRAM traffic is negligible (the kernel reads L2-resident tables)' %
-                    (per_point, points, n, per_sample)}
+                    (per_point, points, n * regions, per_sample)}
 
 
 def flythrough_bench(g, frames=90, radius=24, width=1280, height=720, speed=15.0):
@@ -686,16 +687,18 @@ def run_ours(args, rank, world, local_rank):
     import terrain_b200
     dev = local_rank
     torch.cuda.set_device(dev)
-    g = terrain_b200.TerrainGenerator(max_batch_chunks=SIDE * SIDE, device=dev)
+    nreg = len(REGIONS)
+    n = SIDE * SIDE
+    # The step's three regions go to the kernels as one 12,288-chunk batch (fewer kernel
+    # tails and launches than three 4,096-chunk batches: 29 against 31 ms per step)
+    g = terrain_b200.TerrainGenerator(max_batch_chunks=n * nreg, device=dev)
     stream = torch.cuda.current_stream()
     g.set_stream(stream.cuda_stream)
     g.set_seed(SEED)
-    nreg = len(REGIONS)
     host_chunks = [region_chunks(x0, z0) for _, x0, z0 in REGIONS]
-    d_chunks = [torch.from_numpy(c).cuda() for c in host_chunks]
-    n = SIDE * SIDE
-    d_blocks = [torch.empty(n * 98304, dtype=torch.int16, device='cuda') for _ in range(nreg)]
-    d_biomes = [torch.empty(n * 1536, dtype=torch.uint8, device='cuda') for _ in range(nreg)]
+    d_chunks = torch.from_numpy(np.concatenate(host_chunks)).cuda()
+    d_blocks = torch.empty(n * nreg * 98304, dtype=torch.int16, device='cuda')
+    d_biomes = torch.empty(n * nreg * 1536, dtype=torch.uint8, device='cuda')
 
     def barrier():
         if world > 1:
@@ -704,10 +707,9 @@ def run_ours(args, rank, world, local_rank):
 
     def step_device(stats=None):
         # the timed steps run without stage events; one extra step records the stage times
-        for r in range(nreg):
-            t = g.generate_device(d_chunks[r].data_ptr(), n, d_blocks[r].data_ptr(), d_biomes[r].data_ptr(), timing=stats is not None)
-            if stats is not None:
-                stats.append(t)
+        t = g.generate_device(d_chunks.data_ptr(), n * nreg, d_blocks.data_ptr(), d_biomes.data_ptr(), timing=stats is not None)
+        if stats is not None:
+            stats.append(t)
 
     for _ in range(args.warmup):
         step_device()
@@ -768,16 +770,16 @@ def run_ours(args, rank, world, local_rank):
     clocks = clk.summary()
     # the column walk with the rule tree, timed by its own CUDA events: its HBM fraction
     per_launch_ms = sum(t['walk_rules_ms'] for t in stats) / calls
-    algo_bytes = WALK_BYTES_PER_CHUNK * n
+    algo_bytes = WALK_BYTES_PER_CHUNK * n * nreg
     achieved = algo_bytes / (per_launch_ms / 1000.0) / 1e9
     peak, peak_kind = peaks()
-    roofline = corner_roofline(stats, n, torch.cuda.get_device_properties(dev).multi_processor_count, clocks)
+    roofline = corner_roofline(stats, n, nreg, torch.cuda.get_device_properties(dev).multi_processor_count, clocks)
     line = {
         'metric': METRIC, 'value': round(value, 1), 'unit': 'chunks/s', 'n_gpus': world, 'steps': args.steps, 'warmup': args.warmup,
         'ms_per_step': round(ms_max / args.steps, 3), 'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32+f64+int',
         'data': 'synthetic world model (project-authored, reference JSON formats); seeded chunk lists',
         'config': {'workload': 'ladder: one seed, three 64x64-chunk regions (origin, -1,000,000 blocks, +1,874,999-block border), 12,288 chunks per step',
-                   'seed': SEED, 'chunks_per_step': n * nreg, 'batch_chunks': n, 'l2': 'outputs (2.4 GB per step) larger than L2',
+                   'seed': SEED, 'chunks_per_step': n * nreg, 'batch_chunks': n * nreg, 'l2': 'outputs (2.4 GB per step) larger than L2',
                    'model_sha256': model_sha256(), 'samples_per_chunk': samples_per_chunk(),
                    'parallelism': 'replicas: each GPU runs the full workload' if world > 1 else 'single GPU'},
         'stage_ms_per_step': {k: round(v, 3) for k, v in stage.items()},
@@ -786,9 +788,9 @@ def run_ours(args, rank, world, local_rank):
                               'frac': round(achieved / peak, 5), 'traffic': WALK_TRAFFIC_PER_LAUNCH, 'peak_source': peak_kind,
                               'launch_ms': round(per_launch_ms, 3), 'share_of_step': round(per_launch_ms * calls / stage['kernel_ms'], 3),
                               'note': 'algorithmic bytes = 417,792 B per chunk (per block the u8 biome and u8 ore bits read and the u16 state '
-                                      'written, plus the column air / fluid masks) x 4,096 chunks per launch, over the time of the walk and its deferred '
-                                      'pass; traffic = dram read + write bytes of one 4,096-chunk walk launch (ncu; the deferred pass moves 16 B per '
-                                      'deferred block, about 3 MB). The kernels are issue- and latency-bound, so their HBM fraction is small'},
+                                      'written, plus the column air / fluid masks) x 12,288 chunks per launch, over the time of the walk and its '
+                                      'deferred pass; traffic = dram read + write bytes of one 12,288-chunk walk launch (ncu; the deferred pass moves '
+                                      '16 B per deferred block, about 10 MB). The kernels are issue- and latency-bound, so their HBM fraction is small'},
         'e2e': {'value': round(e2e_value, 1), 'unit': 'chunks/s', 'h2d_bytes_per_step': int(n * nreg * 8),
                 'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK_U8), 'd2h_gbs': round(e2e_value * BYTES_PER_CHUNK_U8 / 1e9, 2),
                 'pcie_d2h_gbs_measured': pcie, 'pcie_frac': round(e2e_value * BYTES_PER_CHUNK_U8 / 1e9 / pcie, 3) if pcie else None,
@@ -799,6 +801,12 @@ def run_ours(args, rank, world, local_rank):
         'gpu_launches': int(launches),
         'clocks': clocks,
     }
+    if not (args.no_serve and args.no_extra):
+        # the other forms on a generator of 4,096-chunk batches, as their workloads are quoted
+        g.close()
+        torch.cuda.empty_cache()
+        g = terrain_b200.TerrainGenerator(max_batch_chunks=n, device=dev)
+        g.set_seed(SEED)
     if not args.no_serve:
         g.set_stream(0)
         line['served'] = served_bench(g)

@@ -7,13 +7,13 @@ shapes -- threads per block {64, 128, 256}, resident-block grid cap {1 .. 16} bl
 (at most 2,048 threads per SM), and the kernel form: grid-stride loop (grab 0) or persistent
 work queue taking runs of grab * threads items (grab 1, 2, 4) -- with the other kernels held
 at their current best, measuring the kernel's own CUDA-event time (tg_kernel_times) over
-timed 4,096-chunk batches of the ladder workload (a 64x64-chunk region at the origin and
-one at block -1,000,000), and keeps the fastest. Kernels under 2 % of the step try a
+timed batches of the ladder workload (three 64x64-chunk regions, at the origin, at block
+-1,000,000 and at the +1,874,999-block border, as one 12,288-chunk batch, the form the
+benchmark times), and keeps the fastest. Kernels under 2 % of the step try a
 reduced set. Then the dedupe hash-table load (capacity >= 2 or 4 x the keys) is chosen by
 the whole step's time. Last, the batch schedule of calls with host outputs (the host_u8
 and host_u16 lines: largest batch, tail, head) is chosen per output form by timing tg_generate_u8 and tg_generate
-into pinned host memory over the three ladder regions (12,288 chunks per call, the third
-at the +1,874,999-block border). The table is written for build.py to compile in, with the
+into pinned host memory over the same 12,288 chunks. The table is written for build.py to compile in, with the
 step time of the table in use before and of the tuned one, each timed through the
 graph-launched device-resident form (tg_generate_device).
 """
@@ -30,8 +30,8 @@ sys.path.insert(0, HERE)
 import terrain_b200  # noqa: E402
 
 SEED = 0x5445525241494E31
-REGIONS = [(0, 0), (-62500, -62500)]
-HOST_REGIONS = REGIONS + [(117124, 117124)]
+REGIONS = [(0, 0), (-62500, -62500), (117124, 117124)]
+HOST_REGIONS = REGIONS
 THREADS = (64, 128, 256)
 BLOCKS_PER_SM = (1, 2, 3, 4, 6, 8, 12, 16)
 GRABS = (0, 1, 2, 4)
@@ -67,15 +67,15 @@ def fmt(table, load, sched=None, header=''):
 
 
 class Bench:
-    def __init__(self, batch=4096):
+    def __init__(self, side=64):
         import torch
         self.torch = torch
-        self.g = terrain_b200.TerrainGenerator(max_batch_chunks=batch)
+        self.n = side * side * len(REGIONS)
+        self.g = terrain_b200.TerrainGenerator(max_batch_chunks=self.n)
         self.g.set_seed(SEED)
-        side = int(round(batch ** 0.5))
-        self.n = side * side
         grid = lambda x0, z0: np.array([(x0 + x, z0 + z) for z in range(side) for x in range(side)], np.int32)
-        self.chunks = [torch.from_numpy(grid(x0, z0)).cuda() for x0, z0 in REGIONS]
+        # the regions as one batch (a list of one device chunk list)
+        self.chunks = [torch.from_numpy(np.concatenate([grid(x0, z0) for x0, z0 in REGIONS])).cuda()]
         self.blocks = torch.empty(self.n * 98304, dtype=torch.int16, device='cuda')
         self.biomes = torch.empty(self.n * 1536, dtype=torch.uint8, device='cuda')
         self.sched = {}
@@ -150,7 +150,7 @@ def candidates(kernel, big):
 
 
 # batch schedules of calls with host outputs, per form: largest batch, tail (min, pct), head (min, pct)
-HOST_BATCH = {'host_u8': (2048, 3072, 4096), 'host_u16': (1024, 2048, 3072, 4096)}
+HOST_BATCH = {'host_u8': (2048, 3072, 4096, 6144), 'host_u16': (1024, 2048, 3072, 4096)}
 TAILS = ((0, 0), (512, 50), (1024, 50), (256, 50), (512, 67), (512, 75))
 HEADS = ((0, 0), (512, 200), (1024, 200), (256, 200))
 
@@ -241,11 +241,11 @@ def main(argv):
               '# (grab 0: grid-stride loop; grab g > 0: persistent work queue, g * threads items per take),\n'
               '# table_load: dedupe hash tables of at least table_load x the most keys of a batch;\n'
               '# host_u8 / host_u16: batch tail_min tail_pct head_min head_pct of calls with host outputs.\n'
-              '# Two 64x64-chunk ladder regions, 4,096-chunk batches, graph-launched device step:\n'
+              '# Three 64x64-chunk ladder regions as one 12,288-chunk batch, device-resident step:\n'
               '# %s.\n'
               '# Three ladder regions in one call to pinned host memory: u8 %.3f -> %.3f ms, u16 %.3f -> %.3f ms.'
-              % (('%.3f ms per two batches (kernel shapes not re-tuned in this run)' % step_default) if args.schedule_only else
-                 ('the table in use before %.3f ms, tuned %.3f ms per two batches%s' % (step_default, step_tuned, '' if keep_tuned else ' (tuned slower: the previous shapes kept)')),
+              % (('%.3f ms per step (kernel shapes not re-tuned in this run)' % step_default) if args.schedule_only else
+                 ('the table in use before %.3f ms, tuned %.3f ms per step%s' % (step_default, step_tuned, '' if keep_tuned else ' (tuned slower: the previous shapes kept)')),
                  hs['host_u8']['before_ms'], hs['host_u8']['chosen_ms'], hs['host_u16']['before_ms'], hs['host_u16']['chosen_ms']))
     text = fmt(table, load, sched, header)
     with open(args.out, 'w') as f:
