@@ -1215,9 +1215,37 @@ TB_HD inline void cell_interp(const Batch& B, int c, int lx, int lz, int cell_y,
     const float* p01 = B.corners + (u01 * kRows + cell_y) * C;
     const float* p11 = B.corners + (u11 * kRows + cell_y) * C;
     const float az = static_cast<float>(zi) * 0.25f, ax = static_cast<float>(xi) * 0.25f;
+    // the two rows of the four corner columns (2 x C channels each), as 16-byte loads on the
+    // device where a row is a whole number of them (the buffer is cudaMalloc-aligned)
+    float r00[2 * C], r10[2 * C], r01[2 * C], r11[2 * C];
+#if defined(__CUDA_ARCH__)
+    if (C % 4 == 0) {
+        auto put = [](float* r, const float4 v) {
+            r[0] = v.x;
+            r[1] = v.y;
+            r[2] = v.z;
+            r[3] = v.w;
+        };
+#pragma unroll
+        for (int k = 0; k < 2 * C; k += 4) {
+            put(r00 + k, __ldg(reinterpret_cast<const float4*>(p00 + k)));
+            put(r10 + k, __ldg(reinterpret_cast<const float4*>(p10 + k)));
+            put(r01 + k, __ldg(reinterpret_cast<const float4*>(p01 + k)));
+            put(r11 + k, __ldg(reinterpret_cast<const float4*>(p11 + k)));
+        }
+    } else
+#endif
+    {
+        for (int k = 0; k < 2 * C; ++k) {
+            r00[k] = p00[k];
+            r10[k] = p10[k];
+            r01[k] = p01[k];
+            r11[k] = p11[k];
+        }
+    }
     for (int k = 0; k < C; ++k) {
-        const float v000 = p00[k], v100 = p10[k], v001 = p01[k], v101 = p11[k];
-        const float v010 = p00[C + k], v110 = p10[C + k], v011 = p01[C + k], v111 = p11[C + k];
+        const float v000 = r00[k], v100 = r10[k], v001 = r01[k], v101 = r11[k];
+        const float v010 = r00[C + k], v110 = r10[C + k], v011 = r01[C + k], v111 = r11[C + k];
         const float v00 = lerpf(az, v000, v001), v01 = lerpf(az, v010, v011);
         const float v10 = lerpf(az, v100, v101), v11 = lerpf(az, v110, v111);
         const float a0 = lerpf(ax, v00, v10), a1 = lerpf(ax, v01, v11);
@@ -1239,9 +1267,10 @@ TB_HD TB_FI int tile_column(int it) {
 #define TB_FILL_TILE 16
 #endif
 
-// item = (chunk * kCellsY + cell_y) * 256 + tile_column: the 8 blocks of one cell column
-TB_HD inline void body_fill(const Batch& B, int it) {
-    const int col = tile_column<TB_FILL_TILE>(it), cell_y = (it >> 8) % kCellsY, c = (it >> 8) / kCellsY;
+// The 8 blocks of one cell column. ORES: evaluate the ore veins of ore_live (else their bits
+// are 0, and the channels only they read are neither interpolated nor stepped).
+template <bool ORES>
+TB_HD TB_FI void fill_cell(const Batch& B, int c, int col, int cell_y, uint32_t ore_live) {
     const int lx = col & 15, lz = col >> 4;
     const int bx = B.cx[c] * 16 + lx, bz = B.cz[c] * 16 + lz;
     const DevSeed& S = B.seeds[B.cseed[c]];
@@ -1267,10 +1296,10 @@ TB_HD inline void body_fill(const Batch& B, int it) {
         const size_t bi = ((y - tbm::kMinY) * 16 + lz) * 16 + lx;
         out[bi] = static_cast<uint16_t>(s);
         if (B.density) B.density[static_cast<size_t>(c) * kBlocksPerChunk + bi] = d;
-        if (TB_ORE_MASK) {
+        if (ORES) {
             uint32_t om = 0;
             for (int v = 0; v < tbm::kNumOres; ++v)
-                if (!(tbgen::gen_ore_density(v, S.nt, bx, y, bz, ch) <= 0.0f)) om |= 1u << v;
+                if (((ore_live >> v) & 1u) && !(tbgen::gen_ore_density(v, S.nt, bx, y, bz, ch) <= 0.0f)) om |= 1u << v;
             if (k < 4) ore_lo |= om << (8 * k);
             else ore_hi |= om << (8 * (k - 4));
         }
@@ -1291,6 +1320,22 @@ TB_HD inline void body_fill(const Batch& B, int it) {
         ow[256] = ore_hi;
     }
     if (top != INT_MIN) max32(B.h0 + static_cast<size_t>(c) * 256 + lx * 16 + lz, top + 1);
+}
+
+// item = (chunk * kCellsY + cell_y) * 256 + tile_column: the 8 blocks of one cell column
+TB_HD inline void body_fill(const Batch& B, int it) {
+    const int col = tile_column<TB_FILL_TILE>(it), cell_y = (it >> 8) % kCellsY, c = (it >> 8) / kCellsY;
+    // the ore veins whose density can be above zero in this cell row, the same for the whole
+    // warp (its items share cell_y): rows where none can be skip the ore work
+#if defined(__CUDA_ARCH__)
+    const uint32_t ore_live = tbm::kOreLiveCellsDev[cell_y];
+#else
+    const uint32_t ore_live = tbm::kOreLiveCells[cell_y];
+#endif
+    if (TB_ORE_MASK && ore_live)
+        fill_cell<true>(B, c, col, cell_y, ore_live);
+    else
+        fill_cell<false>(B, c, col, cell_y, 0u);
 }
 
 // ---- BiomeManager zoom ---------------------------------------------------------------------

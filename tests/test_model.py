@@ -125,3 +125,35 @@ def test_float_literals_are_exact():
         f = np.float32(v)
         lit = gen_eval.flit(f)
         assert np.float32(float.fromhex(lit[:-1])) == f
+
+
+def _live_table():
+    """kOreLiveCells as compiled into the library (the generated header)."""
+    import re
+    text = open(os.path.join(REPO, 'minecraft-terrain-cuda_b200', '_gen', 'model_gen.cuh')).read()
+    m = re.search(r'constexpr uint32_t kOreLiveCells\[(\d+)\] = \{([^}]*)\}', text)
+    return [int(v.strip().rstrip('u'), 16) for v in m.group(2).split(',')]
+
+
+def test_ore_live_cells_against_the_port(ref_model):
+    """The fill evaluates an ore vein's density only in the cell rows whose bit is set in
+    kOreLiveCells. Where a bit is clear the port's density of that vein (ref_point on the
+    vein's density root) must be <= 0 at every height of the row, on every sampled column."""
+    M = gen_eval.Model(os.path.join(MODEL, 'overworld_ir.json'), os.path.join(MODEL, 'overworld_terrain.json'))
+    ores = gen_eval.Gen(M).ores
+    live = _live_table()
+    assert len(live) == M.height // 8
+    assert any(v != (1 << len(ores)) - 1 for v in live), 'no cell row skips a vein in this model'
+    rs = ref_model.seed(0x5445525241494E31)
+    import numpy as np
+    rng = np.random.default_rng(7)
+    cols = np.concatenate([rng.integers(-2000, 2000, size=(24, 2)), [[0, 0], [-1000000, 1874999], [6128 * 16, -6129 * 16]]])
+    ys = np.arange(M.min_y, M.min_y + M.height)
+    xyz = np.array([(x, y, z) for x, z in cols for y in ys], np.int32)
+    for k, o in enumerate(ores):
+        v = rs.point(M.roots[o['density']], xyz).reshape(len(cols), len(ys))
+        for cell in range(M.height // 8):
+            if (live[cell] >> k) & 1:
+                continue
+            block = v[:, 8 * cell:8 * cell + 8]
+            assert (block <= 0).all(), 'vein %d density above zero in skipped cell row %d' % (k, cell)
