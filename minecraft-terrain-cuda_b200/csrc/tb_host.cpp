@@ -12,6 +12,8 @@
 
 namespace tb {
 
+const int kYRows = tbm::kHeight / 8 + 1;
+
 // ---- hashes -------------------------------------------------------------------------------
 namespace {
 
@@ -371,6 +373,13 @@ void build_seed_host(int64_t seed, SeedHost& s) {
         ++placed;
     }
     for (int i = 0; i < 192; ++i) s.clay[i] = static_cast<uint16_t>(bands[i]);
+    // the corner context's y records: row r (height min_y + 8 r) holds the record of each
+    // entry of tbm::kYLayer, with the device's arithmetic (y_record)
+    const NoiseTables nt{s.off.data(), s.perm.data(), s.layers.data(), s.perm2.data()};
+    s.ytab.resize(static_cast<size_t>(kYRows) * tbm::kYLayers);
+    for (int r = 0; r < kYRows; ++r)
+        for (int e = 0; e < tbm::kYLayers; ++e)
+            s.ytab[static_cast<size_t>(r) * tbm::kYLayers + e] = y_record(nt, tbm::kYLayer[e], tbm::kYScale[e], tbm::kYSmeared[e], tbm::kMinY + 8 * r);
 }
 
 // ---- climate R-tree (Climate.RTree build order) ------------------------------------------------

@@ -70,7 +70,13 @@ struct SeedHost {
     std::vector<Positional> gradient;
     int64_t zoom_seed = 0;
     uint16_t clay[192];
+    // per corner row, the y coordinate record of every volume-stack layer of the corner
+    // context (kYRows x tbm::kYLayers, row-major)
+    std::vector<AxisRec> ytab;
 };
+
+// corner rows of a chunk column (one per 8 heights, both ends included)
+extern const int kYRows;
 
 void build_model_host(ModelHost& m);
 void build_seed_host(int64_t seed, SeedHost& s);

@@ -324,58 +324,57 @@ struct AxisRec {
 #define TB_AXIS_SEL(table, plain) (plain)
 #endif
 
-// stack_volume_rt with the x / z records of layer first + k at ax[k], az[k]
-TB_HD TB_NOINLINE inline float stack_volume_ax_rt(const NoiseTables& T, int first, int count, const AxisRec* ax, const AxisRec* az, int32_t by, double yss,
-                                                   float amplitude) {
+// The y coordinate record of one octave layer at corner height by, for a stack of y scale
+// yss: the volume path's y setup (floor, fraction, smoothstep), or for a smeared stack
+// (SmearedPerlinNoise) the floor, the fudged fraction the gradients read and the smoothstep of
+// the plain fraction. It depends only on the seed, the layer and the height, so it is built
+// once per seed for every corner row (on the host) instead of once per sample.
+TB_HD TB_FI AxisRec y_record(const NoiseTables& T, int layer, double yss, bool smeared, int32_t by) {
+    const Layer L = T.layer[layer];
+    const double ys = yss * L.freq;
+    const OctaveOff o = T.off[L.oct];
+    if (!smeared) {
+        const AxisSetup Y = axis_setup(by, ys, o.oy);
+        return {Y.f, Y.r, Y.a, 0};
+    }
+    const double oy = static_cast<double>(by) * ys;
+    const double y = nwrap(oy) + o.oy;
+    const int32_t fy = jfloor_finite(y);
+    const double rel = y - static_cast<double>(fy);
+    const float ay = smoothf(static_cast<float>(rel));
+    const float fudged = static_cast<float>(rel - smear_fudge(oy, rel, o.smear));
+    return {fy, fudged, ay, 0};
+}
+
+// A volume stack (plain or smeared) with the x / z / y records of layer first + k at ax[k],
+// az[k], ay[k]
+template <bool SMEARED>
+TB_HD TB_NOINLINE inline float stack_volume_axy_rt(const NoiseTables& T, int first, int count, const AxisRec* ax, const AxisRec* az, const AxisRec* ay,
+                                                    float amplitude) {
     float acc = 0.0f;
 #pragma unroll 1
     for (int k = 0; k < count; ++k) {
-        TB_COUNT(kOpVolume);
+        TB_COUNT(SMEARED ? kOpVolumeSmeared : kOpVolume);
         const Layer L = T.layer[first + k];
-        const double ys = yss * L.freq;
         const float amp = amplitude * L.amp;
-        const AxisRec X = ax[k], Z = az[k];
-        const AxisSetup Y = axis_setup(by, ys, T.off[L.oct].oy);
+        const AxisRec X = ax[k], Z = az[k], Y = ay[k];
         const CellHash c = octave_hash(T, L.oct, X.f, Y.f, Z.f);
         acc = acc + amp * cell_volume(c, X.r, Z.r, Y.r, X.a, Y.a, Z.a);
     }
     return acc;
 }
 
-TB_HD TB_NOINLINE inline float stack_volume_smeared_ax_rt(const NoiseTables& T, int first, int count, const AxisRec* ax, const AxisRec* az, int32_t by,
-                                                           double yss, float amplitude) {
-    float acc = 0.0f;
-#pragma unroll 1
-    for (int k = 0; k < count; ++k) {
-        TB_COUNT(kOpVolumeSmeared);
-        const Layer L = T.layer[first + k];
-        const double ys = yss * L.freq;
-        const float amp = amplitude * L.amp;
-        const AxisRec X = ax[k], Z = az[k];
-        const OctaveOff o = T.off[L.oct];
-        const double oy = static_cast<double>(by) * ys;
-        const double y = nwrap(oy) + o.oy;
-        const int32_t fy = jfloor_finite(y);
-        const double rel = y - static_cast<double>(fy);
-        const float ay = smoothf(static_cast<float>(rel));
-        const CellHash c = octave_hash(T, L.oct, X.f, fy, Z.f);
-        const float fudged = static_cast<float>(rel - smear_fudge(oy, rel, o.smear));
-        acc = acc + amp * cell_volume(c, X.r, Z.r, fudged, X.a, ay, Z.a);
-    }
-    return acc;
-}
-
 template <int FIRST, int COUNT, bool SMEARED>
-TB_HD TB_FI float stack_volume_ax(const NoiseTables& T, const AxisRec* ax, const AxisRec* az, int32_t by, double yss, float amplitude) {
-    return SMEARED ? stack_volume_smeared_ax_rt(T, FIRST, COUNT, ax, az, by, yss, amplitude) : stack_volume_ax_rt(T, FIRST, COUNT, ax, az, by, yss, amplitude);
+TB_HD TB_FI float stack_volume_ax(const NoiseTables& T, const AxisRec* ax, const AxisRec* az, const AxisRec* ay, float amplitude) {
+    return stack_volume_axy_rt<SMEARED>(T, FIRST, COUNT, ax, az, ay, amplitude);
 }
 
 // The same stacks with the layer run chosen per thread: threads of a warp that evaluate
 // different stacks of one noise (a blended noise's lower or upper limit) share one call.
 template <bool SMEARED>
-TB_HD TB_FI float stack_volume_ax_dyn(const NoiseTables& T, int first, int count, const AxisRec* ax, const AxisRec* az, int32_t by, double yss,
+TB_HD TB_FI float stack_volume_ax_dyn(const NoiseTables& T, int first, int count, const AxisRec* ax, const AxisRec* az, const AxisRec* ay,
                                       float amplitude) {
-    return SMEARED ? stack_volume_smeared_ax_rt(T, first, count, ax, az, by, yss, amplitude) : stack_volume_ax_rt(T, first, count, ax, az, by, yss, amplitude);
+    return stack_volume_axy_rt<SMEARED>(T, first, count, ax, az, ay, amplitude);
 }
 template <bool SMEARED>
 TB_HD TB_FI float stack_volume_dyn(const NoiseTables& T, int first, int count, int32_t bx, int32_t by, int32_t bz, double xzs, double yss, float amplitude) {

@@ -76,6 +76,7 @@ struct DevModel {
 
 struct DevSeed {
     NoiseTables nt;
+    const AxisRec* ytab;   // per corner row, the y record of each corner-context volume layer
     Positional random, aquifer, ore;
     Positional gradient[kMaxGradientRandoms];
     int64_t zoom_seed;
@@ -900,7 +901,8 @@ TB_HD inline void body_corner(const Batch& B, int it) {
     const AxisRec* ax = nullptr;
     const AxisRec* az = nullptr;
 #endif
-    tbgen::gen_corner(B.seeds[slot].nt, qx * 4, tbm::kMinY + 8 * row, qz * 4, B.ccol + static_cast<size_t>(u) * tbm::kCornerCols, ax, az,
+    const AxisRec* ay = B.seeds[slot].ytab + static_cast<size_t>(row) * tbm::kYLayers;
+    tbgen::gen_corner(B.seeds[slot].nt, qx * 4, tbm::kMinY + 8 * row, qz * 4, B.ccol + static_cast<size_t>(u) * tbm::kCornerCols, ax, az, ay,
                       B.corners + (static_cast<size_t>(u) * kRows + row) * tbm::kNumChannels);
 }
 

@@ -810,7 +810,7 @@ struct SeedSlot {
     int64_t seed = 0;
     bool valid = false;
     uint64_t last_use = 0;
-    DevBuf tables;   // octave offsets | layers | paired permutations | byte permutations, 256-byte aligned
+    DevBuf tables;   // octave offsets | layers | paired permutations | byte permutations | corner y records, 256-byte aligned
 };
 
 // one output buffer set (the pipeline's outputs are double-buffered)
@@ -1089,18 +1089,21 @@ struct Generator {
         auto al = [](size_t v) { return (v + 255) & ~static_cast<size_t>(255); };
         const size_t b_off = sizeof(OctaveOff) * h.off.size(), b_lay = sizeof(Layer) * h.layers.size(), b_p2 = sizeof(uint16_t) * h.perm2.size();
         const size_t b_p = TB_PERM_PAIRS ? 0 : h.perm.size();
-        const size_t o_lay = al(b_off), o_p2 = o_lay + al(b_lay), o_p = o_p2 + al(b_p2), total = o_p + al(b_p);
+        const size_t b_y = sizeof(AxisRec) * h.ytab.size();
+        const size_t o_lay = al(b_off), o_p2 = o_lay + al(b_lay), o_p = o_p2 + al(b_p2), o_y = o_p + al(b_p), total = o_y + al(b_y);
         seed_image.assign(total, 0);
         std::memcpy(seed_image.data(), h.off.data(), b_off);
         std::memcpy(seed_image.data() + o_lay, h.layers.data(), b_lay);
         std::memcpy(seed_image.data() + o_p2, h.perm2.data(), b_p2);
         if (b_p) std::memcpy(seed_image.data() + o_p, h.perm.data(), b_p);
+        if (b_y) std::memcpy(seed_image.data() + o_y, h.ytab.data(), b_y);
         if (!sl.tables.p || sl.tables.bytes != total) sl.tables.alloc(total);
         ck(cudaMemcpy(sl.tables.p, seed_image.data(), total, cudaMemcpyHostToDevice), "seed upload");
         const uint8_t* base = sl.tables.as<uint8_t>();
         DevSeed d{};
         d.nt = NoiseTables{reinterpret_cast<const OctaveOff*>(base), b_p ? base + o_p : nullptr, reinterpret_cast<const Layer*>(base + o_lay),
                            reinterpret_cast<const uint16_t*>(base + o_p2)};
+        d.ytab = reinterpret_cast<const AxisRec*>(base + o_y);
         d.random = h.random;
         d.aquifer = h.aquifer;
         d.ore = h.ore;

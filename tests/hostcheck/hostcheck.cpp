@@ -58,6 +58,7 @@ struct HostRun {
         M.f2 = m.f2;
         M.g2 = m.g2;
         D.nt = NoiseTables{s.off.data(), s.perm.data(), s.layers.data(), s.perm2.data()};
+        D.ytab = s.ytab.data();
         D.random = s.random;
         D.aquifer = s.aquifer;
         D.ore = s.ore;
@@ -319,12 +320,14 @@ void axis_row(const NoiseTables& T, int32_t b, bool z, AxisRec* row) {
 int hc_corners(int64_t seed, const int32_t* xyz, int32_t n, float* out) {
     HostRun R(seed);
     float col[tbm::kCornerCols];
-    std::vector<AxisRec> ax(std::max(1, tbm::kAxisLayers)), az(std::max(1, tbm::kAxisLayers));
+    std::vector<AxisRec> ax(std::max(1, tbm::kAxisLayers)), az(std::max(1, tbm::kAxisLayers)), ay(std::max(1, tbm::kYLayers));
     for (int i = 0; i < n; ++i) {
         tbgen::gen_corner_col(R.D.nt, xyz[3 * i], xyz[3 * i + 2], col);
         axis_row(R.D.nt, xyz[3 * i], false, ax.data());
         axis_row(R.D.nt, xyz[3 * i + 2], true, az.data());
-        tbgen::gen_corner(R.D.nt, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], col, ax.data(), az.data(), out + tbm::kNumChannels * i);
+        // the y records at this height, as the seed's table holds them for a corner row
+        for (int e = 0; e < tbm::kYLayers; ++e) ay[e] = y_record(R.D.nt, tbm::kYLayer[e], tbm::kYScale[e], tbm::kYSmeared[e], xyz[3 * i + 1]);
+        tbgen::gen_corner(R.D.nt, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], col, ax.data(), az.data(), ay.data(), out + tbm::kNumChannels * i);
     }
     return 0;
 }
