@@ -910,6 +910,7 @@ struct Generator {
     // seeds
     std::unique_ptr<SeedSlot[]> slots;
     DevBuf d_seeds;
+    DevBuf call_chunks;   // the chunk list of a call with host outputs (grown to the largest call)
     uint64_t use_clock = 0;
     int current_slot = -1;
     // working buffers per lane: lane 0 runs on `stream`, lane 1 on lane_stream
@@ -1338,14 +1339,19 @@ struct Generator {
         ck(cudaMemcpyAsync(W.d_coords.p, o.coords.p, 4 * (3 * static_cast<size_t>(max_batch) + 1), cudaMemcpyHostToDevice, s), "h2d");
     }
 
-    // Runs one batch whose staged coordinates sit in o.coords into output slot o.
+    // Runs one batch into output slot o: its chunks from dev_chunks (n entries of a device
+    // chunk list, current seed) or, when that is null, the staged coordinates in o.coords.
     // narrow: also write u8 copies of the blocks (and aquifer blocks) for the u8 output form.
-    void run_batch(OutSlot& o, int n, tg_timing* t, bool want_aquifer, bool narrow = false) {
+    void run_batch(OutSlot& o, int n, tg_timing* t, bool want_aquifer, bool narrow = false, const tg_chunk_xz* dev_chunks = nullptr) {
         Work& W = work[o.lane];
         cudaStream_t s = o.lane ? lane_stream : stream;
         if (o.busy) ck(cudaStreamWaitEvent(s, o.drained, 0), "wait");   // the slot's previous outputs are copied out
         // the lane's own buffers: ready while the other lane's batch still runs
-        upload_coords(W, o, n, s);
+        if (dev_chunks)
+            launch(k_split_chunks, s, n, dev_chunks, n, static_cast<int32_t>(current_slot), W.d_cx.as<int32_t>(), W.d_cz.as<int32_t>(),
+                   W.d_cs.as<int32_t>(), W.d_n.as<int32_t>());
+        else
+            upload_coords(W, o, n, s);
         reset_lane(W, s, true);
         // A batch that fills the GPU alone runs after the previous one rather than beside it,
         // so each finishes (and its copy starts) as early as possible; smaller ones overlap.
@@ -1482,22 +1488,24 @@ struct Generator {
     void generate(const tg_chunk_xz* chunks, int count, uint16_t* blocks, uint8_t* biomes, uint16_t* aquifer, tg_timing* t,
                   uint8_t* blocks8 = nullptr, uint8_t* aquifer8 = nullptr) {
         if (current_slot < 0) throw Error(TG_ERR_NO_SEED, "tg_set_seed has not been called");
-        order_lanes();
         check_chunks(chunks, count);
-        std::vector<int32_t> cx(max_batch), cz(max_batch), cs(max_batch, current_slot);
+        // The call's chunk list goes to the device once, ahead of lane 1's start; each batch
+        // takes its part on its lane (k_split_chunks), so the host queues every batch without
+        // waiting for earlier ones (the slots' events order the reuse of their buffers) and a
+        // late host thread leaves no gap between batches.
+        if (count > 0) {
+            if (call_chunks.bytes < sizeof(tg_chunk_xz) * static_cast<size_t>(count)) call_chunks.alloc(sizeof(tg_chunk_xz) * static_cast<size_t>(count));
+            ck(cudaMemcpyAsync(call_chunks.p, chunks, sizeof(tg_chunk_xz) * static_cast<size_t>(count), cudaMemcpyHostToDevice, stream), "h2d");
+        }
+        order_lanes();
         const HostSchedule& hs = lt.host[blocks8 ? 1 : 0];
         const int hb = hs.batch > 0 ? std::min(max_batch, hs.batch) : max_batch;
         int off = 0;
         for (const int n : host_schedule(count, hb, hs)) {
-            for (int i = 0; i < n; ++i) {
-                cx[i] = chunks[off + i].x;
-                cz[i] = chunks[off + i].z;
-            }
             OutSlot& o = out[next_out];
             next_out ^= 1;
-            stage(o, n, cx.data(), cz.data(), cs.data());
             const bool narrow = blocks8 != nullptr;
-            run_batch(o, n, t, narrow ? aquifer8 != nullptr : aquifer != nullptr, narrow);
+            run_batch(o, n, t, narrow ? aquifer8 != nullptr : aquifer != nullptr, narrow, call_chunks.as<tg_chunk_xz>() + off);
             const size_t at = static_cast<size_t>(off) * kBlocksPerChunk;
             drain(o, {Piece{narrow ? nullptr : blocks + at, biomes ? biomes + static_cast<size_t>(off) * kQuartsPerChunk : nullptr,
                             (!narrow && aquifer) ? aquifer + at : nullptr, 0, n, narrow ? blocks8 + at : nullptr,
