@@ -918,6 +918,10 @@ struct Generator {
     int lanes = 2;
     cudaStream_t lane_stream = nullptr;
     cudaEvent_t ev_entry = nullptr;
+    // per lane: the stream the biome stage runs on beside the lane's other stages, and the
+    // events that fork it from and join it back into the lane's stream
+    cudaStream_t side_stream[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
     OutSlot out[2];
     int next_out = 0;
     int graph_launches = 0;
@@ -939,6 +943,11 @@ struct Generator {
         ck(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
         ck(cudaStreamCreateWithFlags(&lane_stream, cudaStreamNonBlocking), "cudaStreamCreate");
         ck(cudaEventCreateWithFlags(&ev_entry, cudaEventDisableTiming), "cudaEventCreate");
+        for (int l = 0; l < 2; ++l) {
+            ck(cudaStreamCreateWithFlags(&side_stream[l], cudaStreamNonBlocking), "cudaStreamCreate");
+            ck(cudaEventCreateWithFlags(&ev_fork[l], cudaEventDisableTiming), "cudaEventCreate");
+            ck(cudaEventCreateWithFlags(&ev_join[l], cudaEventDisableTiming), "cudaEventCreate");
+        }
         stream = own_stream;
         out[1].lane = lanes == 2 ? 1 : 0;
         for (auto& e : ev) ck(cudaEventCreate(&e), "cudaEventCreate");
@@ -966,6 +975,11 @@ struct Generator {
         for (auto& e : prof_ev)
             if (e) cudaEventDestroy(e);
         if (ev_entry) cudaEventDestroy(ev_entry);
+        for (int l = 0; l < 2; ++l) {
+            if (ev_fork[l]) cudaEventDestroy(ev_fork[l]);
+            if (ev_join[l]) cudaEventDestroy(ev_join[l]);
+            if (side_stream[l]) cudaStreamDestroy(side_stream[l]);
+        }
         if (lane_stream) cudaStreamDestroy(lane_stream);
         if (copy_stream) cudaStreamDestroy(copy_stream);
         if (own_stream) cudaStreamDestroy(own_stream);
@@ -1229,8 +1243,14 @@ struct Generator {
     }
 
     // every kernel of one batch; with timed set, events split the stages; reset: clear the
-    // lane's counters and tables first (else the caller ran reset_lane before)
-    void enqueue_batch(const Work& W, const Batch& B, cudaStream_t s, long nmax, uint16_t* aquifer_dev, bool timed, bool reset = true) {
+    // lane's counters and tables first (else the caller ran reset_lane before).
+    // fork (untimed batches): the biome stage reads only the chunk list, as do the noise,
+    // aquifer and fill stages, so it runs on the lane's side stream beside them and joins
+    // before the first kernel that reads biomes (zoom_uniform): the long last searches of
+    // its climate kernel then overlap the other stages' kernels instead of leaving SMs idle.
+    // Timed batches keep one stream, so that events split the stages.
+    void enqueue_batch(const Work& W, const Batch& B, cudaStream_t s, long nmax, uint16_t* aquifer_dev, bool timed, bool reset = true,
+                       bool fork = true) {
         auto mark = [&](int i) {
             if (timed) ck(cudaEventRecord(ev[i], s), "event");
         };
@@ -1239,7 +1259,15 @@ struct Generator {
         prof_now = timed && prof;
         if (reset) reset_lane(W, s, true);
         mark(0);
-        enqueue_biomes(W, B, s, nmax, false);
+        const int li = &W == &work[0] ? 0 : 1;
+        const bool side = fork && !timed;
+        cudaStream_t sb = side ? side_stream[li] : s;
+        if (side) {
+            ck(cudaEventRecord(ev_fork[li], s), "event");
+            ck(cudaStreamWaitEvent(sb, ev_fork[li], 0), "wait");
+        }
+        enqueue_biomes(W, B, sb, nmax, false);
+        if (side) ck(cudaEventRecord(ev_join[li], sb), "event");
         mark(1);
         const int32_t* n_dev = B.n_dev;
         run_body<body_cc_insert, 25>(K_CC_INSERT, W, s, 25 * nmax, B, n_dev);
@@ -1256,7 +1284,6 @@ struct Generator {
         run_body<body_corner, kRows, TB_MINB_CORNER>(K_CORNER, W, s, 16 * nmax * kRows, B, cnt_c);
         mark(9);
         run_body<body_zoom_table, kZoomVerts>(K_ZOOM_TABLE, W, s, kZoomVerts * nmax, B, n_dev);
-        run_body<body_zoom_uniform, kZoomCells>(K_ZOOM_UNIFORM, W, s, kZoomCells * nmax, B, n_dev);
         mark(2);
         run_body<body_sg_insert, kGrid>(K_SG_INSERT, W, s, kGrid * nmax, B, n_dev);
         launch(k_number<2, sg_key_item, kGrid>, s, kGrid * nmax, B);
@@ -1272,6 +1299,8 @@ struct Generator {
             ck(cudaMemcpyAsync(aquifer_dev, B.blocks, sizeof(uint16_t) * static_cast<size_t>(max_batch) * kBlocksPerChunk, cudaMemcpyDeviceToDevice, s),
                "d2d");
         mark(4);
+        if (side) ck(cudaStreamWaitEvent(s, ev_join[li], 0), "wait");
+        run_body<body_zoom_uniform, kZoomCells>(K_ZOOM_UNIFORM, W, s, kZoomCells * nmax, B, n_dev);
         run_body<body_surface1, 256>(K_SURFACE1, W, s, 256 * nmax, B, n_dev);
         run_body<body_block_biome, 256>(K_BLOCK_BIOME, W, s, 256L * nmax, B, n_dev);
         mark(6);
@@ -1918,7 +1947,8 @@ struct Generator {
         const QueueView Q = queue_view(0);
         launch(k_queue_take, s, max_batch, Q, max_batch, W.d_cx.as<int32_t>(), W.d_cz.as<int32_t>(), W.d_cs.as<int32_t>(), W.d_n.as<int32_t>());
         const Batch B = batch_view(W, &out[0]);
-        enqueue_batch(W, B, s, max_batch, nullptr, false);
+        // one stream: the iteration is captured into a conditional node's body graph
+        enqueue_batch(W, B, s, max_batch, nullptr, false, true, false);
         launch(k_queue_scatter, s, static_cast<long>(max_batch) * (kScatterBlockVecs + kScatterBiomeVecs), Q, out[0].blocks.as<const uint4>(),
                out[0].biomes.as<const uint4>());
         k_queue_advance<<<1, 1, 0, s>>>(Q, h, looped ? 1 : 0);
