@@ -918,10 +918,10 @@ struct Generator {
     int lanes = 2;
     cudaStream_t lane_stream = nullptr;
     cudaEvent_t ev_entry = nullptr;
-    // per lane: the stream the biome stage runs on beside the lane's other stages, and the
-    // events that fork it from and join it back into the lane's stream
-    cudaStream_t side_stream[2] = {nullptr, nullptr};
-    cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr};
+    // per lane: the streams the biome and aquifer stages run on beside the lane's other
+    // stages, and the events that fork them from and join them back into the lane's stream
+    cudaStream_t side_stream[2] = {nullptr, nullptr}, aq_stream[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork[2] = {nullptr, nullptr}, ev_join[2] = {nullptr, nullptr}, ev_join_aq[2] = {nullptr, nullptr};
     OutSlot out[2];
     int next_out = 0;
     int graph_launches = 0;
@@ -945,8 +945,10 @@ struct Generator {
         ck(cudaEventCreateWithFlags(&ev_entry, cudaEventDisableTiming), "cudaEventCreate");
         for (int l = 0; l < 2; ++l) {
             ck(cudaStreamCreateWithFlags(&side_stream[l], cudaStreamNonBlocking), "cudaStreamCreate");
+            ck(cudaStreamCreateWithFlags(&aq_stream[l], cudaStreamNonBlocking), "cudaStreamCreate");
             ck(cudaEventCreateWithFlags(&ev_fork[l], cudaEventDisableTiming), "cudaEventCreate");
             ck(cudaEventCreateWithFlags(&ev_join[l], cudaEventDisableTiming), "cudaEventCreate");
+            ck(cudaEventCreateWithFlags(&ev_join_aq[l], cudaEventDisableTiming), "cudaEventCreate");
         }
         stream = own_stream;
         out[1].lane = lanes == 2 ? 1 : 0;
@@ -978,7 +980,9 @@ struct Generator {
         for (int l = 0; l < 2; ++l) {
             if (ev_fork[l]) cudaEventDestroy(ev_fork[l]);
             if (ev_join[l]) cudaEventDestroy(ev_join[l]);
+            if (ev_join_aq[l]) cudaEventDestroy(ev_join_aq[l]);
             if (side_stream[l]) cudaStreamDestroy(side_stream[l]);
+            if (aq_stream[l]) cudaStreamDestroy(aq_stream[l]);
         }
         if (lane_stream) cudaStreamDestroy(lane_stream);
         if (copy_stream) cudaStreamDestroy(copy_stream);
@@ -1246,8 +1250,10 @@ struct Generator {
     // lane's counters and tables first (else the caller ran reset_lane before).
     // fork (untimed batches): the biome stage reads only the chunk list, as do the noise,
     // aquifer and fill stages, so it runs on the lane's side stream beside them and joins
-    // before the first kernel that reads biomes (zoom_uniform): the long last searches of
-    // its climate kernel then overlap the other stages' kernels instead of leaving SMs idle.
+    // before the first kernel that reads biomes (zoom_uniform); the aquifer stage does not
+    // read the noise stage's corners either, so it runs on a second side stream beside the
+    // noise stage and joins before the fill. The long last items of each stage's kernels then
+    // overlap the other stages' kernels instead of leaving SMs idle.
     // Timed batches keep one stream, so that events split the stages.
     void enqueue_batch(const Work& W, const Batch& B, cudaStream_t s, long nmax, uint16_t* aquifer_dev, bool timed, bool reset = true,
                        bool fork = true) {
@@ -1262,9 +1268,11 @@ struct Generator {
         const int li = &W == &work[0] ? 0 : 1;
         const bool side = fork && !timed;
         cudaStream_t sb = side ? side_stream[li] : s;
+        cudaStream_t sq = side ? aq_stream[li] : s;
         if (side) {
             ck(cudaEventRecord(ev_fork[li], s), "event");
             ck(cudaStreamWaitEvent(sb, ev_fork[li], 0), "wait");
+            ck(cudaStreamWaitEvent(sq, ev_fork[li], 0), "wait");
         }
         enqueue_biomes(W, B, sb, nmax, false);
         if (side) ck(cudaEventRecord(ev_join[li], sb), "event");
@@ -1285,15 +1293,17 @@ struct Generator {
         mark(9);
         run_body<body_zoom_table, kZoomVerts>(K_ZOOM_TABLE, W, s, kZoomVerts * nmax, B, n_dev);
         mark(2);
-        run_body<body_sg_insert, kGrid>(K_SG_INSERT, W, s, kGrid * nmax, B, n_dev);
-        launch(k_number<2, sg_key_item, kGrid>, s, kGrid * nmax, B);
-        run_body<body_sg_resolve, kGrid>(K_SG_RESOLVE, W, s, kGrid * nmax, B, n_dev);
-        run_body<body_surface_level, 1>(K_SURFACE_LEVEL, W, s, 2 * nmax * 100, B, cnt_s);
-        run_body<body_aquifer_cell, kAqCells>(K_AQ_CELL, W, s, kAqCells * nmax, B, n_dev);
-        run_body<body_aquifer_query, kAqQueries>(K_AQ_QUERY, W, s, kAqQueries * nmax, B, n_dev);
-        run_body<body_aquifer_skip, 1>(K_AQ_SKIP, W, s, nmax, B, n_dev);
+        run_body<body_sg_insert, kGrid>(K_SG_INSERT, W, sq, kGrid * nmax, B, n_dev);
+        launch(k_number<2, sg_key_item, kGrid>, sq, kGrid * nmax, B);
+        run_body<body_sg_resolve, kGrid>(K_SG_RESOLVE, W, sq, kGrid * nmax, B, n_dev);
+        run_body<body_surface_level, 1>(K_SURFACE_LEVEL, W, sq, 2 * nmax * 100, B, cnt_s);
+        run_body<body_aquifer_cell, kAqCells>(K_AQ_CELL, W, sq, kAqCells * nmax, B, n_dev);
+        run_body<body_aquifer_query, kAqQueries>(K_AQ_QUERY, W, sq, kAqQueries * nmax, B, n_dev);
+        run_body<body_aquifer_skip, 1>(K_AQ_SKIP, W, sq, nmax, B, n_dev);
+        if (side) ck(cudaEventRecord(ev_join_aq[li], sq), "event");
         mark(3);
         run_body<body_init_heights, 256>(K_INIT_HEIGHTS, W, s, 256 * nmax, B, n_dev);
+        if (side) ck(cudaStreamWaitEvent(s, ev_join_aq[li], 0), "wait");
         run_body<body_fill, 256 * kCellsY, TB_MINB_FILL>(K_FILL, W, s, 256L * kCellsY * nmax, B, n_dev);
         if (aquifer_dev)
             ck(cudaMemcpyAsync(aquifer_dev, B.blocks, sizeof(uint16_t) * static_cast<size_t>(max_batch) * kBlocksPerChunk, cudaMemcpyDeviceToDevice, s),
