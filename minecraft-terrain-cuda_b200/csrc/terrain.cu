@@ -1249,8 +1249,9 @@ struct Generator {
     // every kernel of one batch; with timed set, events split the stages; reset: clear the
     // lane's counters and tables first (else the caller ran reset_lane before).
     // fork (untimed batches): the biome stage reads only the chunk list, as do the noise,
-    // aquifer and fill stages, so it runs on the lane's side stream beside them and joins
-    // before the first kernel that reads biomes (zoom_uniform); the aquifer stage does not
+    // aquifer and fill stages, so it runs on the lane's side stream beside them, followed by
+    // the zoom tables and the quart biome output, and joins before the surface stage; the
+    // aquifer stage does not
     // read the noise stage's corners either, so it runs on a second side stream beside the
     // noise stage and joins before the fill. The long last items of each stage's kernels then
     // overlap the other stages' kernels instead of leaving SMs idle.
@@ -1274,10 +1275,14 @@ struct Generator {
             ck(cudaStreamWaitEvent(sb, ev_fork[li], 0), "wait");
             ck(cudaStreamWaitEvent(sq, ev_fork[li], 0), "wait");
         }
+        const int32_t* n_dev = B.n_dev;
         enqueue_biomes(W, B, sb, nmax, false);
+        // the zoom tables and the quart biome output need only the chunk list and the biomes
+        run_body<body_zoom_table, kZoomVerts>(K_ZOOM_TABLE, W, sb, kZoomVerts * nmax, B, n_dev);
+        run_body<body_zoom_uniform, kZoomCells>(K_ZOOM_UNIFORM, W, sb, kZoomCells * nmax, B, n_dev);
+        run_body<body_gather, kQuartsPerChunk>(K_GATHER, W, sb, static_cast<long>(kQuartsPerChunk) * nmax, B, n_dev);
         if (side) ck(cudaEventRecord(ev_join[li], sb), "event");
         mark(1);
-        const int32_t* n_dev = B.n_dev;
         run_body<body_cc_insert, 25>(K_CC_INSERT, W, s, 25 * nmax, B, n_dev);
         launch(k_number<1, cc_key, 25>, s, 25 * nmax, B);
         run_body<body_cc_resolve, 25>(K_CC_RESOLVE, W, s, 25 * nmax, B, n_dev);
@@ -1291,7 +1296,6 @@ struct Generator {
         mark(8);
         run_body<body_corner, kRows, TB_MINB_CORNER>(K_CORNER, W, s, 16 * nmax * kRows, B, cnt_c);
         mark(9);
-        run_body<body_zoom_table, kZoomVerts>(K_ZOOM_TABLE, W, s, kZoomVerts * nmax, B, n_dev);
         mark(2);
         run_body<body_sg_insert, kGrid>(K_SG_INSERT, W, sq, kGrid * nmax, B, n_dev);
         launch(k_number<2, sg_key_item, kGrid>, sq, kGrid * nmax, B);
@@ -1310,7 +1314,6 @@ struct Generator {
                "d2d");
         mark(4);
         if (side) ck(cudaStreamWaitEvent(s, ev_join[li], 0), "wait");
-        run_body<body_zoom_uniform, kZoomCells>(K_ZOOM_UNIFORM, W, s, kZoomCells * nmax, B, n_dev);
         run_body<body_surface1, 256>(K_SURFACE1, W, s, 256 * nmax, B, n_dev);
         run_body<body_block_biome, 256>(K_BLOCK_BIOME, W, s, 256L * nmax, B, n_dev);
         mark(6);
@@ -1318,7 +1321,6 @@ struct Generator {
         if (W.defer_cap > 0) run_body<body_walk_deferred, 1>(K_WALK_DEFER, W, s, W.defer_cap, B, W.d_defer_count.as<int32_t>());
         mark(7);
         run_body<body_surface_frozen, 256>(K_FROZEN, W, s, 256 * nmax, B, n_dev);
-        run_body<body_gather, kQuartsPerChunk>(K_GATHER, W, s, static_cast<long>(kQuartsPerChunk) * nmax, B, n_dev);
         mark(5);
         prof_now = false;
     }
