@@ -70,7 +70,9 @@ tg_status tg_create(const char* ir_json_path, const char* terrain_json_path, con
 tg_status tg_destroy(struct tg_generator* gen);
 
 /* Runs the generator's work on the caller's CUDA stream (a cudaStream_t; NULL restores
- * the generator's own stream). Calls still return only when their work is done.
+ * the generator's own stream): each batch starts after the work already queued there, and
+ * the stages it runs on the generator's internal side streams fork from and join back into
+ * that stream. Calls still return only when their work is done.
  * No counterpart in the reference (its streams are internal). */
 tg_status tg_set_stream(struct tg_generator* gen, void* cuda_stream);
 
