@@ -47,9 +47,11 @@ BYTES_PER_CHUNK_U8 = 98304 + 1536
 # data the walk-rules kernel touches once per chunk: the u8 biome and u8 ore-vein bits of each
 # block read, its u16 state written, and the column air / fluid masks (2 x 12 words x 256 columns)
 WALK_BYTES_PER_CHUNK = 98304 * (1 + 1 + 2) + 2 * 12 * 4 * 256
-# dram__bytes_read.sum + dram__bytes_write.sum of one 4,096-chunk launch of the walk-rules
-# kernel in this workload (515.35 MB + 288.65 MB), from a one-pass ncu capture of that launch
-WALK_TRAFFIC_PER_LAUNCH = 803998464
+# dram__bytes_read.sum + dram__bytes_write.sum of one 12,288-chunk launch of the walk-rules
+# kernel in this workload: a one-pass ncu capture of a 4,096-chunk launch (515.35 MB + 288.65
+# MB) scaled by the chunks a launch processes (the traffic is per block, so it grows with
+# them)
+WALK_TRAFFIC_PER_LAUNCH = 3 * 803998464
 # Instructions (per thread) one octave sample needs at least, by pipe, following the
 # reference's perlin_volume (cpu/include/mccuda/noise_eval.h:163-178): per axis the coordinate
 # in FP64 (scale multiply, wrap test, offset add, floor, floor back to double, subtract,
@@ -789,8 +791,8 @@ def run_ours(args, rank, world, local_rank):
                               'launch_ms': round(per_launch_ms, 3), 'share_of_step': round(per_launch_ms * calls / stage['kernel_ms'], 3),
                               'note': 'algorithmic bytes = 417,792 B per chunk (per block the u8 biome and u8 ore bits read and the u16 state '
                                       'written, plus the column air / fluid masks) x 12,288 chunks per launch, over the time of the walk and its '
-                                      'deferred pass; traffic = dram read + write bytes of one 12,288-chunk walk launch (ncu; the deferred pass moves '
-                                      '16 B per deferred block, about 10 MB). The kernels are issue- and latency-bound, so their HBM fraction is small'},
+                                      'deferred pass; traffic = dram read + write bytes of one walk launch (ncu capture of a 4,096-chunk launch scaled to '
+                                      '12,288 chunks; the deferred pass moves 16 B per deferred block, about 10 MB). The kernels are issue- and latency-bound, so their HBM fraction is small'},
         'e2e': {'value': round(e2e_value, 1), 'unit': 'chunks/s', 'h2d_bytes_per_step': int(n * nreg * 8),
                 'd2h_bytes_per_step': int(n * nreg * BYTES_PER_CHUNK_U8), 'd2h_gbs': round(e2e_value * BYTES_PER_CHUNK_U8 / 1e9, 2),
                 'pcie_d2h_gbs_measured': pcie, 'pcie_frac': round(e2e_value * BYTES_PER_CHUNK_U8 / 1e9 / pcie, 3) if pcie else None,
