@@ -101,9 +101,9 @@ TB_HD TB_FI CellHash cell_hash(const uint8_t* P, int32_t fx, int32_t fy, int32_t
 
 // The same eight hashes from the paired table: each 16-bit entry holds perm[i] and
 // perm[i + 1], the two values every lattice step reads together, so 7 loads replace 14.
-TB_HD TB_FI CellHash cell_hash2(const uint16_t* P2, int32_t fx, int32_t fy, int32_t fz) {
-    const uint32_t X = static_cast<uint32_t>(fx), Y = static_cast<uint32_t>(fy), Z = static_cast<uint32_t>(fz);
-    const uint32_t a = P2[X & 255u];
+// From the first lookup's entry a = P2[fx & 255] on.
+TB_HD TB_FI CellHash cell_hash2_from(const uint16_t* P2, uint32_t a, int32_t fy, int32_t fz) {
+    const uint32_t Y = static_cast<uint32_t>(fy), Z = static_cast<uint32_t>(fz);
     const uint32_t b0 = P2[((a & 255u) + Y) & 255u], b1 = P2[((a >> 8) + Y) & 255u];
     const uint32_t c00 = P2[((b0 & 255u) + Z) & 255u], c01 = P2[((b0 >> 8) + Z) & 255u];
     const uint32_t c10 = P2[((b1 & 255u) + Z) & 255u], c11 = P2[((b1 >> 8) + Z) & 255u];
@@ -117,6 +117,9 @@ TB_HD TB_FI CellHash cell_hash2(const uint16_t* P2, int32_t fx, int32_t fy, int3
     c.h[6] = c01 >> 8;
     c.h[7] = c11 >> 8;
     return c;
+}
+TB_HD TB_FI CellHash cell_hash2(const uint16_t* P2, int32_t fx, int32_t fy, int32_t fz) {
+    return cell_hash2_from(P2, P2[static_cast<uint32_t>(fx) & 255u], fy, fz);
 }
 #ifndef TB_PERM_PAIRS
 #define TB_PERM_PAIRS 1
@@ -313,7 +316,7 @@ TB_HD TB_NOINLINE inline float stack_point_smeared_rt(const NoiseTables& T, int 
 struct AxisRec {
     int32_t f;
     float r, a;
-    int32_t pad;
+    int32_t hx;   // x records: the paired-permutation entry of the lattice x (the hash's first lookup); else 0
 };
 #ifndef TB_AXIS_TABLE
 #define TB_AXIS_TABLE 1
@@ -358,7 +361,11 @@ TB_HD TB_NOINLINE inline float stack_volume_axy_rt(const NoiseTables& T, int fir
         const Layer L = T.layer[first + k];
         const float amp = amplitude * L.amp;
         const AxisRec X = ax[k], Z = az[k], Y = ay[k];
+#if TB_PERM_PAIRS
+        const CellHash c = cell_hash2_from(T.perm2 + 256 * L.oct, static_cast<uint32_t>(X.hx), Y.f, Z.f);
+#else
         const CellHash c = octave_hash(T, L.oct, X.f, Y.f, Z.f);
+#endif
         acc = acc + amp * cell_volume(c, X.r, Z.r, Y.r, X.a, Y.a, Z.a);
     }
     return acc;

@@ -873,7 +873,9 @@ TB_HD inline void body_axis_fill(const Batch& B, int it) {
 #endif
     const OctaveOff o = T.off[L.oct];
     const AxisSetup a = axis_setup((sem ? qz : qx) * 4, scale, sem ? o.oz : o.ox);
-    B.axtab[static_cast<size_t>(row) * tbm::kAxisLayers + e] = AxisRec{a.f, a.r, a.a, 0};
+    // an x record also holds the octave's first hash lookup, which depends on x alone
+    const int32_t hx = sem ? 0 : static_cast<int32_t>(T.perm2[256 * L.oct + (static_cast<uint32_t>(a.f) & 255u)]);
+    B.axtab[static_cast<size_t>(row) * tbm::kAxisLayers + e] = AxisRec{a.f, a.r, a.a, hx};
 }
 
 TB_HD inline void body_corner_col(const Batch& B, int u) {

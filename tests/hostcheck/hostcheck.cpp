@@ -313,7 +313,7 @@ void axis_row(const NoiseTables& T, int32_t b, bool z, AxisRec* row) {
         const Layer L = T.layer[tbm::kAxisLayer[e]];
         const OctaveOff o = T.off[L.oct];
         const AxisSetup a = axis_setup(b, tbm::kAxisScale[e] * L.freq, z ? o.oz : o.ox);
-        row[e] = AxisRec{a.f, a.r, a.a, 0};
+        row[e] = AxisRec{a.f, a.r, a.a, z ? 0 : static_cast<int32_t>(T.perm2[256 * L.oct + (static_cast<uint32_t>(a.f) & 255u)])};
     }
 }
 
