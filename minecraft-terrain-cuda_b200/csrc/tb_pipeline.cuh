@@ -1496,8 +1496,13 @@ TB_HD inline void body_zoom_uniform(const Batch& B, int it) {
 // height, written 4 heights to a word (column order). Blocks of a uniform zoom cell take its
 // biome; the others pick the nearest fiddled corner in FP64, the 8 candidates' x and z terms
 // once per group of 4 heights.
+// block_biome's warps hold 4 x 8 column tiles (fewer distinct zoom cells per warp, and more
+// lanes in the same uniform or mixed cell: 1.62 -> 1.52 ms per 12,288-chunk step)
+#ifndef TB_BB_TILE
+#define TB_BB_TILE 4
+#endif
 TB_HD inline void body_block_biome(const Batch& B, int it) {
-    const int c = it >> 8, col = it & 255, lx = col & 15, lz = col >> 4;
+    const int c = it >> 8, col = tile_column<TB_BB_TILE>(it), lx = col & 15, lz = col >> 4;
     const int h = B.h1[(static_cast<size_t>(c) << 8) | (lx << 4) | lz];
     const int top = h > kMaxY ? kMaxY : h;
     if (top < tbm::kMinY) return;
@@ -1856,8 +1861,12 @@ TB_HD inline void column_mask_rebuild(const Batch& B, const Column& C) {
     }
 }
 
+// surface1's warps hold 4 x 8 column tiles too (0.491 -> 0.484 ms per 12,288-chunk step)
+#ifndef TB_S1_TILE
+#define TB_S1_TILE 4
+#endif
 TB_HD inline void body_surface1(const Batch& B, int it) {
-    const int c = it >> 8, lz = (it >> 4) & 15, lx = it & 15;
+    const int c = it >> 8, col1 = tile_column<TB_S1_TILE>(it), lz = col1 >> 4, lx = col1 & 15;
     const int ci = (c << 8) | (lx << 4) | lz;   // x * 16 + z column index
     Column C{&B, &B.seeds[B.cseed[c]], B.blocks + static_cast<size_t>(c) * kBlocksPerChunk, c, lx, lz, B.cx[c] * 16 + lx, B.cz[c] * 16 + lz,
              B.h0[ci]};
